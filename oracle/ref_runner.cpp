@@ -1,0 +1,158 @@
+// Project-written driver around the reference's own, unmodified C++ sources
+// (compiled from the reference tree with the FFTW/MPI shims in ref_shim/).
+// Test infrastructure only: it produces golden vectors and the CPU baseline.
+//
+//   ref_runner run <run-dir> <out.bin> [threads]
+//       Params::load -> Mesh -> Transforms -> Simulation::initialize/run
+//       (src/main.cpp:173-225 path), then writes nt, time, the spectral
+//       velocity [kz][y][kx][3] and pressure [kz][y][kx] (complex<double>).
+//       Prints the step-loop wall time (steady_clock, as src/main.cpp:224-233).
+//   ref_runner nonlinear <run-dir> <velocity.bin> <out.bin>
+//       TimeStepper::nonlinear_term (src/solver/timestepper.cpp:11-17):
+//       writes N [kz][y][kx][3] and the pressure wall BC [kz][2][kx].
+//   ref_runner fine <run-dir> <spectral.bin> <out.bin>
+//       Transforms::channel_xyzfft2 'B' then 'F' of one scalar field
+//       (src/fft/transforms.cpp:615-741): writes physical then spectral.
+//   ref_runner solve <run-dir> <g> <rhs.bin> <out.bin>
+//       EqSolvePV::setup(g) then the fused solve_modes with fused RHS and
+//       sigma correction (src/solver/eqsolve_pv.cpp:311-450); input is the
+//       velocity RHS [kz][y][kx][3], pressure BC [kz][2][kx], velocity BC
+//       [kz][2][kx][3]; writes pressure, velocity, u_dpdx_unit, w_dpdz_unit.
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <iostream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "core/cpu_device.hpp"
+#include "core/mesh.hpp"
+#include "core/mpi_context.hpp"
+#include "core/params.hpp"
+#include "fft/transforms.hpp"
+#include "sim/simulation.hpp"
+#include "solver/eqsolve_pv.hpp"
+#include "solver/fields.hpp"
+#include "solver/timestepper.hpp"
+
+// Friend hook declared by the reference (src/solver/eqsolve_pv.hpp:11,34).
+struct EqSolvePVTestAccess {
+    static void solve(EqSolvePV &s, ScalarField &p, const ScalarBoundary &pbc, VectorField &v,
+                      const VectorField &rhs, const VectorBoundary &vbc) {
+        s.solve_modes(p, nullptr, pbc, v, rhs, vbc, true);
+    }
+};
+
+namespace {
+template <typename T> void read_all(const std::string &path, std::vector<T> &out) {
+    std::ifstream in(path, std::ios::binary);
+    if (!in) throw std::runtime_error("cannot open " + path);
+    in.seekg(0, std::ios::end);
+    const auto bytes = static_cast<std::size_t>(in.tellg());
+    in.seekg(0);
+    if (bytes != out.size() * sizeof(T))
+        throw std::runtime_error(path + ": expected " + std::to_string(out.size() * sizeof(T)) +
+                                 " bytes, found " + std::to_string(bytes));
+    in.read(reinterpret_cast<char *>(out.data()), static_cast<std::streamsize>(bytes));
+}
+
+template <typename T> void write(std::ofstream &out, const T *data, std::size_t n) {
+    out.write(reinterpret_cast<const char *>(data), static_cast<std::streamsize>(n * sizeof(T)));
+}
+
+void fill(Array4D<std::complex<double>> &f, const std::complex<double> *src) {
+    std::copy(src, src + f.size(), f.data());
+}
+}  // namespace
+
+int main(int argc, char **argv) {
+    if (argc < 4) {
+        std::cerr << "usage: ref_runner run|nonlinear|fine|solve <run-dir> ...\n";
+        return 2;
+    }
+    const std::string mode = argv[1];
+    const std::string dir = argv[2];
+    try {
+        int threads = 1;
+        if (mode == "run" && argc > 4) threads = std::atoi(argv[4]);
+        cpu_device(threads);
+        MpiContext mpi(MPI_COMM_WORLD);
+        Params params = Params::load(dir);
+        Mesh mesh(params.mesh, params.parm.XL, params.parm.ZL, 0, 1);
+        Transforms fft(mesh, params.parm.XL, params.parm.ZL, params.parm.Re, "", &mpi);
+        if (mode == "run") {
+            Simulation sim(params, mesh, fft, dir, &mpi);
+            sim.initialize();
+            const auto start = std::chrono::steady_clock::now();
+            sim.run();
+            const double wall =
+                std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
+            std::cout << "ref_runner: steps " << params.ctrl.NSTEPS << " wall " << wall
+                      << " s threads " << threads << "\n";
+            std::ofstream out(argv[3], std::ios::binary);
+            const std::int64_t nt = sim.nt();
+            const double t = sim.time();
+            write(out, &nt, 1);
+            write(out, &t, 1);
+            write(out, sim.velocity().data(), sim.velocity().size());
+            write(out, sim.pressure().data(), sim.pressure().size());
+            return out ? 0 : 1;
+        }
+        if (mode == "nonlinear" && argc >= 5) {
+            EqSolvePV solver(params, mesh, fft);
+            TimeStepper stepper(params, mesh, fft, solver);
+            VectorField velocity = make_vector_field(mesh), nl = make_vector_field(mesh);
+            ScalarBoundary bc = make_scalar_boundary(mesh);
+            std::vector<std::complex<double>> buf(velocity.size());
+            read_all(argv[3], buf);
+            fill(velocity, buf.data());
+            stepper.nonlinear_term(nl, velocity, bc);
+            std::ofstream out(argv[4], std::ios::binary);
+            write(out, nl.data(), nl.size());
+            write(out, bc.data(), bc.size());
+            return out ? 0 : 1;
+        }
+        if (mode == "fine" && argc >= 5) {
+            ScalarField spec = make_scalar_field(mesh), back = make_scalar_field(mesh);
+            std::vector<std::complex<double>> buf(spec.size());
+            read_all(argv[3], buf);
+            fill(spec, buf.data());
+            std::vector<double> phys(static_cast<std::size_t>(mesh.NZ2) * (mesh.NY2P + 1) *
+                                     mesh.NX2);
+            fft.channel_xyzfft2('B', phys.data(), spec.data());
+            fft.channel_xyzfft2('F', phys.data(), back.data());
+            std::ofstream out(argv[4], std::ios::binary);
+            write(out, phys.data(), phys.size());
+            write(out, back.data(), back.size());
+            return out ? 0 : 1;
+        }
+        if (mode == "solve" && argc >= 6) {
+            const double g = std::atof(argv[3]);
+            EqSolvePV solver(params, mesh, fft);
+            solver.setup(g);
+            VectorField rhs = make_vector_field(mesh), vel = make_vector_field(mesh);
+            ScalarField pres = make_scalar_field(mesh);
+            ScalarBoundary pbc = make_scalar_boundary(mesh);
+            VectorBoundary vbc = make_vector_boundary(mesh);
+            std::vector<std::complex<double>> buf(rhs.size() + pbc.size() + vbc.size());
+            read_all(argv[4], buf);
+            fill(rhs, buf.data());
+            fill(pbc, buf.data() + rhs.size());
+            fill(vbc, buf.data() + rhs.size() + pbc.size());
+            EqSolvePVTestAccess::solve(solver, pres, pbc, vel, rhs, vbc);
+            std::ofstream out(argv[5], std::ios::binary);
+            write(out, pres.data(), pres.size());
+            write(out, vel.data(), vel.size());
+            write(out, solver.u_dpdx_unit().data(), solver.u_dpdx_unit().size());
+            write(out, solver.w_dpdz_unit().data(), solver.w_dpdz_unit().size());
+            return out ? 0 : 1;
+        }
+        std::cerr << "ref_runner: bad arguments\n";
+        return 2;
+    } catch (const std::exception &e) {
+        std::cerr << "ref_runner: " << e.what() << "\n";
+        return 1;
+    }
+}

@@ -1,0 +1,95 @@
+"""Generate the golden fixtures in this folder from the reference's own sources.
+
+Runs ``oracle/_ref/ref_runner`` (the reference C++ solver compiled from its
+unmodified sources against the project FFTW/MPI shims; ``make -C oracle``)
+on small seeded inputs and stores inputs and outputs as compressed npz files:
+
+  golden_step.npz       16x17x16 channel (3/2 product grid), 4 steps from a
+                        seeded divergence-free field: velocity and pressure.
+  golden_example.npz    the reference's unit-test case shrunk to 16^3
+                        (NXS=NZS=8, NYS=14, product grid = base grid, so the
+                        Nyquist branches run; constant flow rate, wall
+                        blowing 1e-3), 3 steps.
+  golden_nonlinear.npz  nonlinear term N and pressure wall BC for a seeded
+                        band-limited velocity (same shapes).
+  golden_solve.npz      setup(g=150) + fused solve of a seeded RHS with
+                        random wall data (NXS=5: a ragged x extent).
+  golden_fine.npz       fine-grid backward/forward transforms of a band
+                        spectrum on a 3/2 product grid.
+
+Usage: python tests/golden/make_golden.py   (needs oracle/_ref built)
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path[:0] = [os.path.join(ROOT, "tests"), os.path.join(ROOT, "oracle")]
+
+import ref_io  # noqa: E402
+from oracle_cases import band_spectrum, channel_case, divergence_free_field, example_case, orc  # noqa: E402
+
+
+def mesh_dict(m, p):
+    return dict(mesh=np.array([m.NX, m.NY, m.NZ, m.NXS, m.NYS, m.NZS, m.NX2, m.NY2, m.NZ2]),
+                dom=np.array([m.XL, m.ZL]),
+                parm=np.array([p.Re, p.G_pre, p.a_pre0, p.b_pre0, *p.a_V, *p.b_V,
+                               p.INDEX_GRAD_PRE, p.THETA, p.DT, p.V_Microblow0]))
+
+
+def main():
+    if not ref_io.available():
+        raise SystemExit("oracle/_ref is not built: run make -C oracle")
+    # 1. small channel, 4 steps
+    m, p = channel_case(16)
+    u0 = divergence_free_field(m, p, seed=11, amp=0.05, kmax=4)
+    ru, rp, _ = ref_io.run_steps(m, p, u0, 4)
+    np.savez_compressed(os.path.join(HERE, "golden_step.npz"), **mesh_dict(m, p), nsteps=4,
+                        u0=np.stack(u0), u=np.stack(ru), p=rp)
+    # 2. example case at 16^3 (full-spectrum Nyquist branch), 3 steps
+    m, p = example_case(NXS=8, NYS=14, NZS=8, N2=16, N=16)
+    u0 = [band_spectrum(m, s, 1e-3) for s in (21, 22, 23)]
+    u0[0][m.NZS, :, 0] += np.array([1.5 * (v) for v in
+                                    _cheb_1my2(m.ncy)])  # laminar mean 1.5(1-y^2)
+    ru, rp, _ = ref_io.run_steps(m, p, u0, 3)
+    np.savez_compressed(os.path.join(HERE, "golden_example.npz"), **mesh_dict(m, p), nsteps=3,
+                        u0=np.stack(u0), u=np.stack(ru), p=rp)
+    # 3. nonlinear term
+    us = [band_spectrum(m, s, 0.1) for s in (4, 5, 6)]
+    N, B = ref_io.nonlinear(m, p, us)
+    np.savez_compressed(os.path.join(HERE, "golden_nonlinear.npz"), **mesh_dict(m, p),
+                        u=np.stack(us), N=np.stack(N), B=np.stack(B))
+    # 4. solve (Dirichlet walls; random wall data and RHS)
+    m, p = example_case(NXS=5, NYS=14, NZS=8, N2=16, N=16)
+    rng = np.random.default_rng(31)
+    sh = m.spectral_shape()
+    rv = [(rng.standard_normal(sh) + 1j * rng.standard_normal(sh)) * 1e-3 for _ in range(3)]
+    bp = tuple((rng.standard_normal((m.nkz, m.nkx)) + 1j * rng.standard_normal((m.nkz, m.nkx))) * 1e-3
+               for _ in range(2))
+    bv = [tuple((rng.standard_normal((m.nkz, m.nkx)) + 1j * rng.standard_normal((m.nkz, m.nkx))) * 1e-3
+                for _ in range(2)) for _ in range(3)]
+    pres, vel, uu, wu = ref_io.solve(m, p, 150.0, rv, bp, bv)
+    np.savez_compressed(os.path.join(HERE, "golden_solve.npz"), **mesh_dict(m, p), g=150.0,
+                        rhs=np.stack(rv), bc_p=np.stack(bp), bc_v=np.array([np.stack(b) for b in bv]),
+                        p=pres, v=np.stack(vel), u_unit=uu, w_unit=wu)
+    # 5. fine transforms on a 3/2 grid
+    m, p = channel_case(16)
+    U = band_spectrum(m, 41)
+    phys, back = ref_io.fine(m, p, U)
+    np.savez_compressed(os.path.join(HERE, "golden_fine.npz"), **mesh_dict(m, p), U=U,
+                        phys=phys, back=back)
+    print("golden fixtures written to", HERE)
+
+
+def _cheb_1my2(ncy):
+    # 1 - y^2 = 0.5 T0 - 0.5 T2
+    a = np.zeros(ncy)
+    a[0] = 0.5
+    a[2] = -0.5
+    return a
+
+
+if __name__ == "__main__":
+    main()

@@ -22,9 +22,10 @@ import channel_oracle as orc  # noqa: E402
 PI = math.acos(-1.0)
 
 
-def example_case(NXS=16, NYS=30, NZS=16, N2=32, a_v1=1.0, b_v1=0.0):
-    """The reference unit-test fixture (examples/config.toml values)."""
-    m = orc.Mesh(32, 32, 32, NXS, NYS, NZS, N2, N2, N2, 10.0, 10.0)
+def example_case(NXS=16, NYS=30, NZS=16, N2=32, a_v1=1.0, b_v1=0.0, N=32):
+    """The reference unit-test fixture (examples/config.toml values); ``N``
+    shrinks the base grid for small fixtures."""
+    m = orc.Mesh(N, N, N, NXS, NYS, NZS, N2, N2, N2, 10.0, 10.0)
     a_V = (1.0, a_v1, 1.0)
     b_V = (0.0, b_v1, 0.0)
     p = orc.Parm(Re=2800.0, G_pre=0.0, a_pre0=0.0, b_pre0=1.0, a_V=a_V, b_V=b_V,
