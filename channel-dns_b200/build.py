@@ -1,0 +1,38 @@
+"""Build libcdns_cuda.so in-tree for sm_100a (nvcc, no JIT).
+
+Usage: python channel-dns_b200/build.py [--debug]
+The library lands beside the Python package: channel-dns_b200/cdns/libcdns_cuda.so
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+OUT = os.path.join(HERE, "cdns", "libcdns_cuda.so")
+SOURCES = ["context.cu", "transforms.cu", "solver.cu", "layout.cu"]
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def build(verbose: bool = False, extra=None) -> str:
+    srcs = [os.path.join(CSRC, s) for s in SOURCES]
+    deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cuh")]
+    deps.append(os.path.join(ROOT, "include", "cdns.h"))
+    if os.path.exists(OUT) and all(os.path.getmtime(OUT) >= os.path.getmtime(d) for d in deps) \
+            and not extra:
+        return OUT
+    cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
+           "-I", os.path.join(ROOT, "include"), "-o", OUT, *srcs, "-lcudart"]
+    if extra:
+        cmd[1:1] = list(extra)
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return OUT
+
+
+if __name__ == "__main__":
+    extra = ["-Xptxas", "-v"] if "--ptxas" in sys.argv else None
+    print(build(verbose=True, extra=extra))

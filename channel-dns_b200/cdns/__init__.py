@@ -1,0 +1,317 @@
+"""Python host side of the B200 channel-dns time step (ctypes over the C ABI).
+
+The product is ``libcdns_cuda.so`` (``include/cdns.h``); this module mirrors
+the reference driver's view of the hot path -- Params/Mesh from a run
+directory's ``config.toml`` (src/core/params.cpp:130-228), a context that
+owns the device state, ``step``/``run`` of Simulation::run
+(src/sim/simulation.cpp:173-185) and the state hand-over in the reference's
+spectral layout.  There is no CPU fallback: every call goes to the CUDA
+library, and importing without the built library raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+from dataclasses import dataclass, field
+from typing import Optional, Sequence, Tuple
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcdns_cuda.so")
+
+CDNS_OK = 0
+STATUS = {1: "CDNS_ERR_ARG", 2: "CDNS_ERR_CUDA", 3: "CDNS_ERR_STATE", 4: "CDNS_ERR_NONFINITE",
+          5: "CDNS_ERR_PIVOT", 6: "CDNS_ERR_NOMEM"}
+
+
+class CdnsError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{STATUS.get(code, code)}: {message}")
+        self.code = code
+
+
+class MeshDesc(ctypes.Structure):
+    _fields_ = [("NX", ctypes.c_int), ("NY", ctypes.c_int), ("NZ", ctypes.c_int),
+                ("NXS", ctypes.c_int), ("NYS", ctypes.c_int), ("NZS", ctypes.c_int),
+                ("NX2", ctypes.c_int), ("NY2", ctypes.c_int), ("NZ2", ctypes.c_int),
+                ("XL", ctypes.c_double), ("ZL", ctypes.c_double)]
+
+
+class ParamsDesc(ctypes.Structure):
+    _fields_ = [("Re", ctypes.c_double), ("G_pre", ctypes.c_double), ("a_pre0", ctypes.c_double),
+                ("b_pre0", ctypes.c_double), ("a_V", ctypes.c_double * 3), ("b_V", ctypes.c_double * 3),
+                ("INDEX_GRAD_PRE", ctypes.c_int), ("THETA", ctypes.c_double), ("DT", ctypes.c_double),
+                ("V_Microblow0", ctypes.c_double)]
+
+
+_lib = None
+
+_SIGNATURES = {
+    "cdns_create": [ctypes.POINTER(MeshDesc), ctypes.POINTER(ParamsDesc), ctypes.c_int, ctypes.c_int,
+                    ctypes.POINTER(ctypes.c_void_p)],
+    "cdns_destroy": [ctypes.c_void_p],
+    "cdns_set_velocity": [ctypes.c_void_p, ctypes.c_void_p],
+    "cdns_get_velocity": [ctypes.c_void_p, ctypes.c_void_p],
+    "cdns_get_pressure": [ctypes.c_void_p, ctypes.c_void_p],
+    "cdns_set_velocity_bc": [ctypes.c_void_p, ctypes.c_void_p],
+    "cdns_set_velocity_device": [ctypes.c_void_p, ctypes.c_void_p],
+    "cdns_get_velocity_device": [ctypes.c_void_p, ctypes.c_void_p],
+    "cdns_step": [ctypes.c_void_p, ctypes.c_int],
+    "cdns_run": [ctypes.c_void_p, ctypes.c_int, ctypes.c_int],
+    "cdns_synchronize": [ctypes.c_void_p],
+    "cdns_get_dpdx": [ctypes.c_void_p, ctypes.c_void_p],
+    "cdns_nonlinear": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+    "cdns_transform_fine": [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
+    "cdns_solve": [ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+    "cdns_profile_begin": [ctypes.c_void_p],
+    "cdns_profile_end": [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)],
+    "cdns_stage_count": [],
+    "cdns_stage_name": [ctypes.c_int],
+    "cdns_device_bytes": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t)],
+    "cdns_get_stream": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)],
+    "cdns_last_error": [ctypes.c_char_p, ctypes.c_size_t],
+    "cdns_version": [],
+}
+
+
+def lib() -> ctypes.CDLL:
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with channel-dns_b200/build.py")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, args in _SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = ctypes.c_int
+        L.cdns_stage_name.restype = ctypes.c_char_p
+        L.cdns_version.restype = ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+def _check(code: int) -> None:
+    if code != CDNS_OK:
+        buf = ctypes.create_string_buffer(1024)
+        lib().cdns_last_error(buf, 1024)
+        raise CdnsError(code, buf.value.decode(errors="replace"))
+
+
+# ---------------------------------------------------------------------------
+# Mesh / parameters (src/core/params.hpp, src/core/params.cpp)
+# ---------------------------------------------------------------------------
+@dataclass
+class Mesh:
+    NX: int
+    NY: int
+    NZ: int
+    NXS: int
+    NYS: int
+    NZS: int
+    NX2: int
+    NY2: int
+    NZ2: int
+    XL: float
+    ZL: float
+
+    @property
+    def spectral_shape(self) -> Tuple[int, int, int]:
+        return (2 * self.NZS + 1, self.NYS + 1, self.NXS + 1)
+
+    @property
+    def fine_shape(self) -> Tuple[int, int, int]:
+        return (self.NZ2, self.NY2 + 1, self.NX2)
+
+    def desc(self) -> MeshDesc:
+        return MeshDesc(self.NX, self.NY, self.NZ, self.NXS, self.NYS, self.NZS, self.NX2, self.NY2,
+                        self.NZ2, self.XL, self.ZL)
+
+
+@dataclass
+class Params:
+    Re: float
+    DT: float
+    G_pre: float = 0.0
+    a_pre0: float = 0.0
+    b_pre0: float = 1.0
+    a_V: Sequence[float] = (1.0, 1.0, 1.0)
+    b_V: Sequence[float] = (0.0, 0.0, 0.0)
+    INDEX_GRAD_PRE: int = 1
+    THETA: float = 0.0
+    V_Microblow0: float = 0.0
+
+    def desc(self) -> ParamsDesc:
+        return ParamsDesc(self.Re, self.G_pre, self.a_pre0, self.b_pre0, (ctypes.c_double * 3)(*self.a_V),
+                          (ctypes.c_double * 3)(*self.b_V), self.INDEX_GRAD_PRE, self.THETA, self.DT,
+                          self.V_Microblow0)
+
+
+def load_config(run_dir: str) -> Tuple[Mesh, Params, dict]:
+    """Read ``<run_dir>/config.toml`` as Params::load does (src/core/params.cpp:130-228):
+    case-insensitive keys in [mesh], [parm], [control].  Returns (mesh, params, control)."""
+    import tomllib
+    with open(os.path.join(run_dir, "config.toml"), "rb") as fh:
+        raw = tomllib.load(fh)
+    t = {k.lower(): {kk.lower(): vv for kk, vv in v.items()} if isinstance(v, dict) else v
+         for k, v in raw.items()}
+    me, pa, co = t["mesh"], t["parm"], t["control"]
+    if int(me.get("index_serial", 1)) != 1:
+        raise ValueError("the GPU step runs the single-rank layout (INDEX_Serial = 1)")
+    mesh = Mesh(me["nx"], me["ny"], me["nz"], me["nxs"], me["nys"], me["nzs"], me["nx2"], me["ny2"],
+                me["nz2"], float(pa["xl"]), float(pa["zl"]))
+    params = Params(Re=float(pa["re"]), DT=float(co["dt"]), G_pre=float(pa["g_pre"]),
+                    a_pre0=float(pa["a_pre0"]), b_pre0=float(pa["b_pre0"]),
+                    a_V=tuple(float(v) for v in pa["a_v"]), b_V=tuple(float(v) for v in pa["b_v"]),
+                    INDEX_GRAD_PRE=int(pa["index_grad_pre"]), THETA=float(pa["theta"]),
+                    V_Microblow0=float(co["v_microblow0"]))
+    return mesh, params, co
+
+
+def step_coefficients(iteration: int, dt: float, reynolds: float):
+    """src/sim/simulation.cpp:36-45 (host mirror of the coefficients the
+    library computes)."""
+    if iteration < 1 or dt <= 0.0:
+        raise ValueError("invalid time-step coefficients")
+    eff = iteration if iteration < 3 else 2
+    a0 = float(eff) / dt
+    a1 = float(1 - eff) / (2.0 * dt)
+    return a0, a1, float(eff), float(1 - eff), (a0 + a1) * reynolds
+
+
+def _ptr(a: np.ndarray) -> ctypes.c_void_p:
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class Context:
+    """One device context: the state of Simulation's hot path on a B200."""
+
+    def __init__(self, mesh: Mesh, params: Params, device: int = 0, precision: int = 0):
+        self.mesh = mesh
+        self.params = params
+        self._h = ctypes.c_void_p()
+        md, pd = mesh.desc(), params.desc()
+        _check(lib().cdns_create(ctypes.byref(md), ctypes.byref(pd), precision, device,
+                                 ctypes.byref(self._h)))
+
+    def close(self) -> None:
+        if self._h:
+            lib().cdns_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    # ---- state hand-over (reference layout) ----
+    def set_velocity(self, u: np.ndarray) -> None:
+        u = np.ascontiguousarray(u, dtype=np.complex128)
+        if u.shape != self.mesh.spectral_shape + (3,):
+            raise ValueError(f"velocity must have shape {self.mesh.spectral_shape + (3,)}")
+        _check(lib().cdns_set_velocity(self._h, _ptr(u)))
+
+    def get_velocity(self) -> np.ndarray:
+        out = np.empty(self.mesh.spectral_shape + (3,), dtype=np.complex128)
+        _check(lib().cdns_get_velocity(self._h, _ptr(out)))
+        return out
+
+    def get_pressure(self) -> np.ndarray:
+        out = np.empty(self.mesh.spectral_shape, dtype=np.complex128)
+        _check(lib().cdns_get_pressure(self._h, _ptr(out)))
+        return out
+
+    def set_velocity_bc(self, bc: np.ndarray) -> None:
+        nkz, _, nkx = self.mesh.spectral_shape
+        bc = np.ascontiguousarray(bc, dtype=np.complex128)
+        if bc.shape != (nkz, 2, nkx, 3):
+            raise ValueError("velocity BC must have shape [2*NZS+1][2][NXS+1][3]")
+        _check(lib().cdns_set_velocity_bc(self._h, _ptr(bc)))
+
+    def set_velocity_device(self, ptr: int) -> None:
+        _check(lib().cdns_set_velocity_device(self._h, ctypes.c_void_p(ptr)))
+
+    def get_velocity_device(self, ptr: int) -> None:
+        _check(lib().cdns_get_velocity_device(self._h, ctypes.c_void_p(ptr)))
+
+    # ---- stepping ----
+    def step(self, iteration: int) -> None:
+        _check(lib().cdns_step(self._h, iteration))
+
+    def run(self, first_iteration: int, nsteps: int) -> None:
+        _check(lib().cdns_run(self._h, first_iteration, nsteps))
+
+    def synchronize(self) -> None:
+        _check(lib().cdns_synchronize(self._h))
+
+    def dpdx(self) -> Tuple[float, float]:
+        out = np.zeros(2)
+        _check(lib().cdns_get_dpdx(self._h, _ptr(out)))
+        return float(out[0]), float(out[1])
+
+    # ---- pieces of the hot path ----
+    def nonlinear(self, u: np.ndarray):
+        u = np.ascontiguousarray(u, dtype=np.complex128)
+        nkz, ncy, nkx = self.mesh.spectral_shape
+        N = np.empty((nkz, ncy, nkx, 3), dtype=np.complex128)
+        B = np.empty((nkz, 2, nkx), dtype=np.complex128)
+        _check(lib().cdns_nonlinear(self._h, _ptr(u), _ptr(N), _ptr(B)))
+        return N, B
+
+    def transform_fine(self, direction: str, data: np.ndarray) -> np.ndarray:
+        if direction == "B":
+            src = np.ascontiguousarray(data, dtype=np.complex128)
+            out = np.empty(self.mesh.fine_shape, dtype=np.float64)
+        elif direction == "F":
+            src = np.ascontiguousarray(data, dtype=np.float64)
+            out = np.empty(self.mesh.spectral_shape, dtype=np.complex128)
+        else:
+            raise ValueError("direction must be 'B' or 'F'")
+        _check(lib().cdns_transform_fine(self._h, ord(direction), _ptr(src), _ptr(out)))
+        return out
+
+    def solve(self, g: float, rhs: np.ndarray, pressure_bc: np.ndarray, velocity_bc: np.ndarray):
+        nkz, ncy, nkx = self.mesh.spectral_shape
+        rhs = np.ascontiguousarray(rhs, dtype=np.complex128)
+        pbc = np.ascontiguousarray(pressure_bc, dtype=np.complex128)
+        vbc = np.ascontiguousarray(velocity_bc, dtype=np.complex128)
+        p = np.empty((nkz, ncy, nkx), dtype=np.complex128)
+        v = np.empty((nkz, ncy, nkx, 3), dtype=np.complex128)
+        units = np.empty(2 * ncy)
+        _check(lib().cdns_solve(self._h, g, _ptr(rhs), _ptr(pbc), _ptr(vbc), _ptr(p), _ptr(v),
+                                _ptr(units)))
+        return p, v, units[:ncy].copy(), units[ncy:].copy()
+
+    # ---- per-stage timing ----
+    def profile_begin(self) -> None:
+        _check(lib().cdns_profile_begin(self._h))
+
+    def profile_end(self):
+        n = lib().cdns_stage_count()
+        ms = np.zeros(n)
+        steps = ctypes.c_int(0)
+        _check(lib().cdns_profile_end(self._h, _ptr(ms), ctypes.byref(steps)))
+        names = [lib().cdns_stage_name(i).decode() for i in range(n)]
+        return dict(zip(names, ms.tolist())), steps.value
+
+    def stream_ptr(self) -> int:
+        s = ctypes.c_void_p()
+        _check(lib().cdns_get_stream(self._h, ctypes.byref(s)))
+        return int(s.value or 0)
+
+    def device_bytes(self) -> int:
+        b = ctypes.c_size_t(0)
+        _check(lib().cdns_device_bytes(self._h, ctypes.byref(b)))
+        return int(b.value)
+
+
+def version() -> str:
+    return lib().cdns_version().decode()

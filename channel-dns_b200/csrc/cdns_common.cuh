@@ -1,0 +1,68 @@
+// Shared device-side definitions for the channel-dns B200 step.
+//
+// Spectral fields live in HBM component-planar: component c of a vector field
+// is a contiguous complex<double> array [kz+NZS][y][kx] (the reference's
+// per-component order, src/core/array4d.hpp:62-67, with the component index
+// moved outermost).  The flattened column index col = kz_idx*nkx + kx numbers
+// the independent (kz, kx) Fourier modes.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace cdns {
+
+struct Dims {
+    int NX2, NY2, NZ2;   // product (fine) grid: x points, y intervals, z points
+    int NXS, NYS, NZS;   // retained modes
+    int nkx, nkz, ncy;   // NXS+1, 2 NZS+1, NYS+1
+    int ny2;             // NY2+1 Gauss-Lobatto points
+    int ncol;            // nkz*nkx spectral columns
+    int nyh;             // NY2/2+1 (half of the y points, symmetric pairs)
+    long long Ns;        // nkz*ncy*nkx complex values per spectral component
+};
+
+// Read-only per-context tables in device memory.
+struct Tables {
+    const double *wavx;   // [nkx]  kx*2pi/XL
+    const double *wavz;   // [nkz]  kz*2pi/ZL
+    const double *WL, *WD, *WR;  // [ncy] Chebyshev integration weights
+    const double *cosy;   // [2*NY2] cos(pi m / NY2)
+    const double2 *root_x;  // [NX2] exp(-2 pi i k / NX2)
+    const double2 *root_z;  // [NZ2] exp(-2 pi i k / NZ2)
+};
+
+struct FftPlan {
+    int n;
+    int nrad;
+    int radix[12];
+};
+
+__host__ __device__ inline double2 mk(double re, double im) { return make_double2(re, im); }
+__device__ inline double2 cadd(double2 a, double2 b) { return mk(a.x + b.x, a.y + b.y); }
+__device__ inline double2 csub(double2 a, double2 b) { return mk(a.x - b.x, a.y - b.y); }
+__device__ inline double2 cmul(double2 a, double2 b) {
+    return mk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ inline double2 cscale(double s, double2 a) { return mk(s * a.x, s * a.y); }
+__device__ inline double2 cconj(double2 a) { return mk(a.x, -a.y); }
+// (i*k)*(a+ib) in the reference's form (src/core/complex_ops.hpp:6-8)
+__device__ inline double2 fderiv(double k, double2 v) { return mk(-k * v.y, k * v.x); }
+// complex division in Smith's form (what libgcc's __divdc3 reduces to for
+// finite operands)
+__device__ inline double2 cdiv(double2 a, double2 b) {
+    if (fabs(b.x) >= fabs(b.y)) {
+        const double r = b.y / b.x;
+        const double den = b.x + b.y * r;
+        return mk((a.x + a.y * r) / den, (a.y - a.x * r) / den);
+    }
+    const double r = b.x / b.y;
+    const double den = b.x * r + b.y;
+    return mk((a.x * r + a.y) / den, (a.y * r - a.x) / den);
+}
+__device__ inline double2 cdivr(double2 a, double s) { return mk(a.x / s, a.y / s); }
+
+// Error bits recorded on the device and read by the host after a step.
+enum : unsigned { ERR_NONFINITE = 1u, ERR_PIVOT = 2u };
+
+}  // namespace cdns

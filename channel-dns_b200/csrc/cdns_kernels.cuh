@@ -1,0 +1,76 @@
+// Launch wrappers shared between the kernel translation units and the
+// context code.
+#pragma once
+
+#include "cdns_common.cuh"
+
+namespace cdns {
+
+// ---- transforms.cu ----
+cudaError_t configure_transform_kernels(const Dims &d);
+void launch_curl_ysynth(const Dims &d, const Tables &t, const double2 *u, double2 *F, double2 *bw,
+                        double re, bool curl, cudaStream_t s);
+void launch_z_backward(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *F,
+                       double2 *G, int nf, cudaStream_t s);
+void launch_x_cross(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G,
+                    double2 *H, cudaStream_t s);
+void launch_z_forward(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *H,
+                      double2 *F, int nf, cudaStream_t s);
+void launch_y_analysis(const Dims &d, const Tables &t, const double2 *F, double2 *S, int nf,
+                       cudaStream_t s);
+void launch_x_c2r(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G,
+                  double *phys, cudaStream_t s);
+void launch_x_r2c(const Dims &d, const FftPlan &P, const double2 *roots, const double *phys,
+                  double2 *H, cudaStream_t s);
+
+// ---- solver.cu ----
+// Precomputed solver state (EqSolvePV members, src/solver/eqsolve_pv.hpp:60-76).
+struct SolverState {
+    double *wn_p, *wn_v;        // [ncol]
+    double *ad_p, *ad_v;        // [nkz][ncy][nkx]
+    double2 *p_inf;             // [2][Ns]
+    double2 *v_inf;             // [2][3][Ns]
+    double2 *inf_div;           // [2 (response)][2 (wall)][ncol]
+    double2 *p_b;               // [Ns]
+    double2 *v_b;               // [3][Ns]
+    double2 *sigma0;            // [2][ncol]
+    double *unit;               // [2][ncy] u_dpdx_unit, w_dpdz_unit ; [2*ncy..] qx, qz
+};
+
+struct PhysParams {
+    double Re, G_pre, a_pre0, b_pre0;
+    double a_V[3], b_V[3];
+    int grad_pre;               // INDEX_GRAD_PRE
+    double gx, gz;              // GRAD_PRE_X/Z
+    double qxm, qzm;            // QXmean/QZmean
+};
+
+struct StepArgs {
+    const double2 *u, *u_prev, *N, *N_prev;   // planar 3-component spectral fields
+    const double2 *bw;          // [2][ncol] vorticity part of the wall condition
+    const double2 *B_prev;      // [2][ncol]
+    double2 *B_new;             // [2][ncol]
+    const double2 *bc_v;        // [3][2][ncol]
+    double2 *u_out;             // [3][Ns]
+    double2 *p_out;             // [Ns]
+    double *dpdx;               // [2]
+    unsigned *err;
+    double a0, a1, b0, b1;
+    const double2 *bc_p;        // if set: pressure wall data [2][ncol] used as is
+    int solve_only;             // 1: solve_modes alone (no zero-mode / flow correction)
+};
+
+void setup_solver(const Dims &d, const Tables &t, const PhysParams &pp, double g_v,
+                  SolverState &st, double2 *scratch, cudaStream_t s);
+void launch_step_solve(const Dims &d, const Tables &t, const PhysParams &pp, double g_v,
+                       const SolverState &st, const StepArgs &a, cudaStream_t s);
+cudaError_t configure_solver_kernels(const Dims &d);
+// Pressure wall data of a standalone nonlinear evaluation: B = bw + endpoint sums of N_y.
+void launch_pressure_bc(const Dims &d, const double2 *N, const double2 *bw, double2 *B,
+                        cudaStream_t s);
+
+// ---- layout.cu ----
+void launch_deinterleave(const double2 *src, double2 *dst, long long n, int nc, cudaStream_t s);
+void launch_interleave(const double2 *src, double2 *dst, long long n, int nc, cudaStream_t s);
+
+}  // namespace cdns

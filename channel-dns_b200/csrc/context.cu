@@ -1,0 +1,632 @@
+// cdns context: device state, step orchestration (stream launches and CUDA
+// graphs) and the extern "C" entry points declared in include/cdns.h.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/cdns.h"
+#include "cdns_kernels.cuh"
+
+using namespace cdns;
+
+namespace {
+thread_local std::string g_error;
+
+int fail(int code, const std::string &msg) {
+    g_error = msg;
+    return code;
+}
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(CDNS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+constexpr int kStages = 6;
+const char *kStageNames[kStages] = {"curl_ysynth", "z_backward", "x_cross",
+                                    "z_forward",   "y_analysis", "solve"};
+constexpr int kMaxProfSteps = 256;
+
+bool plan_fft(int n, FftPlan &p) {
+    p.n = n;
+    p.nrad = 0;
+    int m = n;
+    auto push = [&](int r) {
+        if (p.nrad >= 12) return false;
+        p.radix[p.nrad++] = r;
+        return true;
+    };
+    while (m % 4 == 0) { if (!push(4)) return false; m /= 4; }
+    while (m % 2 == 0) { if (!push(2)) return false; m /= 2; }
+    for (int q = 3; m > 1; q += 2) {
+        while (m % q == 0) {
+            if (q > 13 || !push(q)) return false;
+            m /= q;
+        }
+    }
+    return true;
+}
+}  // namespace
+
+struct cdns_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    Dims d{};
+    Tables t{};
+    FftPlan px{}, pz{};
+    PhysParams pp{};
+    double DT = 0.0;
+    std::vector<void *> allocs;
+    size_t bytes = 0;
+    // state (component planar)
+    double2 *U[2] = {nullptr, nullptr};   // velocity / previous velocity
+    double2 *Nb[2] = {nullptr, nullptr};  // nonlinear term, current / previous
+    double2 *Bb[2] = {nullptr, nullptr};  // pressure wall data, current / previous
+    int cur = 0;                          // U[cur] = u, Nb[cur] = next N, Bb[cur] = next B
+    double2 *p = nullptr, *bw = nullptr, *bc_v = nullptr, *bc_p = nullptr;
+    double2 *F = nullptr, *G = nullptr, *H = nullptr, *aux = nullptr, *aux2 = nullptr, *zero3 = nullptr;
+    double *phys = nullptr;
+    double *dpdx = nullptr;
+    unsigned *err = nullptr;
+    SolverState st{};
+    double g_setup = NAN;
+    bool have_velocity = false;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    bool prof = false;
+    int prof_steps = 0;
+    std::vector<cudaEvent_t> ev;
+
+    template <typename T> int alloc(T *&ptr, size_t count) {
+        void *p = nullptr;
+        const size_t b = sizeof(T) * (count ? count : 1);
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e != cudaSuccess) return fail(CDNS_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        e = cudaMemset(p, 0, b);
+        if (e != cudaSuccess) return fail(CDNS_ERR_CUDA, cudaGetErrorString(e));
+        allocs.push_back(p);
+        bytes += b;
+        ptr = static_cast<T *>(p);
+        return CDNS_OK;
+    }
+};
+
+namespace {
+int upload(cdns_ctx *c, void *dst, const void *src, size_t b) {
+    CK(cudaMemcpyAsync(dst, src, b, cudaMemcpyHostToDevice, c->stream));
+    return CDNS_OK;
+}
+
+void step_coefficients(int it, double dt, double re, double &a0, double &a1, double &b0, double &b1,
+                       double &g) {
+    // src/sim/simulation.cpp:36-45
+    const int eff = it < 3 ? it : 2;
+    a0 = (double)eff / dt;
+    a1 = (double)(1 - eff) / (2.0 * dt);
+    b0 = (double)eff;
+    b1 = (double)(1 - eff);
+    g = (a0 + a1) * re;
+}
+
+// Nonlinear stages K1..K5a: u -> N (planar spectral), bw.
+void enqueue_nonlinear(cdns_ctx *c, const double2 *u, double2 *N, bool prof, int step_slot) {
+    const Dims &d = c->d;
+    cudaStream_t s = c->stream;
+    auto mark = [&](int stage) {
+        if (prof) cudaEventRecord(c->ev[(size_t)step_slot * (kStages + 1) + stage], s);
+    };
+    mark(0);
+    launch_curl_ysynth(d, c->t, u, c->F, c->bw, c->pp.Re, true, s);
+    mark(1);
+    launch_z_backward(d, c->pz, c->t.root_z, c->F, c->G, 6, s);
+    mark(2);
+    launch_x_cross(d, c->px, c->t.root_x, c->G, c->H, s);
+    mark(3);
+    launch_z_forward(d, c->pz, c->t.root_z, c->H, c->F, 3, s);
+    mark(4);
+    launch_y_analysis(d, c->t, c->F, N, 3, s);
+    mark(5);
+}
+
+void enqueue_step_body(cdns_ctx *c, double a0, double a1, double b0, double b1, double g_v,
+                       bool prof, int slot) {
+    const int k = c->cur;
+    enqueue_nonlinear(c, c->U[k], c->Nb[k], prof, slot);
+    StepArgs a{};
+    a.u = c->U[k];
+    a.u_prev = c->U[1 - k];
+    a.N = c->Nb[k];
+    a.N_prev = c->Nb[1 - k];
+    a.bw = c->bw;
+    a.B_prev = c->Bb[1 - k];
+    a.B_new = c->Bb[k];
+    a.bc_v = c->bc_v;
+    a.u_out = c->U[1 - k];
+    a.p_out = c->p;
+    a.dpdx = c->dpdx;
+    a.err = c->err;
+    a.a0 = a0;
+    a.a1 = a1;
+    a.b0 = b0;
+    a.b1 = b1;
+    launch_step_solve(c->d, c->t, c->pp, g_v, c->st, a, c->stream);
+    if (prof) cudaEventRecord(c->ev[(size_t)slot * (kStages + 1) + kStages], c->stream);
+}
+
+int do_setup(cdns_ctx *c, double g_v) {
+    if (c->g_setup == g_v) return CDNS_OK;  // deterministic: same g gives the same state
+    setup_solver(c->d, c->t, c->pp, g_v, c->st, nullptr, c->stream);
+    CK(cudaGetLastError());
+    c->g_setup = g_v;
+    return CDNS_OK;
+}
+
+int one_step(cdns_ctx *c, int it) {
+    if (!c->have_velocity) return fail(CDNS_ERR_STATE, "cdns_step before cdns_set_velocity");
+    if (it < 1) return fail(CDNS_ERR_ARG, "iteration must be >= 1");
+    double a0, a1, b0, b1, g;
+    step_coefficients(it, c->DT, c->pp.Re, a0, a1, b0, b1, g);
+    // EqSolvePV::setup runs at it = 1, 2 (src/sim/simulation.cpp:176-177); later
+    // steps reuse the it = 2 state, whose g equals theirs.  Re-running setup
+    // whenever the stored g differs keeps that invariant after cdns_solve.
+    {
+        int r = do_setup(c, g);
+        if (r) return r;
+    }
+    if (c->prof) {
+        if (c->prof_steps >= kMaxProfSteps) return fail(CDNS_ERR_STATE, "profiling window full");
+        enqueue_step_body(c, a0, a1, b0, b1, g, true, c->prof_steps);
+        c->prof_steps++;
+    } else if (it >= 3) {
+        cudaGraphExec_t &ge = c->graph[c->cur];
+        if (!ge) {
+            cudaGraph_t graph;
+            CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            enqueue_step_body(c, a0, a1, b0, b1, g, false, 0);
+            CK(cudaStreamEndCapture(c->stream, &graph));
+            CK(cudaGraphInstantiate(&ge, graph, 0));
+            CK(cudaGraphDestroy(graph));
+        }
+        CK(cudaGraphLaunch(ge, c->stream));
+    } else {
+        enqueue_step_body(c, a0, a1, b0, b1, g, false, 0);
+    }
+    CK(cudaGetLastError());
+    c->cur = 1 - c->cur;
+    return CDNS_OK;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+}  // namespace
+
+extern "C" {
+
+int cdns_create(const cdns_mesh_desc *m, const cdns_params *p, int precision, int device,
+                cdns_ctx **out) {
+    if (!m || !p || !out) return fail(CDNS_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (precision != CDNS_PRECISION_FP64) return fail(CDNS_ERR_ARG, "unsupported precision mode");
+    if (m->NYS < 4 || m->NXS < 0 || m->NZS < 0 || m->NY2 < m->NYS || m->NY2 < 2 ||
+        m->NX2 < 2 * m->NXS || m->NZ2 < 2 * m->NZS || m->NX2 < 1 || m->NZ2 < 1 ||
+        !(m->XL > 0) || !(m->ZL > 0))
+        return fail(CDNS_ERR_ARG, "invalid mesh: need NYS>=4, NY2>=NYS, NX2>=2 NXS, NZ2>=2 NZS");
+    if (!(p->DT > 0.0) || !(p->Re > 0.0)) return fail(CDNS_ERR_ARG, "DT and Re must be positive");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(CDNS_ERR_CUDA, "no CUDA device available");
+    if (device < 0 || device >= ndev) return fail(CDNS_ERR_ARG, "bad device index");
+    DeviceGuard guard(device);
+    cdns_ctx *c = new (std::nothrow) cdns_ctx();
+    if (!c) return fail(CDNS_ERR_NOMEM, "host allocation failed");
+    c->device = device;
+    Dims &d = c->d;
+    d.NX2 = m->NX2; d.NY2 = m->NY2; d.NZ2 = m->NZ2;
+    d.NXS = m->NXS; d.NYS = m->NYS; d.NZS = m->NZS;
+    d.nkx = m->NXS + 1; d.nkz = 2 * m->NZS + 1; d.ncy = m->NYS + 1; d.ny2 = m->NY2 + 1;
+    d.ncol = d.nkx * d.nkz;
+    d.nyh = m->NY2 / 2 + 1;
+    d.Ns = (long long)d.nkz * d.ncy * d.nkx;
+    if (!plan_fft(d.NX2, c->px) || !plan_fft(d.NZ2, c->pz)) {
+        delete c;
+        return fail(CDNS_ERR_ARG, "NX2/NZ2 must factor into primes <= 13");
+    }
+    const size_t smem_solve = 16 * 6 * (size_t)d.ncy * 8 + 8 * (2 * (size_t)d.ncy * 8 + 3 * d.ncy);
+    if (smem_solve > 220 * 1024 || (size_t)16 * d.NZ2 * 33 > 220 * 1024 ||
+        (size_t)16 * d.NX2 * 25 > 220 * 1024) {
+        delete c;
+        return fail(CDNS_ERR_ARG, "mesh exceeds the shared-memory tiling limits");
+    }
+    // physics parameters (src/core/params.cpp:296-307)
+    PhysParams &pp = c->pp;
+    pp.Re = p->Re; pp.G_pre = p->G_pre; pp.a_pre0 = p->a_pre0; pp.b_pre0 = p->b_pre0;
+    for (int i = 0; i < 3; ++i) { pp.a_V[i] = p->a_V[i]; pp.b_V[i] = p->b_V[i]; }
+    pp.grad_pre = p->INDEX_GRAD_PRE;
+    const double pi = std::acos(-1.0);
+    const double th = p->THETA * pi / 180.0;
+    if (p->INDEX_GRAD_PRE == 1) {
+        pp.gx = -std::cos(th); pp.gz = -std::sin(th); pp.qxm = pp.qzm = 0.0;
+    } else {
+        pp.qxm = std::cos(th); pp.qzm = std::sin(th); pp.gx = pp.gz = 0.0;
+    }
+    c->DT = p->DT;
+    int r = 0;
+    auto bail = [&](int code) { cdns_destroy(c); return code; };
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(CDNS_ERR_CUDA, "stream creation failed"));
+    // ---- tables (src/fft/transforms.cpp:71-108) ----
+    std::vector<double> wavx(d.nkx), wavz(d.nkz), WL(d.ncy, 0.0), WD(d.ncy, 0.0), WR(d.ncy, 0.0),
+        cosy(2 * (size_t)d.NY2);
+    const double alx = 2.0 * pi / m->XL, alz = 2.0 * pi / m->ZL;
+    for (int k = 0; k < d.nkx; ++k) wavx[k] = k * alx;
+    for (int k = -d.NZS; k <= d.NZS; ++k) wavz[k + d.NZS] = k * alz;
+    const int n = d.NYS;
+    for (int iy = n; iy >= 2; --iy) {
+        WL[iy] = 1.0 / (4.0 * iy * (iy - 1));
+        WD[iy] = -1.0 / (2.0 * (iy * iy - 1));
+        WR[iy] = 1.0 / (4.0 * iy * (iy + 1));
+    }
+    WL[2] = 2.0 * WL[2];
+    for (int iy = n - 1; iy <= n; ++iy) WD[iy] = 0.0;
+    for (int iy = n - 3; iy <= n; ++iy) WR[iy] = 0.0;
+    const long double pil = 3.141592653589793238462643383279502884L;
+    for (int mm = 0; mm < 2 * d.NY2; ++mm) {
+        if (2 * mm == d.NY2 || 2 * mm == 3 * d.NY2) cosy[mm] = 0.0;
+        else cosy[mm] = (double)cosl(pil * (long double)mm / (long double)d.NY2);
+    }
+    auto roots = [&](int nn) {
+        std::vector<double2> rr(nn);
+        for (int k = 0; k < nn; ++k) {
+            const long double a = 2.0L * pil * (long double)k / (long double)nn;
+            rr[k] = make_double2((double)cosl(a), (double)(-sinl(a)));
+        }
+        return rr;
+    };
+    const auto rx = roots(d.NX2), rz = roots(d.NZ2);
+    double *tab = nullptr;
+    const size_t ntab = d.nkx + d.nkz + 3 * (size_t)d.ncy + cosy.size() + 2 * (size_t)d.NX2 + 2 * (size_t)d.NZ2;
+    if ((r = c->alloc(tab, ntab))) return bail(r);
+    size_t o = 0;
+    auto put = [&](const void *src, size_t count) {
+        double *dst = tab + o;
+        o += count;
+        return std::make_pair(dst, upload(c, dst, src, count * sizeof(double)));
+    };
+    auto pw = put(wavx.data(), wavx.size()); c->t.wavx = pw.first;
+    auto pz = put(wavz.data(), wavz.size()); c->t.wavz = pz.first;
+    auto pl = put(WL.data(), WL.size()); c->t.WL = pl.first;
+    auto pd = put(WD.data(), WD.size()); c->t.WD = pd.first;
+    auto pr = put(WR.data(), WR.size()); c->t.WR = pr.first;
+    auto pc = put(cosy.data(), cosy.size()); c->t.cosy = pc.first;
+    auto px = put(rx.data(), 2 * rx.size()); c->t.root_x = reinterpret_cast<const double2 *>(px.first);
+    auto pzz = put(rz.data(), 2 * rz.size()); c->t.root_z = reinterpret_cast<const double2 *>(pzz.first);
+    if (pw.second || pz.second || pl.second || pd.second || pr.second || pc.second || px.second || pzz.second)
+        return bail(CDNS_ERR_CUDA);
+    // ---- state and workspaces ----
+    const size_t Ns = (size_t)d.Ns, nc = d.ncol;
+    const size_t fbuf = 6 * (size_t)d.ny2 * nc;
+    const size_t gbuf = 6 * (size_t)d.ny2 * d.NZ2 * d.nkx;
+    const size_t hbuf = 3 * (size_t)d.ny2 * d.NZ2 * d.nkx;
+    if ((r = c->alloc(c->U[0], 3 * Ns)) || (r = c->alloc(c->U[1], 3 * Ns)) ||
+        (r = c->alloc(c->Nb[0], 3 * Ns)) || (r = c->alloc(c->Nb[1], 3 * Ns)) ||
+        (r = c->alloc(c->Bb[0], 2 * nc)) || (r = c->alloc(c->Bb[1], 2 * nc)) ||
+        (r = c->alloc(c->p, Ns)) || (r = c->alloc(c->bw, 2 * nc)) || (r = c->alloc(c->bc_v, 6 * nc)) ||
+        (r = c->alloc(c->bc_p, 2 * nc)) || (r = c->alloc(c->F, fbuf)) || (r = c->alloc(c->G, gbuf)) ||
+        (r = c->alloc(c->H, hbuf)) || (r = c->alloc(c->aux, 3 * Ns)) || (r = c->alloc(c->aux2, 3 * Ns)) ||
+        (r = c->alloc(c->zero3, 3 * Ns)) ||
+        (r = c->alloc(c->phys, (size_t)d.NZ2 * d.ny2 * d.NX2)) || (r = c->alloc(c->dpdx, 2)) ||
+        (r = c->alloc(c->err, 1)))
+        return bail(r);
+    SolverState &st = c->st;
+    if ((r = c->alloc(st.wn_p, nc)) || (r = c->alloc(st.wn_v, nc)) || (r = c->alloc(st.ad_p, Ns)) ||
+        (r = c->alloc(st.ad_v, Ns)) || (r = c->alloc(st.p_inf, 2 * Ns)) || (r = c->alloc(st.v_inf, 6 * Ns)) ||
+        (r = c->alloc(st.inf_div, 4 * nc)) || (r = c->alloc(st.p_b, Ns)) || (r = c->alloc(st.v_b, 3 * Ns)) ||
+        (r = c->alloc(st.sigma0, 2 * nc)) || (r = c->alloc(st.unit, 2 * (size_t)d.ncy + 2)))
+        return bail(r);
+    cudaError_t e = configure_transform_kernels(d);
+    if (e == cudaSuccess) e = configure_solver_kernels(d);
+    if (e != cudaSuccess) return bail(fail(CDNS_ERR_CUDA, cudaGetErrorString(e)));
+    // velocity_boundary (src/sim/initial_bc.cpp:95-101): v = V_Microblow0 on the zero mode
+    std::vector<double2> bc(6 * nc, make_double2(0, 0));
+    const int zc = d.NZS * d.nkx;
+    bc[(2 * 1 + 0) * nc + zc] = make_double2(p->V_Microblow0, 0.0);
+    bc[(2 * 1 + 1) * nc + zc] = make_double2(p->V_Microblow0, 0.0);
+    if ((r = upload(c, c->bc_v, bc.data(), bc.size() * sizeof(double2)))) return bail(r);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(fail(CDNS_ERR_CUDA, "sync"));
+    *out = c;
+    return CDNS_OK;
+}
+
+int cdns_destroy(cdns_ctx *c) {
+    if (!c) return CDNS_OK;
+    DeviceGuard guard(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto &g : c->graph)
+        if (g) cudaGraphExecDestroy(g);
+    for (auto ev : c->ev) cudaEventDestroy(ev);
+    for (void *p : c->allocs) cudaFree(p);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return CDNS_OK;
+}
+
+int cdns_set_velocity_device(cdns_ctx *c, const double *v) {
+    if (!c || !v) return fail(CDNS_ERR_ARG, "null argument");
+    DeviceGuard guard(c->device);
+    const Dims &d = c->d;
+    c->cur = 0;
+    launch_deinterleave(reinterpret_cast<const double2 *>(v), c->U[0], d.Ns, 3, c->stream);
+    CK(cudaMemsetAsync(c->U[1], 0, sizeof(double2) * 3 * d.Ns, c->stream));
+    CK(cudaMemsetAsync(c->Nb[0], 0, sizeof(double2) * 3 * d.Ns, c->stream));
+    CK(cudaMemsetAsync(c->Nb[1], 0, sizeof(double2) * 3 * d.Ns, c->stream));
+    CK(cudaMemsetAsync(c->Bb[0], 0, sizeof(double2) * 2 * d.ncol, c->stream));
+    CK(cudaMemsetAsync(c->Bb[1], 0, sizeof(double2) * 2 * d.ncol, c->stream));
+    CK(cudaGetLastError());
+    c->have_velocity = true;
+    return CDNS_OK;
+}
+
+int cdns_set_velocity(cdns_ctx *c, const double *v) {
+    if (!c || !v) return fail(CDNS_ERR_ARG, "null argument");
+    DeviceGuard guard(c->device);
+    CK(cudaMemcpyAsync(c->aux, v, sizeof(double2) * 3 * c->d.Ns, cudaMemcpyHostToDevice, c->stream));
+    int r = cdns_set_velocity_device(c, reinterpret_cast<const double *>(c->aux));
+    if (r) return r;
+    CK(cudaStreamSynchronize(c->stream));
+    return CDNS_OK;
+}
+
+int cdns_get_velocity_device(cdns_ctx *c, double *v) {
+    if (!c || !v) return fail(CDNS_ERR_ARG, "null argument");
+    if (!c->have_velocity) return fail(CDNS_ERR_STATE, "no velocity set");
+    DeviceGuard guard(c->device);
+    launch_interleave(c->U[c->cur], reinterpret_cast<double2 *>(v), c->d.Ns, 3, c->stream);
+    CK(cudaGetLastError());
+    return CDNS_OK;
+}
+
+int cdns_get_velocity(cdns_ctx *c, double *v) {
+    if (!c || !v) return fail(CDNS_ERR_ARG, "null argument");
+    int r = cdns_get_velocity_device(c, reinterpret_cast<double *>(c->aux2));
+    if (r) return r;
+    DeviceGuard guard(c->device);
+    CK(cudaMemcpyAsync(v, c->aux2, sizeof(double2) * 3 * c->d.Ns, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return CDNS_OK;
+}
+
+int cdns_get_pressure(cdns_ctx *c, double *p) {
+    if (!c || !p) return fail(CDNS_ERR_ARG, "null argument");
+    DeviceGuard guard(c->device);
+    CK(cudaMemcpyAsync(p, c->p, sizeof(double2) * c->d.Ns, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return CDNS_OK;
+}
+
+int cdns_set_velocity_bc(cdns_ctx *c, const double *bc) {
+    if (!c || !bc) return fail(CDNS_ERR_ARG, "null argument");
+    DeviceGuard guard(c->device);
+    const Dims &d = c->d;
+    const size_t nc = d.ncol;
+    std::vector<double2> v(6 * nc);
+    const double2 *src = reinterpret_cast<const double2 *>(bc);
+    for (int kz = 0; kz < d.nkz; ++kz)
+        for (int w = 0; w < 2; ++w)
+            for (int kx = 0; kx < d.nkx; ++kx)
+                for (int comp = 0; comp < 3; ++comp)
+                    v[(2 * comp + w) * nc + (size_t)kz * d.nkx + kx] =
+                        src[(((size_t)kz * 2 + w) * d.nkx + kx) * 3 + comp];
+    CK(cudaMemcpyAsync(c->bc_v, v.data(), v.size() * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return CDNS_OK;
+}
+
+int cdns_step(cdns_ctx *c, int iteration) {
+    if (!c) return fail(CDNS_ERR_ARG, "null context");
+    DeviceGuard guard(c->device);
+    return one_step(c, iteration);
+}
+
+int cdns_run(cdns_ctx *c, int first, int nsteps) {
+    if (!c) return fail(CDNS_ERR_ARG, "null context");
+    if (nsteps < 0) return fail(CDNS_ERR_ARG, "negative step count");
+    DeviceGuard guard(c->device);
+    for (int i = 0; i < nsteps; ++i) {
+        int r = one_step(c, first + i);
+        if (r) return r;
+    }
+    return CDNS_OK;
+}
+
+int cdns_synchronize(cdns_ctx *c) {
+    if (!c) return fail(CDNS_ERR_ARG, "null context");
+    DeviceGuard guard(c->device);
+    CK(cudaStreamSynchronize(c->stream));
+    unsigned e = 0;
+    CK(cudaMemcpy(&e, c->err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (e) {
+        CK(cudaMemset(c->err, 0, sizeof(unsigned)));
+        if (e & ERR_NONFINITE) return fail(CDNS_ERR_NONFINITE, "non-finite value in the step output");
+        return fail(CDNS_ERR_PIVOT, "zero or non-finite tau pivot or flow response");
+    }
+    return CDNS_OK;
+}
+
+int cdns_get_dpdx(cdns_ctx *c, double out[2]) {
+    if (!c || !out) return fail(CDNS_ERR_ARG, "null argument");
+    DeviceGuard guard(c->device);
+    CK(cudaMemcpyAsync(out, c->dpdx, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return CDNS_OK;
+}
+
+int cdns_nonlinear(cdns_ctx *c, const double *velocity, double *nl, double *pbc) {
+    if (!c || !velocity || !nl) return fail(CDNS_ERR_ARG, "null argument");
+    DeviceGuard guard(c->device);
+    const Dims &d = c->d;
+    CK(cudaMemcpyAsync(c->aux2, velocity, sizeof(double2) * 3 * d.Ns, cudaMemcpyHostToDevice, c->stream));
+    launch_deinterleave(c->aux2, c->aux, d.Ns, 3, c->stream);
+    enqueue_nonlinear(c, c->aux, c->aux2, false, 0);
+    launch_pressure_bc(d, c->aux2, c->bw, c->bc_p, c->stream);
+    launch_interleave(c->aux2, c->aux, d.Ns, 3, c->stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(nl, c->aux, sizeof(double2) * 3 * d.Ns, cudaMemcpyDeviceToHost, c->stream));
+    std::vector<double2> b(2 * (size_t)d.ncol);
+    CK(cudaMemcpyAsync(b.data(), c->bc_p, b.size() * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (pbc) {
+        double2 *o = reinterpret_cast<double2 *>(pbc);
+        for (int kz = 0; kz < d.nkz; ++kz)
+            for (int w = 0; w < 2; ++w)
+                for (int kx = 0; kx < d.nkx; ++kx)
+                    o[((size_t)kz * 2 + w) * d.nkx + kx] = b[(size_t)w * d.ncol + (size_t)kz * d.nkx + kx];
+    }
+    return CDNS_OK;
+}
+
+int cdns_transform_fine(cdns_ctx *c, int dir, const double *in, double *out) {
+    if (!c || !in || !out) return fail(CDNS_ERR_ARG, "null argument");
+    DeviceGuard guard(c->device);
+    const Dims &d = c->d;
+    const size_t nphys = (size_t)d.NZ2 * d.ny2 * d.NX2;
+    if (dir == 'B') {
+        CK(cudaMemcpyAsync(c->aux, in, sizeof(double2) * d.Ns, cudaMemcpyHostToDevice, c->stream));
+        launch_curl_ysynth(d, c->t, c->aux, c->F, c->bw, c->pp.Re, false, c->stream);
+        launch_z_backward(d, c->pz, c->t.root_z, c->F, c->G, 1, c->stream);
+        launch_x_c2r(d, c->px, c->t.root_x, c->G, c->phys, c->stream);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(out, c->phys, sizeof(double) * nphys, cudaMemcpyDeviceToHost, c->stream));
+    } else if (dir == 'F') {
+        CK(cudaMemcpyAsync(c->phys, in, sizeof(double) * nphys, cudaMemcpyHostToDevice, c->stream));
+        launch_x_r2c(d, c->px, c->t.root_x, c->phys, c->H, c->stream);
+        launch_z_forward(d, c->pz, c->t.root_z, c->H, c->F, 1, c->stream);
+        launch_y_analysis(d, c->t, c->F, c->aux, 1, c->stream);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(out, c->aux, sizeof(double2) * d.Ns, cudaMemcpyDeviceToHost, c->stream));
+    } else {
+        return fail(CDNS_ERR_ARG, "direction must be 'B' or 'F'");
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return CDNS_OK;
+}
+
+int cdns_solve(cdns_ctx *c, double g, const double *rhs, const double *pbc, const double *vbc,
+               double *pressure, double *velocity, double *units) {
+    if (!c || !rhs || !pbc || !vbc || !pressure || !velocity) return fail(CDNS_ERR_ARG, "null argument");
+    DeviceGuard guard(c->device);
+    const Dims &d = c->d;
+    const size_t nc = d.ncol;
+    int r = do_setup(c, g);
+    if (r) return r;
+    // velocity BC and pressure BC into solver layouts
+    std::vector<double2> bv(6 * nc), bp(2 * nc);
+    const double2 *sv = reinterpret_cast<const double2 *>(vbc);
+    const double2 *sp = reinterpret_cast<const double2 *>(pbc);
+    for (int kz = 0; kz < d.nkz; ++kz)
+        for (int w = 0; w < 2; ++w)
+            for (int kx = 0; kx < d.nkx; ++kx) {
+                const size_t col = (size_t)kz * d.nkx + kx;
+                bp[w * nc + col] = sp[((size_t)kz * 2 + w) * d.nkx + kx];
+                for (int comp = 0; comp < 3; ++comp)
+                    bv[(2 * comp + w) * nc + col] = sv[(((size_t)kz * 2 + w) * d.nkx + kx) * 3 + comp];
+            }
+    double2 *dbv = c->G, *dbp = c->G + 6 * nc;
+    CK(cudaMemcpyAsync(dbv, bv.data(), bv.size() * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(dbp, bp.data(), bp.size() * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->aux2, rhs, sizeof(double2) * 3 * d.Ns, cudaMemcpyHostToDevice, c->stream));
+    launch_deinterleave(c->aux2, c->aux, d.Ns, 3, c->stream);
+    const double2 *zero = c->zero3;  // zeros for the unused history terms
+    StepArgs a{};
+    a.u = c->aux;
+    a.u_prev = zero;
+    a.N = zero;
+    a.N_prev = zero;
+    a.bw = c->bw;
+    a.B_prev = c->bc_p;
+    a.B_new = c->bc_p;
+    a.bc_v = dbv;
+    a.bc_p = dbp;
+    a.u_out = c->aux2;
+    a.p_out = c->F;
+    a.dpdx = c->dpdx;
+    a.err = c->err;
+    a.a0 = 1.0;
+    a.solve_only = 1;
+    launch_step_solve(d, c->t, c->pp, g, c->st, a, c->stream);
+    launch_interleave(c->aux2, c->aux, d.Ns, 3, c->stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(velocity, c->aux, sizeof(double2) * 3 * d.Ns, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(pressure, c->F, sizeof(double2) * d.Ns, cudaMemcpyDeviceToHost, c->stream));
+    if (units) CK(cudaMemcpyAsync(units, c->st.unit, sizeof(double) * 2 * d.ncy, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return CDNS_OK;
+}
+
+int cdns_profile_begin(cdns_ctx *c) {
+    if (!c) return fail(CDNS_ERR_ARG, "null context");
+    DeviceGuard guard(c->device);
+    if (c->ev.empty()) {
+        c->ev.resize((size_t)kMaxProfSteps * (kStages + 1));
+        for (auto &e : c->ev) CK(cudaEventCreate(&e));
+    }
+    c->prof = true;
+    c->prof_steps = 0;
+    return CDNS_OK;
+}
+
+int cdns_profile_end(cdns_ctx *c, double *stage_ms, int *nsteps) {
+    if (!c || !stage_ms) return fail(CDNS_ERR_ARG, "null argument");
+    DeviceGuard guard(c->device);
+    CK(cudaStreamSynchronize(c->stream));
+    for (int s = 0; s < kStages; ++s) stage_ms[s] = 0.0;
+    for (int i = 0; i < c->prof_steps; ++i)
+        for (int s = 0; s < kStages; ++s) {
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, c->ev[(size_t)i * (kStages + 1) + s],
+                                    c->ev[(size_t)i * (kStages + 1) + s + 1]));
+            stage_ms[s] += ms;
+        }
+    if (nsteps) *nsteps = c->prof_steps;
+    c->prof = false;
+    c->prof_steps = 0;
+    return CDNS_OK;
+}
+
+int cdns_stage_count(void) { return kStages; }
+const char *cdns_stage_name(int s) { return (s >= 0 && s < kStages) ? kStageNames[s] : ""; }
+
+int cdns_get_stream(cdns_ctx *c, void **stream) {
+    if (!c || !stream) return fail(CDNS_ERR_ARG, "null argument");
+    *stream = (void *)c->stream;
+    return CDNS_OK;
+}
+
+int cdns_device_bytes(cdns_ctx *c, size_t *b) {
+    if (!c || !b) return fail(CDNS_ERR_ARG, "null argument");
+    *b = c->bytes;
+    return CDNS_OK;
+}
+
+int cdns_last_error(char *buf, size_t len) {
+    if (!buf || !len) return CDNS_ERR_ARG;
+    std::snprintf(buf, len, "%s", g_error.c_str());
+    return CDNS_OK;
+}
+
+const char *cdns_version(void) { return "cdns-b200 0.1 (sm_100a, fp64)"; }
+
+}  // extern "C"

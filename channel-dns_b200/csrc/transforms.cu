@@ -1,0 +1,534 @@
+// Fine-grid (3/2 product grid) transforms of the channel-dns nonlinear term,
+// written for sm_100a.  Stage layout in HBM (complex<double>):
+//
+//   spectral   S[c][kz][y][kx]          (c = component, Ns per component)
+//   Ypys       F[f][j][kz][kx]          after the Chebyshev synthesis (j = GL point)
+//   Zphys      G[f][j][z][kx]           after the inverse z FFT
+//   Xspec      H[f][j][z][kx]           products after the forward x FFT
+//   Zspec      F[f][j][kz][kx]          after the forward z FFT
+//
+// Reference semantics (src/fft/transforms.cpp:615-741): the synthesis is the
+// unnormalised DCT-I of the zero-padded column with c_0 doubled, followed by
+// the 0.5 z-expansion factor; both factors are powers of two, so they are
+// folded into f_j = sum_k w_k c_k cos(pi j k / NY2) (w_k = 1, or 1/2 for
+// k = NY2).  The analysis keeps x1/NX2 before the z FFT, x1/NZ2 after it, and
+// DCT-I scaling 1/(2 NY2) at k=0, 1/NY2 otherwise.
+#include "cdns_kernels.cuh"
+#include "fft_lines.cuh"
+
+namespace cdns {
+
+// ---------------------------------------------------------------------------
+// K1: curl + Chebyshev synthesis, one thread per (spectral column, JT point
+// pairs).  The even/odd split f_j = E_j + O_j, f_{NY2-j} = E_j - O_j halves
+// the multiply-adds.  The curl's y-derivative recurrence
+// (src/solver/vector_ops.cpp:17-25, :112-151) runs along the descending
+// coefficient loop in registers.  Row group 0 also accumulates the vorticity
+// part of the pressure wall condition (src/solver/timestepper.cpp:26-43).
+// ---------------------------------------------------------------------------
+template <int JT, bool CURL>
+__global__ void __launch_bounds__(128)
+k_curl_ysynth(Dims d, Tables t, const double2 *__restrict__ u, double2 *__restrict__ F,
+              double2 *__restrict__ bw, double inv_re_unused, double re) {
+    constexpr int NF = CURL ? 6 : 1;
+    extern __shared__ double s_cos[];
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int twoN = 2 * d.NY2;
+    for (int i = tid; i < twoN; i += blockDim.x * blockDim.y) s_cos[i] = t.cosy[i];
+    __syncthreads();
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    const int g = blockIdx.y * blockDim.y + threadIdx.y;
+    const int j0 = g * JT;
+    if (col >= d.ncol || j0 >= d.nyh) return;
+    const int kzi = col / d.nkx;
+    const int kx = col - kzi * d.nkx;
+    const double ax = t.wavx[kx], az = t.wavz[kzi];
+    const double2 *U = u + (long long)kzi * d.ncy * d.nkx + kx;
+    const double2 *V = U + d.Ns;
+    const double2 *W = V + d.Ns;
+    const int nys = d.NYS;
+    int idx[JT];
+#pragma unroll
+    for (int q = 0; q < JT; ++q) idx[q] = ((j0 + q) * nys) % twoN;
+    double2 accE[JT][NF], accO[JT][NF];
+#pragma unroll
+    for (int q = 0; q < JT; ++q)
+#pragma unroll
+        for (int f = 0; f < NF; ++f) accE[q][f] = accO[q][f] = mk(0.0, 0.0);
+    double2 u1 = mk(0, 0), w1 = mk(0, 0), du1 = mk(0, 0), du2 = mk(0, 0), dw1 = mk(0, 0),
+            dw2 = mk(0, 0);
+    double2 btop = mk(0, 0), bbot = mk(0, 0);
+    const bool wall_sums = CURL && g == 0;
+    const double axr = ax / re, azr = az / re;
+    for (int k = nys; k >= 0; --k) {
+        double2 fld[NF];
+        const double2 uk = U[(long long)k * d.nkx];
+        if (CURL) {
+            const double2 vk = V[(long long)k * d.nkx];
+            const double2 wk = W[(long long)k * d.nkx];
+            double2 duk, dwk;
+            if (k == nys) {
+                duk = mk(0, 0);
+                dwk = mk(0, 0);
+            } else {
+                const double s = (double)(2 * (k + 1));
+                duk = cadd(du2, cscale(s, u1));
+                dwk = cadd(dw2, cscale(s, w1));
+            }
+            if (k == 0) {
+                duk = cscale(0.5, duk);
+                dwk = cscale(0.5, dwk);
+            }
+            du2 = du1; du1 = duk; u1 = uk;
+            dw2 = dw1; dw1 = dwk; w1 = wk;
+            const double2 ox = csub(dwk, fderiv(az, vk));
+            const double2 oy = csub(fderiv(az, uk), fderiv(ax, wk));
+            const double2 oz = csub(fderiv(ax, vk), duk);
+            fld[0] = uk;
+            if (NF == 6) {
+                fld[1] = vk; fld[2] = wk; fld[3] = ox; fld[4] = oy; fld[5] = oz;
+            }
+            if (wall_sums) {
+                const double2 wall = csub(fderiv(axr, oz), fderiv(azr, ox));
+                btop = cadd(btop, wall);
+                bbot = (k & 1) ? cadd(bbot, wall) : csub(bbot, wall);
+            }
+        } else {
+            fld[0] = uk;
+        }
+        const double wgt = (k == d.NY2) ? 0.5 : 1.0;
+        if (k & 1) {
+#pragma unroll
+            for (int q = 0; q < JT; ++q) {
+                const double c = s_cos[idx[q]] * wgt;
+#pragma unroll
+                for (int f = 0; f < NF; ++f) {
+                    accO[q][f].x += c * fld[f].x;
+                    accO[q][f].y += c * fld[f].y;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < JT; ++q) {
+                const double c = s_cos[idx[q]] * wgt;
+#pragma unroll
+                for (int f = 0; f < NF; ++f) {
+                    accE[q][f].x += c * fld[f].x;
+                    accE[q][f].y += c * fld[f].y;
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < JT; ++q) {
+            idx[q] -= j0 + q;
+            if (idx[q] < 0) idx[q] += twoN;
+        }
+    }
+    if (wall_sums) {
+        bw[col] = btop;
+        bw[d.ncol + col] = bbot;
+    }
+    const long long plane = (long long)d.ncol;
+#pragma unroll
+    for (int q = 0; q < JT; ++q) {
+        const int j = j0 + q;
+        if (j >= d.nyh) break;
+        const int jm = d.NY2 - j;
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+            double2 *Ff = F + (long long)f * d.ny2 * plane;
+            Ff[(long long)j * plane + col] = cadd(accE[q][f], accO[q][f]);
+            if (jm != j) Ff[(long long)jm * plane + col] = csub(accE[q][f], accO[q][f]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// K2: inverse z FFT.  Block = one (field, y point) plane x TL kx lines.  The
+// kz in [-NZS, NZS] coefficients are expanded into the NZ2 slots (negative
+// Nyquist slot wins at a full z spectrum, src/fft/transforms.cpp:715-732).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128)
+k_z_backward(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 *__restrict__ F,
+             double2 *__restrict__ G, int TL) {
+    extern __shared__ double2 sm[];
+    const int n = d.NZ2;
+    double2 *s_root = sm;
+    double2 *a = sm + n;
+    double2 *b = a + n * TL;
+    const int f = blockIdx.z, j = blockIdx.y, kx0 = blockIdx.x * TL;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s_root[i] = roots[i];
+    const double2 *Fp = F + ((long long)f * d.ny2 + j) * d.ncol;
+    for (int i = threadIdx.x; i < n * TL; i += blockDim.x) {
+        const int z = i / TL, line = i - (i / TL) * TL;
+        const int kx = kx0 + line;
+        int kz;
+        bool keep;
+        if (z <= d.NZS) {
+            kz = z;
+            keep = true;
+            if (z == n - d.NZS) kz = -d.NZS;  // full z spectrum: negative Nyquist wins
+        } else if (z >= n - d.NZS) {
+            kz = z - n;
+            keep = true;
+        } else {
+            kz = 0;
+            keep = false;
+        }
+        double2 v = mk(0, 0);
+        if (keep && kx < d.nkx) v = Fp[(kz + d.NZS) * d.nkx + kx];
+        a[i] = v;
+    }
+    __syncthreads();
+    const double2 *res = fft_lines<+1>(a, b, TL, P, s_root);
+    double2 *Gp = G + ((long long)f * d.ny2 + j) * (long long)n * d.nkx;
+    for (int i = threadIdx.x; i < n * TL; i += blockDim.x) {
+        const int z = i / TL, line = i - (i / TL) * TL;
+        const int kx = kx0 + line;
+        if (kx < d.nkx) Gp[(long long)z * d.nkx + kx] = res[i];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// K3: inverse x FFT of the six fields, u x omega, forward x FFT of the three
+// products.  Block = RW rows (z, j); real rows are packed in pairs into one
+// complex line (a + i b); c2r drops the imaginary parts of the DC and Nyquist
+// bins as FFTW does.  Products: N = u x omega (src/solver/vector_ops.cpp:263-269),
+// packed as (N0 + i N1) and (N2 of row r + i N2 of row r+1).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+k_x_cross(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 *__restrict__ G,
+          double2 *__restrict__ H, int RW) {
+    extern __shared__ double2 sm[];
+    const int n = d.NX2;
+    double2 *s_root = sm;
+    const int L = 3 * RW;
+    double2 *a = sm + n;
+    double2 *b = a + n * L;
+    const int j = blockIdx.y, z0 = blockIdx.x * RW;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s_root[i] = roots[i];
+    const long long fstride = (long long)d.ny2 * d.NZ2 * d.nkx;
+    const double2 *Gj = G + (long long)j * d.NZ2 * d.nkx;
+    const int nyq = (n % 2 == 0) ? n / 2 : -1;
+    for (int i = threadIdx.x; i < n * L; i += blockDim.x) {
+        const int k = i / L, line = i - (i / L) * L;
+        const int r = line / 3, p = line - (line / 3) * 3;
+        const int z = z0 + r;
+        double2 v = mk(0, 0);
+        if (z < d.NZ2) {
+            int m;
+            bool mirror;
+            if (k <= d.NXS) { m = k; mirror = false; }
+            else if (k >= n - d.NXS && k != nyq) { m = n - k; mirror = true; }
+            else { m = -1; mirror = false; }
+            if (m >= 0) {
+                const double2 *row = Gj + (long long)z * d.nkx + m;
+                double2 A = row[(2 * p) * fstride];
+                double2 B = row[(2 * p + 1) * fstride];
+                if (m == 0 || m == nyq) { A.y = 0.0; B.y = 0.0; }
+                v = mirror ? mk(A.x + B.y, B.x - A.y) : mk(A.x - B.y, A.y + B.x);
+            }
+        }
+        a[i] = v;
+    }
+    __syncthreads();
+    double2 *res = fft_lines<+1>(a, b, L, P, s_root);
+    double2 *oth = (res == a) ? b : a;
+    // products, packed into 3 lines per pair of rows: (N0+iN1)_r, (N0+iN1)_{r+1}, (N2_r + i N2_{r+1})
+    const int L2 = 3 * ((RW + 1) / 2);
+    for (int i = threadIdx.x; i < n * RW; i += blockDim.x) {
+        const int x = i / RW, r = i - (i / RW) * RW;
+        const double2 p0 = res[x * L + 3 * r];
+        const double2 p1 = res[x * L + 3 * r + 1];
+        const double2 p2 = res[x * L + 3 * r + 2];
+        const double uu = p0.x, vv = p0.y, ww = p1.x, ox = p1.y, oy = p2.x, oz = p2.y;
+        const double n0 = vv * oz - ww * oy;
+        const double n1 = ww * ox - uu * oz;
+        const double n2 = uu * oy - vv * ox;
+        const int pr = r >> 1, odd = r & 1;
+        oth[x * L2 + 3 * pr + odd] = mk(n0, n1);
+        if (odd) oth[x * L2 + 3 * pr + 2].y = n2;
+        else oth[x * L2 + 3 * pr + 2].x = n2;
+    }
+    if (RW & 1) {  // odd row count: the last N2 line has no partner
+        for (int x = threadIdx.x; x < n; x += blockDim.x) {
+            oth[x * L2 + 3 * (RW / 2) + 1] = mk(0, 0);
+            oth[x * L2 + 3 * (RW / 2) + 2].y = 0.0;
+        }
+    }
+    __syncthreads();
+    double2 *res2 = fft_lines<-1>(oth, res, L2, P, s_root);
+    const double invn = 1.0 / (double)n;
+    for (int i = threadIdx.x; i < d.nkx * RW * 3; i += blockDim.x) {
+        const int k = i / (RW * 3);
+        const int rem = i - k * (RW * 3);
+        const int r = rem / 3, f = rem - (rem / 3) * 3;
+        const int z = z0 + r;
+        if (z >= d.NZ2) continue;
+        const int km = (n - k) % n;
+        const int pr = r >> 1, odd = r & 1;
+        const int line = (f < 2) ? 3 * pr + odd : 3 * pr + 2;
+        const double2 P0 = res2[k * L2 + line];
+        const double2 Pm = res2[km * L2 + line];
+        double2 out;
+        // unpack: A = (P + conj Pm)/2, B = (P - conj Pm)/(2i)
+        const bool takeA = (f == 0) || (f == 2 && !odd);
+        if (takeA) out = mk(0.5 * (P0.x + Pm.x), 0.5 * (P0.y - Pm.y));
+        else out = mk(0.5 * (P0.y + Pm.y), -0.5 * (P0.x - Pm.x));
+        H[(long long)f * fstride + ((long long)j * d.NZ2 + z) * d.nkx + k] = cscale(invn, out);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// K4: forward z FFT, keep |kz| <= NZS, x1/NZ2 (src/fft/transforms.cpp:658-665).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128)
+k_z_forward(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 *__restrict__ H,
+            double2 *__restrict__ F, int TL) {
+    extern __shared__ double2 sm[];
+    const int n = d.NZ2;
+    double2 *s_root = sm;
+    double2 *a = sm + n;
+    double2 *b = a + n * TL;
+    const int f = blockIdx.z, j = blockIdx.y, kx0 = blockIdx.x * TL;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s_root[i] = roots[i];
+    const double2 *Hp = H + ((long long)f * d.ny2 + j) * (long long)n * d.nkx;
+    for (int i = threadIdx.x; i < n * TL; i += blockDim.x) {
+        const int z = i / TL, line = i - (i / TL) * TL;
+        const int kx = kx0 + line;
+        a[i] = kx < d.nkx ? Hp[(long long)z * d.nkx + kx] : mk(0, 0);
+    }
+    __syncthreads();
+    const double2 *res = fft_lines<-1>(a, b, TL, P, s_root);
+    const double invn = 1.0 / (double)n;
+    double2 *Fp = F + ((long long)f * d.ny2 + j) * d.ncol;
+    for (int i = threadIdx.x; i < d.nkz * TL; i += blockDim.x) {
+        const int kzi = i / TL, line = i - (i / TL) * TL;
+        const int kx = kx0 + line;
+        if (kx >= d.nkx) continue;
+        const int kz = kzi - d.NZS;
+        const int slot = kz >= 0 ? kz : n + kz;
+        Fp[kzi * d.nkx + kx] = cscale(invn, res[slot * TL + line]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// K5a: Chebyshev analysis (DCT-I) of the products, keep k <= NYS.  One thread
+// per (spectral column, KT coefficients); symmetric pairs e_j = x_j + x_{N-j},
+// o_j = x_j - x_{N-j} feed the even / odd coefficients.
+// ---------------------------------------------------------------------------
+template <int KT>
+__global__ void __launch_bounds__(128)
+k_y_analysis(Dims d, Tables t, const double2 *__restrict__ F, double2 *__restrict__ S, int nf) {
+    extern __shared__ double s_cos[];
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int N = d.NY2, twoN = 2 * N;
+    for (int i = tid; i < twoN; i += blockDim.x * blockDim.y) s_cos[i] = t.cosy[i];
+    __syncthreads();
+    const int fc = blockIdx.x * blockDim.x + threadIdx.x;
+    const int g = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k0 = g * KT;
+    if (fc >= nf * d.ncol || k0 > d.NYS) return;
+    const int f = fc / d.ncol, col = fc - (fc / d.ncol) * d.ncol;
+    const double2 *X = F + (long long)f * d.ny2 * d.ncol + col;
+    double2 acc[KT];
+    int idx[KT];
+#pragma unroll
+    for (int q = 0; q < KT; ++q) { acc[q] = mk(0, 0); idx[q] = 0; }
+    for (int j = 0; j < d.nyh; ++j) {
+        const double2 xa = X[(long long)j * d.ncol];
+        double2 e, o;
+        if (N - j == j) {
+            e = xa;
+            o = mk(0, 0);
+        } else {
+            const double2 xb = X[(long long)(N - j) * d.ncol];
+            e = cadd(xa, xb);
+            o = csub(xa, xb);
+        }
+        const double wgt = (j == 0) ? 1.0 : 2.0;
+#pragma unroll
+        for (int q = 0; q < KT; ++q) {
+            const int k = k0 + q;
+            const double c = s_cos[idx[q]] * wgt;
+            const double2 src = (k & 1) ? o : e;
+            acc[q].x += c * src.x;
+            acc[q].y += c * src.y;
+            idx[q] += k;
+            if (idx[q] >= twoN) idx[q] -= twoN;
+        }
+    }
+    const int kzi = col / d.nkx, kx = col - (col / d.nkx) * d.nkx;
+    double2 *Sf = S + (long long)f * d.Ns + (long long)kzi * d.ncy * d.nkx + kx;
+#pragma unroll
+    for (int q = 0; q < KT; ++q) {
+        const int k = k0 + q;
+        if (k > d.NYS) break;
+        const double s = (k == 0) ? 1.0 / (2.0 * N) : 1.0 / (double)N;
+        Sf[(long long)k * d.nkx] = cscale(s, acc[q]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Single-field x transforms for the standalone fine transform (tests and
+// to-physical output): c2r / r2c of one real field [z][j][x].
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128)
+k_x_c2r(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 *__restrict__ G,
+        double *__restrict__ phys, int RW) {
+    extern __shared__ double2 sm[];
+    const int n = d.NX2;
+    double2 *s_root = sm;
+    const int L = (RW + 1) / 2;  // two real rows per complex line
+    double2 *a = sm + n;
+    double2 *b = a + n * L;
+    const int j = blockIdx.y, z0 = blockIdx.x * RW;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s_root[i] = roots[i];
+    const int nyq = (n % 2 == 0) ? n / 2 : -1;
+    for (int i = threadIdx.x; i < n * L; i += blockDim.x) {
+        const int k = i / L, line = i - (i / L) * L;
+        double2 A = mk(0, 0), B = mk(0, 0);
+        int m;
+        bool mirror;
+        if (k <= d.NXS) { m = k; mirror = false; }
+        else if (k >= n - d.NXS && k != nyq) { m = n - k; mirror = true; }
+        else { m = -1; mirror = false; }
+        if (m >= 0) {
+            const int za = z0 + 2 * line, zb = za + 1;
+            if (za < d.NZ2 && za < z0 + RW) A = G[((long long)j * d.NZ2 + za) * d.nkx + m];
+            if (zb < d.NZ2 && zb < z0 + RW) B = G[((long long)j * d.NZ2 + zb) * d.nkx + m];
+            if (m == 0 || m == nyq) { A.y = 0.0; B.y = 0.0; }
+        }
+        a[i] = mirror ? mk(A.x + B.y, B.x - A.y) : mk(A.x - B.y, A.y + B.x);
+    }
+    __syncthreads();
+    const double2 *res = fft_lines<+1>(a, b, L, P, s_root);
+    for (int i = threadIdx.x; i < n * RW; i += blockDim.x) {
+        const int x = i / RW, r = i - (i / RW) * RW;
+        const int z = z0 + r;
+        if (z >= d.NZ2) continue;
+        const double2 v = res[x * L + (r >> 1)];
+        phys[((long long)z * d.ny2 + j) * n + x] = (r & 1) ? v.y : v.x;
+    }
+}
+
+__global__ void __launch_bounds__(128)
+k_x_r2c(Dims d, FftPlan P, const double2 *__restrict__ roots, const double *__restrict__ phys,
+        double2 *__restrict__ H, int RW) {
+    extern __shared__ double2 sm[];
+    const int n = d.NX2;
+    double2 *s_root = sm;
+    const int L = (RW + 1) / 2;
+    double2 *a = sm + n;
+    double2 *b = a + n * L;
+    const int j = blockIdx.y, z0 = blockIdx.x * RW;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s_root[i] = roots[i];
+    for (int i = threadIdx.x; i < n * L; i += blockDim.x) {
+        const int x = i / L, line = i - (i / L) * L;
+        const int za = z0 + 2 * line, zb = za + 1;
+        double va = 0, vb = 0;
+        if (za < d.NZ2 && za < z0 + RW) va = phys[((long long)za * d.ny2 + j) * n + x];
+        if (zb < d.NZ2 && zb < z0 + RW) vb = phys[((long long)zb * d.ny2 + j) * n + x];
+        a[i] = mk(va, vb);
+    }
+    __syncthreads();
+    const double2 *res = fft_lines<-1>(a, b, L, P, s_root);
+    const double invn = 1.0 / (double)n;
+    for (int i = threadIdx.x; i < d.nkx * RW; i += blockDim.x) {
+        const int k = i / RW, r = i - (i / RW) * RW;
+        const int z = z0 + r;
+        if (z >= d.NZ2) continue;
+        const int km = (n - k) % n;
+        const double2 P0 = res[k * L + (r >> 1)];
+        const double2 Pm = res[km * L + (r >> 1)];
+        const double2 out = (r & 1) ? mk(0.5 * (P0.y + Pm.y), -0.5 * (P0.x - Pm.x))
+                                    : mk(0.5 * (P0.x + Pm.x), 0.5 * (P0.y - Pm.y));
+        H[((long long)j * d.NZ2 + z) * d.nkx + k] = cscale(invn, out);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host launchers
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kJT = 2;
+constexpr int kKT = 8;
+constexpr int kTL = 16;
+constexpr int kRW = 4;
+constexpr int kRWs = 8;
+}  // namespace
+
+size_t smem_zfft(const Dims &d) { return sizeof(double2) * (size_t)d.NZ2 * (1 + 2 * kTL); }
+size_t smem_xcross(const Dims &d) { return sizeof(double2) * (size_t)d.NX2 * (1 + 2 * 3 * kRW); }
+size_t smem_xsingle(const Dims &d) {
+    return sizeof(double2) * (size_t)d.NX2 * (1 + 2 * ((kRWs + 1) / 2));
+}
+
+cudaError_t configure_transform_kernels(const Dims &d) {
+    cudaError_t e;
+    e = cudaFuncSetAttribute(k_z_backward, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem_zfft(d));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_z_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem_zfft(d));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_x_cross, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem_xcross(d));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_x_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem_xsingle(d));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_x_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem_xsingle(d));
+    return e;
+}
+
+void launch_curl_ysynth(const Dims &d, const Tables &t, const double2 *u, double2 *F, double2 *bw,
+                        double re, bool curl, cudaStream_t s) {
+    dim3 block(32, 4);
+    const int groups = (d.nyh + kJT - 1) / kJT;
+    dim3 grid((d.ncol + 31) / 32, (groups + 3) / 4);
+    const size_t sm = sizeof(double) * 2 * d.NY2;
+    if (curl) k_curl_ysynth<kJT, true><<<grid, block, sm, s>>>(d, t, u, F, bw, 0.0, re);
+    else k_curl_ysynth<kJT, false><<<grid, block, sm, s>>>(d, t, u, F, bw, 0.0, re);
+}
+
+void launch_z_backward(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *F,
+                       double2 *G, int nf, cudaStream_t s) {
+    dim3 grid((d.nkx + kTL - 1) / kTL, d.ny2, nf);
+    k_z_backward<<<grid, 128, smem_zfft(d), s>>>(d, P, roots, F, G, kTL);
+}
+
+void launch_x_cross(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G,
+                    double2 *H, cudaStream_t s) {
+    dim3 grid((d.NZ2 + kRW - 1) / kRW, d.ny2);
+    k_x_cross<<<grid, 256, smem_xcross(d), s>>>(d, P, roots, G, H, kRW);
+}
+
+void launch_z_forward(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *H,
+                      double2 *F, int nf, cudaStream_t s) {
+    dim3 grid((d.nkx + kTL - 1) / kTL, d.ny2, nf);
+    k_z_forward<<<grid, 128, smem_zfft(d), s>>>(d, P, roots, H, F, kTL);
+}
+
+void launch_y_analysis(const Dims &d, const Tables &t, const double2 *F, double2 *S, int nf,
+                       cudaStream_t s) {
+    dim3 block(32, 4);
+    const int groups = (d.ncy + kKT - 1) / kKT;
+    dim3 grid((nf * d.ncol + 31) / 32, (groups + 3) / 4);
+    k_y_analysis<kKT><<<grid, block, sizeof(double) * 2 * d.NY2, s>>>(d, t, F, S, nf);
+}
+
+void launch_x_c2r(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G,
+                  double *phys, cudaStream_t s) {
+    dim3 grid((d.NZ2 + kRWs - 1) / kRWs, d.ny2);
+    k_x_c2r<<<grid, 128, smem_xsingle(d), s>>>(d, P, roots, G, phys, kRWs);
+}
+
+void launch_x_r2c(const Dims &d, const FftPlan &P, const double2 *roots, const double *phys,
+                  double2 *H, cudaStream_t s) {
+    dim3 grid((d.NZ2 + kRWs - 1) / kRWs, d.ny2);
+    k_x_r2c<<<grid, 128, smem_xsingle(d), s>>>(d, P, roots, phys, H, kRWs);
+}
+
+}  // namespace cdns

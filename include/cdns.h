@@ -1,0 +1,157 @@
+/* cdns.h -- C ABI of the B200 (sm_100a) channel-dns time step.
+ *
+ * This library replaces the per-time-step hot path of the reference solver
+ * (hesse-x/channel-dns): the body of Simulation::enqueue_serial_step
+ * (src/sim/simulation.cpp:142-171) together with the objects it drives --
+ * Transforms::xyzfft2_impl (src/fft/transforms.cpp:615-741),
+ * vector_ops::enqueue_curl / enqueue_cross_product
+ * (src/solver/vector_ops.cpp:112-151, :250-272), TimeStepper
+ * (src/solver/timestepper.cpp:19-68), EqSolvePV::setup / solve_modes
+ * (src/solver/eqsolve_pv.cpp:311-509) and Simulation::correct_flow
+ * (src/sim/simulation.cpp:111-140).  The reference's C++ driver keeps config
+ * parsing, restart/physical output and statistics; it hands the state over
+ * in its own memory layout.
+ *
+ * Conventions
+ *  - Every function returns CDNS_OK (0) or a nonzero cdns_status; no C++
+ *    exception crosses the ABI and device code never traps.  The message of
+ *    the last failure on the calling thread is available from
+ *    cdns_last_error().
+ *  - Complex arrays are interleaved (re, im) doubles in the reference layout
+ *    (src/core/array4d.hpp:62-67, src/solver/fields.hpp:17-22):
+ *      velocity   [2*NZS+1][NYS+1][NXS+1][3]   (component innermost)
+ *      pressure   [2*NZS+1][NYS+1][NXS+1]
+ *      vel. BC    [2*NZS+1][2][NXS+1][3]       (wall 0 is y=+1, wall 1 is y=-1)
+ *      fine phys. [NZ2][NY2+1][NX2]            (real)
+ *    Host pointers may be pageable or pinned; *_device variants take device
+ *    pointers on the context's GPU and copy on the context's stream.
+ *  - One context per host thread; the context owns its CUDA stream, its
+ *    device buffers and its captured step graphs.
+ */
+#ifndef CDNS_H
+#define CDNS_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    CDNS_OK = 0,
+    CDNS_ERR_ARG = 1,         /* bad argument, size or unsupported mesh */
+    CDNS_ERR_CUDA = 2,        /* CUDA runtime failure */
+    CDNS_ERR_STATE = 3,       /* call out of order (e.g. step before set_velocity) */
+    CDNS_ERR_NONFINITE = 4,   /* the step produced NaN/Inf (reference: finite check) */
+    CDNS_ERR_PIVOT = 5,       /* zero or non-finite tau pivot / flow response */
+    CDNS_ERR_NOMEM = 6        /* device allocation failed */
+} cdns_status;
+
+typedef enum { CDNS_PRECISION_FP64 = 0 } cdns_precision;
+
+/* Mesh, mirrors MeshParm (src/core/params.hpp:6-11) + XL/ZL
+ * (src/core/mesh.hpp:9-37).  Single rank: INDEX_Serial = 1. */
+typedef struct {
+    int NX, NY, NZ;
+    int NXS, NYS, NZS;
+    int NX2, NY2, NZ2;
+    double XL, ZL;
+} cdns_mesh_desc;
+
+/* Physical and control parameters, mirrors Parm / Control
+ * (src/core/params.hpp:13-35) and the derived GRAD_PRE / QXmean values
+ * (src/core/params.cpp:296-307, recomputed from THETA). */
+typedef struct {
+    double Re;
+    double G_pre, a_pre0, b_pre0;
+    double a_V[3], b_V[3];
+    int INDEX_GRAD_PRE;
+    double THETA;            /* degrees */
+    double DT;
+    double V_Microblow0;
+} cdns_params;
+
+typedef struct cdns_ctx cdns_ctx;
+
+/* Create a context on CUDA device `device`.  Replaces the construction of
+ * Transforms (src/fft/transforms.cpp:59-281), EqSolvePV
+ * (src/solver/eqsolve_pv.cpp:132-146) and TimeStepper.  The velocity
+ * boundary data starts as velocity_boundary() (src/sim/initial_bc.cpp:95-101). */
+int cdns_create(const cdns_mesh_desc *mesh, const cdns_params *params, int precision,
+                int device, cdns_ctx **out);
+int cdns_destroy(cdns_ctx *ctx);
+
+/* State transfer in the reference layout.  set_velocity also restarts the
+ * multistep history (a restart is first order, doc/algorithm.md:104).
+ * Replaces FieldIO::read_restart's hand-over (src/io/field_io.cpp:311-427). */
+int cdns_set_velocity(cdns_ctx *ctx, const double *velocity);
+int cdns_get_velocity(cdns_ctx *ctx, double *velocity);
+int cdns_get_pressure(cdns_ctx *ctx, double *pressure);
+int cdns_set_velocity_bc(cdns_ctx *ctx, const double *bc);
+int cdns_set_velocity_device(cdns_ctx *ctx, const double *velocity_dev);
+int cdns_get_velocity_device(cdns_ctx *ctx, double *velocity_dev);
+
+/* One time step of Simulation::run (src/sim/simulation.cpp:174-185,
+ * INDEX_Serial = 1): step_coefficients(iteration), EqSolvePV::setup at
+ * iteration < 3, enqueue_serial_step and correct_flow.  `iteration` is the
+ * 1-based loop counter `it`.  Asynchronous on the context stream;
+ * status checks (non-finite values, pivots) are reported by cdns_synchronize. */
+int cdns_step(cdns_ctx *ctx, int iteration);
+
+/* `nsteps` steps starting at loop counter `first_iteration`; steps with
+ * it >= 3 replay captured CUDA graphs.  Returns after enqueueing. */
+int cdns_run(cdns_ctx *ctx, int first_iteration, int nsteps);
+
+/* Wait for the context stream; returns CDNS_ERR_NONFINITE / CDNS_ERR_PIVOT if
+ * a step since the last call raised one. */
+int cdns_synchronize(cdns_ctx *ctx);
+
+/* Pressure gradient of the last step (dpdx_, dpdz_ of Simulation, used by
+ * Statistics::accumulate). */
+int cdns_get_dpdx(cdns_ctx *ctx, double out[2]);
+
+/* Nonlinear term alone, TimeStepper::nonlinear_term
+ * (src/solver/timestepper.cpp:11-17): N = u x curl u on the product grid and
+ * the pressure wall data B [2*NZS+1][2][NXS+1]. */
+int cdns_nonlinear(cdns_ctx *ctx, const double *velocity, double *nonlinear, double *pressure_bc);
+
+/* Fine-grid transform of one scalar field, Transforms::channel_xyzfft2
+ * (src/fft/transforms.cpp:615-741).  direction 'B': spectral -> physical,
+ * 'F': physical -> spectral. */
+int cdns_transform_fine(cdns_ctx *ctx, int direction, const double *in, double *out);
+
+/* EqSolvePV::setup(g) followed by the fused solve (solve_modes with fused
+ * RHS divergence and sigma correction, src/solver/eqsolve_pv.cpp:311-450)
+ * of a given velocity RHS [..][3], pressure wall data [..][2][..] and velocity
+ * wall data [..][2][..][3]; writes pressure and velocity and, if `units` is
+ * not NULL, u_dpdx_unit then w_dpdz_unit (2*(NYS+1) doubles). */
+int cdns_solve(cdns_ctx *ctx, double g, const double *rhs_velocity, const double *pressure_bc,
+               const double *velocity_bc, double *pressure, double *velocity, double *units);
+
+/* Per-stage device timing for roofline accounting.  Between
+ * cdns_profile_begin and cdns_profile_end, steps launch stage by stage on
+ * the context stream with CUDA events between stages (no graph replay);
+ * cdns_profile_end synchronises and writes the summed milliseconds of each
+ * stage into stage_ms[cdns_stage_count()] and the number of steps timed. */
+int cdns_profile_begin(cdns_ctx *ctx);
+int cdns_profile_end(cdns_ctx *ctx, double *stage_ms, int *nsteps);
+int cdns_stage_count(void);
+const char *cdns_stage_name(int stage);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that order their
+ * own work or CUDA events against the step. */
+int cdns_get_stream(cdns_ctx *ctx, void **stream);
+
+/* Number of bytes of device memory the context holds. */
+int cdns_device_bytes(cdns_ctx *ctx, size_t *bytes);
+
+/* Copy the last error message of the calling thread into buf. */
+int cdns_last_error(char *buf, size_t len);
+
+/* Library version string. */
+const char *cdns_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CDNS_H */

@@ -1,0 +1,221 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle and with the
+golden vectors of the reference's own sources.  Needs a B200.
+
+Tolerances (FP64 throughout; differences are rounding-order only):
+  transforms, nonlinear term  max |gpu - ref| <= 1e-12 * max|ref|
+  solver                      |gpu - ref| <= 1e-10 * max(1, |ref|)   (reference's own bar,
+                              tests/test_eqsolve.cpp:174-179)
+  time steps                  relative L2 <= 1e-10 per velocity component, divergence <= 1e-12
+"""
+import numpy as np
+import pytest
+
+import cdns
+from golden_io import load
+from oracle_cases import band_spectrum, channel_case, divergence_free_field, example_case, orc
+
+pytestmark = pytest.mark.gpu
+
+
+def ctx_for(m, p):
+    mesh = cdns.Mesh(m.NX, m.NY, m.NZ, m.NXS, m.NYS, m.NZS, m.NX2, m.NY2, m.NZ2, m.XL, m.ZL)
+    params = cdns.Params(Re=p.Re, DT=p.DT, G_pre=p.G_pre, a_pre0=p.a_pre0, b_pre0=p.b_pre0,
+                         a_V=p.a_V, b_V=p.b_V, INDEX_GRAD_PRE=p.INDEX_GRAD_PRE, THETA=p.THETA,
+                         V_Microblow0=p.V_Microblow0)
+    return cdns.Context(mesh, params)
+
+
+def rel_max(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+# ---------------------------------------------------------------- transforms
+@pytest.mark.parametrize("case", ["golden", "full", "trunc", "channel48"])
+def test_fine_transforms(case):
+    if case == "golden":
+        m, p, d = load("golden_fine.npz")
+        U = d["U"]
+        phys_ref, back_ref = d["phys"], d["back"]
+    else:
+        if case == "full":
+            m, p = example_case()          # 32^3, NX2 = 2 NXS: Nyquist branches
+        elif case == "trunc":
+            m, p = example_case(NXS=10, NYS=20, NZS=10)
+        else:
+            m, p = channel_case(32)        # 48 x 49 x 48 product grid
+        U = band_spectrum(m, 5)
+        phys_ref = orc.fine_backward(m, U)
+        back_ref = orc.fine_forward(m, phys_ref)
+    c = ctx_for(m, p)
+    phys = c.transform_fine("B", U)
+    assert rel_max(phys, phys_ref) <= 1e-12
+    back = c.transform_fine("F", phys_ref)
+    assert rel_max(back, back_ref) <= 1e-12
+    assert np.abs(back - U).max() <= 1e-12 * np.abs(U).max()   # round trip (band-limited)
+
+
+def test_fine_forward_analytic_nyquist_peak():
+    """tests/test_xyzfft.cpp:323-353: a fine-grid Nyquist mode has peak 1.0."""
+    m, p = example_case()
+    c = ctx_for(m, p)
+    iz = np.arange(m.NZ2)[:, None, None]
+    iy = np.arange(m.NY2 + 1)[None, :, None]
+    ix = np.arange(m.NX2)[None, None, :]
+    P = np.cos(2 * np.pi * 16 * ix / m.NX2) * np.cos(3 * np.pi * iy / m.NY2) * np.cos(2 * np.pi * 3 * iz / m.NZ2)
+    U = c.transform_fine("F", P)
+    ref = orc.fine_forward(m, P)
+    assert np.abs(U - ref).max() < 1e-12
+    assert abs(U[m.NZS + 3, 3, 16] - 0.5) < 1e-12
+
+
+# ------------------------------------------------------------- nonlinear term
+@pytest.mark.parametrize("case", ["golden", "channel32"])
+def test_nonlinear_term(case):
+    if case == "golden":
+        m, p, d = load("golden_nonlinear.npz")
+        u = list(d["u"])
+        N_ref, B_ref = list(d["N"]), (d["B"][0], d["B"][1])
+    else:
+        m, p = channel_case(32)
+        u = divergence_free_field(m, p, seed=3, amp=0.05, kmax=6)
+        cst = orc.make_constants(m, p.Re)
+        N_ref, _, B_ref = orc.nonlinear_term(m, cst, u)
+    c = ctx_for(m, p)
+    N, B = c.nonlinear(np.stack(u, axis=-1))
+    for k in range(3):
+        assert rel_max(N[..., k], N_ref[k]) <= 1e-12
+    assert rel_max(B[:, 0], B_ref[0]) <= 1e-12
+    assert rel_max(B[:, 1], B_ref[1]) <= 1e-12
+
+
+def test_uniform_velocity_has_zero_nonlinear_term():
+    """tests/test_timestepper.cpp:57-74."""
+    m, p = example_case()
+    c = ctx_for(m, p)
+    u = np.zeros(m.spectral_shape() + (3,), dtype=np.complex128)
+    u[m.NZS, 0, 0] = [1.0, 2.0, 3.0]
+    N, B = c.nonlinear(u)
+    assert np.abs(N).max() < 1e-12 and np.abs(B).max() < 1e-12
+
+
+# ---------------------------------------------------------------------- solver
+def test_solver_matches_reference_golden():
+    m, p, d = load("golden_solve.npz")
+    c = ctx_for(m, p)
+    rhs = np.stack(list(d["rhs"]), axis=-1)
+    pbc = np.stack([d["bc_p"][0], d["bc_p"][1]], axis=1)
+    vbc = np.stack([np.stack([d["bc_v"][k][0], d["bc_v"][k][1]], axis=1) for k in range(3)], axis=-1)
+    pres, vel, uu, wu = c.solve(float(d["g"]), rhs, pbc, vbc)
+    assert np.all(np.abs(pres - d["p"]) <= 1e-10 * np.maximum(1.0, np.abs(d["p"])))
+    for k in range(3):
+        assert np.all(np.abs(vel[..., k] - d["v"][k]) <= 1e-10 * np.maximum(1.0, np.abs(d["v"][k])))
+    assert np.abs(uu - d["u_unit"]).max() <= 1e-12 * np.abs(d["u_unit"]).max()
+    assert np.abs(wu - d["w_unit"]).max() <= 1e-12 * np.abs(d["w_unit"]).max()
+
+
+@pytest.mark.parametrize("nxs", [7, 8, 16])
+@pytest.mark.parametrize("neumann", [False, True])
+def test_solver_matches_oracle(nxs, neumann):
+    """Fused solve vs the oracle on the reference's equivalence-test inputs
+    (tests/test_eqsolve.cpp:138-185 construction), Dirichlet and Neumann v."""
+    m, p = example_case(NXS=nxs, a_v1=0.0 if neumann else 1.0, b_v1=1.0 if neumann else 0.0)
+    cst = orc.make_constants(m, p.Re)
+    s = orc.Solver(m, p, cst)
+    with np.errstate(all="ignore"):
+        s.setup(150.0)
+    sh = m.spectral_shape()
+    n = int(np.prod(sh))
+    iv = np.arange(3 * n).reshape(sh + (3,))
+    rv = np.sin(iv * 0.17) * 0.001 + 1j * np.cos(iv * 0.23) * 0.002
+    ib = np.arange(m.nkz * 2 * m.nkx).reshape(m.nkz, 2, m.nkx)
+    bp = np.sin(ib * 0.11) * 0.001 + 1j * np.cos(ib * 0.29) * 0.002
+    ibv = np.arange(m.nkz * 2 * m.nkx * 3).reshape(m.nkz, 2, m.nkx, 3)
+    bv = np.sin(ibv * 0.31) * 0.001 + 1j * np.cos(ibv * 0.37) * 0.002
+    ep, ev = s.solve_modes(None, (bp[:, 0], bp[:, 1]), [rv[..., k] for k in range(3)],
+                           [(bv[:, 0, :, k], bv[:, 1, :, k]) for k in range(3)], True)
+    c = ctx_for(m, p)
+    pres, vel, _, _ = c.solve(150.0, rv, bp, bv)
+    scale_p = max(1.0, np.abs(ep).max())
+    assert np.abs(pres - ep).max() <= 1e-10 * scale_p
+    for k in range(3):
+        assert np.abs(vel[..., k] - ev[k]).max() <= 1e-10 * max(1.0, np.abs(ev[k]).max())
+
+
+# ------------------------------------------------------------------ time steps
+def _run_gpu(m, p, u0, nsteps, graphs=True):
+    c = ctx_for(m, p)
+    c.set_velocity(np.stack(u0, axis=-1))
+    if graphs:
+        c.run(1, nsteps)
+    else:
+        for it in range(1, nsteps + 1):
+            c.step(it)
+    c.synchronize()
+    return c, c.get_velocity(), c.get_pressure()
+
+
+@pytest.mark.parametrize("name", ["golden_step.npz", "golden_example.npz"])
+def test_steps_match_reference_golden(name):
+    m, p, d = load(name)
+    _, v, pr = _run_gpu(m, p, list(d["u0"]), int(d["nsteps"]))
+    for k in range(3):
+        assert orc.rel_l2(v[..., k], d["u"][k]) <= 1e-10
+    assert orc.rel_l2(pr, d["p"]) <= 1e-9
+
+
+@pytest.mark.parametrize("graphs", [True, False])
+def test_config0_five_steps(graphs):
+    """32x33x32 (48^3 product grid), 4pi x 2 x 2pi, fixed dp/dx, Re_tau=180,
+    laminar + 5% divergence-free perturbation on |k|<=4, 5 steps."""
+    m, p = channel_case(32)
+    u0 = divergence_free_field(m, p, seed=0, amp=0.05, kmax=4)
+    sim = orc.Simulation(m, p, u0)
+    with np.errstate(all="ignore"):
+        sim.run(5)
+    c, v, pr = _run_gpu(m, p, u0, 5, graphs=graphs)
+    cst = orc.make_constants(m, p.Re)
+    for k in range(3):
+        assert orc.rel_l2(v[..., k], sim.u[k]) <= 1e-10
+    assert orc.rel_l2(pr, sim.pressure) <= 1e-9
+    div = orc.divergence(cst, [v[..., k] for k in range(3)])
+    assert np.abs(div).max() <= 1e-12 * max(1.0, np.abs(v).max())
+    assert c.dpdx() == pytest.approx((-1.0, -0.0))
+
+
+def test_constant_flux_mode_and_blowing():
+    """Constant flow rate (INDEX_GRAD_PRE=0) with wall blowing V_Microblow0
+    (the reference's example configuration), 6 steps against the oracle."""
+    m, p = example_case(NXS=8, NYS=14, NZS=8, N2=16, N=16)
+    u0 = [band_spectrum(m, s, 1e-3) for s in (21, 22, 23)]
+    u0[0][m.NZS, 0, 0] += 0.75
+    u0[0][m.NZS, 2, 0] += -0.75
+    sim = orc.Simulation(m, p, u0)
+    with np.errstate(all="ignore"):
+        sim.run(6)
+    c, v, pr = _run_gpu(m, p, u0, 6)
+    for k in range(3):
+        assert orc.rel_l2(v[..., k], sim.u[k]) <= 1e-10
+    dx, dz = c.dpdx()
+    assert dx == pytest.approx(sim.dpdx, rel=1e-9, abs=1e-14)
+    assert v[m.NZS, 0, 0, 1] == pytest.approx(1e-3)
+
+
+def test_nonfinite_input_is_reported():
+    """Failure detection without a GPU fault: a NaN seeded into the input field
+    is flagged by the device-side finite check and returned as a status."""
+    m, p = channel_case(16)
+    u0 = divergence_free_field(m, p, seed=1, amp=0.05, kmax=3)
+    u0[1][m.NZS + 1, 3, 2] = np.nan
+    c = ctx_for(m, p)
+    c.set_velocity(np.stack(u0, axis=-1))
+    c.run(1, 2)
+    with pytest.raises(cdns.CdnsError) as e:
+        c.synchronize()
+    assert e.value.code == 4
+
+
+def test_bad_mesh_is_rejected():
+    m, p = channel_case(16)
+    with pytest.raises(cdns.CdnsError) as e:
+        cdns.Context(cdns.Mesh(16, 16, 16, 8, 14, 8, 12, 16, 24, 1.0, 1.0), cdns.Params(Re=1.0, DT=1e-3))
+    assert e.value.code == 1
