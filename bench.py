@@ -1,0 +1,361 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 channel-dns time step.
+
+Workload: Re_tau = 180 channel, 128 x 129 x 128 base grid (NXS = NZS = 64,
+NYS = 126), 196 x 193 x 196 dealiased product grid, 4 pi x 2 x 2 pi, fixed
+mean pressure gradient, DT = 5e-5, FP64.  Initial field: seeded Reichardt
+log-law mean profile plus a divergence-free perturbation with a k^-5/3
+envelope at 10 % rms (synthetic, cdns/fields.py).
+
+  value   steps/s with the state resident in HBM: K graph-replayed steady
+          steps (it > W >= 3) timed with CUDA events on the library stream,
+          max over ranks, x ranks.
+  e2e     steps/s through the C ABI with host buffers: upload of the state
+          from pinned memory, K steps called one by one from iteration 1
+          (setup included) each reading back its pressure gradient, and the
+          download of velocity and pressure, timed with the same events.
+  roofline  the dominant stage's algorithmic HBM bytes per launch over its
+          CUDA-event duration (per-stage pass after the timed region).
+  cpu_baseline  the reference's own sources (oracle/_ref, built with the
+          project FFTW/MPI shims) on this host's cores, bounded sample.
+
+``--impl reference`` times the reference CPU solver alone on the same
+workload.  With torchrun (N > 1) every rank advances its own channel
+(replicas, no collective in the data path; scaling "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "channel-dns_b200"))
+
+METRIC = ("Reτ180 128×129×128 steps/s: FP64 vs FP32/FP64 (err≤1e-6); "
+          "adjoint/fwd cost")
+PI = math.acos(-1.0)
+WORKLOAD = {"workload": "retau180_fp64_step", "grid": "128x129x128", "product_grid": "196x193x196",
+            "domain": "4pi x 2 x 2pi", "Re_tau": 180, "DT": 5e-5, "forcing": "fixed dp/dx",
+            "precision": "fp64", "l2_policy": "inputs larger than L2 (about 1.7 GB of stage traffic per step)"}
+
+
+def workload_mesh():
+    import cdns
+    mesh = cdns.Mesh(128, 128, 128, 64, 126, 64, 196, 192, 196, 4.0 * PI, 2.0 * PI)
+    params = cdns.Params(Re=180.0, DT=5e-5, INDEX_GRAD_PRE=1)
+    return mesh, params
+
+
+def stage_bytes(mesh):
+    """Algorithmic HBM bytes per launch of each stage (16 B per complex value;
+    every stage reads and writes its operands once)."""
+    nkx, nkz, ncy = mesh.NXS + 1, 2 * mesh.NZS + 1, mesh.NYS + 1
+    ny2 = mesh.NY2 + 1
+    Ns = nkz * ncy * nkx
+    Ny = nkz * ny2 * nkx
+    Nz = mesh.NZ2 * ny2 * nkx
+    return {
+        "curl_ysynth": 16 * (3 * Ns + 6 * Ny),
+        "z_backward": 16 * 6 * (Ny + Nz),
+        "x_cross": 16 * 9 * Nz,
+        "z_forward": 16 * 3 * (Nz + Ny),
+        "y_analysis": 16 * (3 * Ny + 3 * Ns),
+        # R from u, u_prev, N, N_prev (12), influence + B-problem fields (12),
+        # tau pivots ad_p, ad_v (1 complex-equivalent), writes u, p (4)
+        "solve": 16 * 29 * Ns,
+    }
+
+
+def step_bytes_model(mesh):
+    """Stage-pass model of the whole step (5 fused stages):
+    16 (3Ns + 6Ny) + 96 (Ny + Nz) + 144 Nz + 48 (Nz + Ny) + 16 (3Ny + 29 Ns)."""
+    nkx, nkz, ncy = mesh.NXS + 1, 2 * mesh.NZS + 1, mesh.NYS + 1
+    ny2 = mesh.NY2 + 1
+    Ns, Ny, Nz = nkz * ncy * nkx, nkz * ny2 * nkx, mesh.NZ2 * ny2 * nkx
+    return 16 * (3 * Ns + 6 * Ny) + 96 * (Ny + Nz) + 144 * Nz + 48 * (Nz + Ny) + 16 * (3 * Ny + 29 * Ns)
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        fd, self.path = tempfile.mkstemp(prefix="cdns_clocks_", suffix=".csv")
+        os.close(fd)
+        self.fh = open(self.path, "w")
+        self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                      "-lms", "200", "-i", str(self.dev)], stdout=self.fh,
+                                     stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def reference_arm_time(steps: int, warmup: int, threads: int):
+    """Steady steps/s of the reference CPU solver: T(n1 + steps) - T(n1),
+    each run from the same restart (setup and final output cancel)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_io  # the reference sources built in oracle/_ref (checker / baseline only)
+    import cdns
+    from cdns.fields import divergence_free_field
+    mesh, params = workload_mesh()
+    u0 = divergence_free_field(mesh, params, seed=1, amp=0.1, spectrum="k53", mean="loglaw")
+
+    class _M:
+        pass
+
+    m = _M()
+    for k in ("NX", "NY", "NZ", "NXS", "NYS", "NZS", "NX2", "NY2", "NZ2", "XL", "ZL"):
+        setattr(m, k, getattr(mesh, k))
+    m.nkz, m.ncy, m.nkx = 2 * mesh.NZS + 1, mesh.NYS + 1, mesh.NXS + 1
+
+    class _P:
+        pass
+
+    p = _P()
+    p.Re, p.DT, p.G_pre, p.a_pre0, p.b_pre0 = 180.0, 5e-5, 0.0, 0.0, 1.0
+    p.a_V, p.b_V, p.INDEX_GRAD_PRE, p.THETA, p.V_Microblow0 = (1.0, 1.0, 1.0), (0.0, 0.0, 0.0), 1, 0.0, 0.0
+    if ref_io.available():
+        n1 = max(warmup, 2)
+        _, _, t1 = ref_io.run_steps(m, p, u0, n1, threads=threads)
+        _, _, t2 = ref_io.run_steps(m, p, u0, n1 + steps, threads=threads)
+        dt = max(t2 - t1, 1e-9)
+        return steps / dt, {"kind": "reference", "cores": threads,
+                            "sample": f"reference sources + project FFT shim (oracle/_ref), "
+                                      f"T({n1 + steps} steps) - T({n1} steps) from one restart, "
+                                      f"{threads} threads"}
+    # the numpy restatement, single thread, one steady step
+    import numpy as np
+    import channel_oracle as orc
+    om = orc.Mesh(*(getattr(mesh, k) for k in ("NX", "NY", "NZ", "NXS", "NYS", "NZS", "NX2", "NY2", "NZ2")),
+                  mesh.XL, mesh.ZL)
+    op = orc.Parm(Re=180.0, DT=5e-5)
+    sim = orc.Simulation(om, op, u0)
+    with np.errstate(all="ignore"):
+        sim.run(2)
+        t = time.perf_counter()
+        sim.run(steps)
+        dt = time.perf_counter() - t
+    return steps / dt, {"kind": "port", "cores": 1,
+                        "sample": f"numpy oracle, {steps} steady steps after 2 setup steps"}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    steps = max(1, min(args.steps, 10))
+    v, info = reference_arm_time(steps, args.warmup, threads)
+    line = {"metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": args.gpus, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(WORKLOAD), "impl": "reference",
+            "cpu_baseline": dict(info, value=v, unit="steps/s"),
+            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=0, help="steps of the e2e pass (default: min(K, 200))")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+    if args.warmup < 3:
+        raise SystemExit("--warmup must be >= 3")
+
+    import numpy as np
+    import torch
+    import cdns
+    from cdns.fields import divergence_free_field
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    mesh, params = workload_mesh()
+    u0 = divergence_free_field(mesh, params, seed=1 + rank, amp=0.1, spectrum="k53", mean="loglaw")
+    host_u = torch.from_numpy(np.stack(u0, axis=-1)).pin_memory()
+    host_v = torch.empty_like(host_u).pin_memory()
+    host_p = torch.empty(host_u.shape[:-1], dtype=torch.complex128).pin_memory()
+    ctx = cdns.Context(mesh, params, device=local)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=local)
+    K, W = args.steps, args.warmup
+
+    # ---- device-resident throughput ------------------------------------
+    clocks = ClockSampler(local)
+    clocks.start()
+    ctx.set_velocity(host_u.numpy())
+    ctx.run(1, W)
+    ctx.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ctx.run(W + 1, K)
+    e1.record(stream)
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms_total = e0.elapsed_time(e1)
+    t = torch.tensor([ms_total], device=f"cuda:{local}", dtype=torch.float64)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    ms_per_step = ms_max / K
+    value = world * K / (ms_max / 1000.0)
+
+    # ---- per-stage timing (roofline of the dominant stage) ---------------
+    ctx.profile_begin()
+    nprof = 20
+    ctx.run(W + K + 1, nprof)
+    stage_ms, nst = ctx.profile_end()
+    per_launch = {k: v / nst for k, v in stage_ms.items()}
+    sb = stage_bytes(mesh)
+    top = max(per_launch, key=per_launch.get)
+    peak, peak_kind = measured_peak()
+    achieved = sb[top] / (per_launch[top] * 1e-3) / 1e9
+    step_model = step_bytes_model(mesh)
+
+    # ---- end to end through the C ABI with host buffers -------------------
+    KE = args.e2e_steps or min(K, 200)
+    ctx2 = cdns.Context(mesh, params, device=local)
+    s2 = torch.cuda.ExternalStream(ctx2.stream_ptr(), device=local)
+    barrier()
+    torch.cuda.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(s2)
+    ctx2.set_velocity(host_u.numpy())
+    dp = None
+    for it in range(1, KE + 1):
+        ctx2.step(it)
+        dp = ctx2.dpdx()
+    ctx2.synchronize()
+    v_np = ctx2.get_velocity()
+    p_np = ctx2.get_pressure()
+    f1.record(s2)
+    torch.cuda.synchronize()
+    e2e_ms = f0.elapsed_time(f1)
+    t = torch.tensor([e2e_ms], device=f"cuda:{local}", dtype=torch.float64)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_ms = float(t.item())
+    e2e_value = world * KE / (e2e_ms / 1000.0)
+    state_bytes = host_u.numel() * 16
+    h2d = state_bytes / KE
+    d2h = 16 + (host_u.numel() + host_p.numel()) * 16 / KE
+    finite = bool(np.isfinite(v_np).all() and np.isfinite(p_np).all())
+
+    # ---- CPU baseline (rank 0, N = 1) ----------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            v_cpu, info = reference_arm_time(2, 2, os.cpu_count() or 1)
+            cpu = dict(info, value=v_cpu, unit="steps/s")
+        except Exception as exc:  # the baseline must not hide the GPU line
+            cpu = {"value": None, "unit": "steps/s", "error": str(exc)[:200]}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": K,
+            "warmup": W, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(WORKLOAD, parallelism=f"replicas{world}",
+                           grid_points_steps_per_s=value * 128 * 129 * 128,
+                           product_points_steps_per_s=value * 196 * 193 * 196,
+                           step_model_bytes=step_model,
+                           step_roofline_frac=(step_model / (ms_per_step * 1e-3) / 1e9) / peak),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "kernel": top,
+                         "algorithmic_bytes": sb[top], "launch_ms": per_launch[top],
+                         "peak_source": peak_kind,
+                         "stage_ms": {k: round(v, 5) for k, v in per_launch.items()}},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": KE, "finite": finite,
+                    "protocol": "upload + steps 1..K one call each with dpdx readback + download"},
+            "clocks": clk,
+            "gpu_launches": 6 * K,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    ctx2.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

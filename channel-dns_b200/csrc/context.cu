@@ -298,12 +298,15 @@ int cdns_create(const cdns_mesh_desc *m, const cdns_params *p, int precision, in
     };
     const auto rx = roots(d.NX2), rz = roots(d.NZ2);
     double *tab = nullptr;
-    const size_t ntab = d.nkx + d.nkz + 3 * (size_t)d.ncy + cosy.size() + 2 * (size_t)d.NX2 + 2 * (size_t)d.NZ2;
+    // every table starts on a 256-byte boundary (double2 tables need 16)
+    auto rup = [](size_t n) { return (n + 31) / 32 * 32; };
+    const size_t ntab = rup(d.nkx) + rup(d.nkz) + 3 * rup(d.ncy) + rup(cosy.size()) +
+                        rup(2 * (size_t)d.NX2) + rup(2 * (size_t)d.NZ2);
     if ((r = c->alloc(tab, ntab))) return bail(r);
     size_t o = 0;
     auto put = [&](const void *src, size_t count) {
         double *dst = tab + o;
-        o += count;
+        o += rup(count);
         return std::make_pair(dst, upload(c, dst, src, count * sizeof(double)));
     };
     auto pw = put(wavx.data(), wavx.size()); c->t.wavx = pw.first;

@@ -14,8 +14,9 @@ import sys
 import numpy as np
 
 _ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-if os.path.join(_ROOT, "oracle") not in sys.path:
-    sys.path.insert(0, os.path.join(_ROOT, "oracle"))
+for _p in (os.path.join(_ROOT, "oracle"), os.path.join(_ROOT, "channel-dns_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
 
 import channel_oracle as orc  # noqa: E402
 
@@ -89,99 +90,7 @@ def band_spectrum(m: orc.Mesh, seed: int, amp: float = 1.0) -> np.ndarray:
 def divergence_free_field(m: orc.Mesh, p: orc.Parm, seed: int, amp: float,
                           kmax: int | None = None, spectrum: str = "flat",
                           mean: str = "laminar"):
-    """Seeded, exactly divergence-free spectral velocity satisfying no-slip.
-
-    The perturbation is u = curl(psi) with psi = (0, phi(y) g, 0) + (0,0,...)
-    built from wall-vanishing Chebyshev combinations, so div u = 0 holds to
-    rounding and u vanishes at both walls.  ``spectrum`` "flat" keeps Fourier
-    modes with |kx|,|kz| <= kmax; "k53" applies a k^-5/3 envelope.  ``mean``
-    "laminar" adds u = (Re/2)(1-y^2) (fixed pressure gradient); "loglaw" adds a
-    turbulent-like mean profile projected on Chebyshev modes.
-    """
-    rng = np.random.default_rng(seed)
-    c = orc.make_constants(m, p.Re)
-    nkz, ncy, nkx = m.spectral_shape()
-    zk = m.NZS
-    ny = m.NYS
-    # Chebyshev coefficients of (1-y^2)^2 * q(y): use a random low-order q and
-    # multiply in physical space on Gauss-Lobatto points, then transform.
-    npts = 2 * ncy
-    yj = np.cos(PI * np.arange(npts) / (npts - 1))
-
-    def cheb_coeffs(vals):
-        # DCT-I based interpolation on npts Gauss-Lobatto points
-        import scipy.fft as sfft
-        a = sfft.dct(vals, type=1, axis=-1) / (npts - 1)
-        a[..., 0] *= 0.5
-        a[..., -1] *= 0.5
-        return a[..., :ncy]
-
-    nq = min(8, max(ncy - 5, 1))
-    ux = np.zeros((nkz, ncy, nkx), dtype=np.complex128)
-    uy = np.zeros_like(ux)
-    uz = np.zeros_like(ux)
-    env = (1.0 - yj * yj) ** 2
-    T = np.cos(np.outer(np.arange(nq), np.arccos(np.clip(yj, -1, 1))))
-    for ikz in range(nkz):
-        kz = ikz - zk
-        for kx in range(nkx):
-            if kx == 0 and kz == 0:
-                continue
-            if spectrum == "flat":
-                if kmax is not None and (kx > kmax or abs(kz) > kmax):
-                    continue
-                scale = 1.0
-            else:
-                k = math.sqrt(kx * kx + kz * kz)
-                scale = k ** (-5.0 / 6.0)  # energy ~ k^-5/3
-            if kx == 0 and kz < 0:
-                continue  # filled by Hermitian symmetry below
-            # two potentials A, B (complex Chebyshev combos, wall-vanishing with
-            # vanishing derivative): u = curl((0, A, 0)) + curl(curl((0, B, 0)))
-            qa = (rng.standard_normal(nq) + 1j * rng.standard_normal(nq)) * scale
-            qb = (rng.standard_normal(nq) + 1j * rng.standard_normal(nq)) * scale
-            A = cheb_coeffs(env * (qa @ T))
-            B = cheb_coeffs(env * (qb @ T))
-            ax = c.WAVX[kx]
-            az = c.WAVZ[ikz]
-            dB = orc.derivative_y(B[None, :, None])[0, :, 0]
-            # curl((0,A,0)) = (-dA/dz, 0, dA/dx) = (-i az A, 0, i ax A)
-            # curl curl((0,B,0)) = (i ax dB/dy, ax^2 B + az^2 B, i az dB/dy)
-            vx = -1j * az * A + 1j * ax * dB
-            vy = (ax * ax + az * az) * B
-            vz = 1j * ax * A + 1j * az * dB
-            ux[ikz, :, kx] = vx
-            uy[ikz, :, kx] = vy
-            uz[ikz, :, kx] = vz
-            if kx == 0:
-                ux[2 * zk - ikz, :, 0] = np.conj(vx)
-                uy[2 * zk - ikz, :, 0] = np.conj(vy)
-                uz[2 * zk - ikz, :, 0] = np.conj(vz)
-    # full-spectrum Nyquist slots are left empty (never used by the configs)
-    # normalise perturbation rms in physical space
-    up = [orc.fine_backward(m, f) for f in (ux, uy, uz)]
-    rms = math.sqrt(sum(float(np.mean(f * f)) for f in up) / 3.0)
-    uc = p.Re / 2.0 if p.INDEX_GRAD_PRE == 1 else 1.5
-    if mean == "laminar":
-        mean_vals = uc * (1.0 - yj * yj)
-        ref = uc
-    else:
-        # Reichardt's smooth law of the wall in wall units (u_tau = 1,
-        # Re_tau = Re): a turbulent-mean-like profile.
-        yp = (1.0 - np.abs(yj)) * p.Re
-        kappa = 0.41
-        mean_vals = (np.log1p(kappa * yp) / kappa
-                     + 7.8 * (1.0 - np.exp(-yp / 11.0) - (yp / 11.0) * np.exp(-yp / 3.0)))
-        ref = float(mean_vals.max())
-    s = (amp * ref / rms) if rms > 0 else 0.0
-    ux *= s
-    uy *= s
-    uz *= s
-    a = cheb_coeffs(mean_vals)
-    # enforce u = 0 at both walls exactly after truncation (T0, T1 correction)
-    top = float(np.sum(a))
-    bot = float(np.sum(a * (-1.0) ** np.arange(ncy)))
-    a[0] -= 0.5 * (top + bot)
-    a[1] -= 0.5 * (top - bot)
-    ux[zk, :, 0] = a
-    return [ux, uy, uz]
+    """Seeded, exactly divergence-free spectral velocity satisfying no-slip
+    (the generator the benchmark uses, channel-dns_b200/cdns/fields.py)."""
+    from cdns.fields import divergence_free_field as gen
+    return gen(m, p, seed, amp, kmax=kmax, spectrum=spectrum, mean=mean)
