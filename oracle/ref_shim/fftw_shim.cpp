@@ -7,8 +7,8 @@
 //   c2r   the real inverse of a Hermitian half spectrum (imaginary parts of
 //         the DC and, for even n, Nyquist bins are ignored)
 //   REDFT00 (n points)  Y_k = x_0 + (-1)^k x_{n-1} + 2 sum_{j=1}^{n-2} x_j cos(pi j k/(n-1))
-// The engine is an iterative mixed-radix Stockham FFT (radix 4, 2, and a
-// direct DFT for odd factors); even-length real transforms are packed into a
+// The engine is an iterative mixed-radix Stockham FFT (radix 4, 2, odd radices
+// by symmetric pairs, per-pass twiddle tables); even-length real transforms are packed into a
 // half-length complex FFT; REDFT00 is the real part of the r2c transform of
 // the even extension of length 2(n-1).
 #include "fftw3.h"
@@ -26,71 +26,153 @@
 namespace {
 using cd = std::complex<double>;
 
+// Odd-radix butterfly by symmetric pairs: y_q = x_0 + sum_t [ (x_t + x_{R-t}) cos(2 pi t q/R)
+//   + sign * i (x_t - x_{R-t}) sin(2 pi t q/R) ].
+template <int R>
+inline void bfly_odd(cd *v, const double *cs, const double *sn, int sign) {
+    constexpr int h = R / 2;
+    double sr[h + 1], si[h + 1], dr[h + 1], di[h + 1];
+    for (int t = 1; t <= h; ++t) {
+        sr[t] = v[t].real() + v[R - t].real();
+        si[t] = v[t].imag() + v[R - t].imag();
+        dr[t] = v[t].real() - v[R - t].real();
+        di[t] = v[t].imag() - v[R - t].imag();
+    }
+    double y0r = v[0].real(), y0i = v[0].imag();
+    for (int t = 1; t <= h; ++t) { y0r += sr[t]; y0i += si[t]; }
+    cd out[R];
+    out[0] = cd(y0r, y0i);
+    for (int q = 1; q <= h; ++q) {
+        double rr = v[0].real(), ri = v[0].imag(), ir = 0.0, ii = 0.0;
+        for (int t = 1; t <= h; ++t) {
+            const int idx = (t * q) % R;
+            rr += cs[idx] * sr[t];
+            ri += cs[idx] * si[t];
+            ir += sn[idx] * dr[t];
+            ii += sn[idx] * di[t];
+        }
+        // sign * i * (ir + i ii) = sign * (-ii + i ir)
+        const double ar = -sign * ii, ai = sign * ir;
+        out[q] = cd(rr + ar, ri + ai);
+        out[R - q] = cd(rr - ar, ri - ai);
+    }
+    for (int q = 0; q < R; ++q) v[q] = out[q];
+}
+
 struct Cfft {
+    struct Pass {
+        int R, ns, m;
+        std::vector<cd> tw;  // [k < ns][q = 1..R-1]: exp(sign 2 pi i q k / (ns R))
+    };
     int n = 0;
     int sign = -1;
-    std::vector<int> radix;
-    std::vector<cd> root;  // root[k] = exp(sign 2 pi i k / n)
+    std::vector<Pass> pass;
+    std::vector<cd> root;       // exp(sign 2 pi i k / n), generic radices
+    double cs[16][16], sn[16][16];  // per odd radix: cos/sin(2 pi m / R)
+
+    static cd polar_exact(long double num, long double den, int sign) {
+        const long double a = 2.0L * 3.141592653589793238462643383279502884L * num / den;
+        return cd(static_cast<double>(std::cos(a)), static_cast<double>(sign * std::sin(a)));
+    }
 
     Cfft(int n_, int sign_) : n(n_), sign(sign_) {
+        std::vector<int> radix;
         int m = n;
         while (m % 4 == 0) { radix.push_back(4); m /= 4; }
         while (m % 2 == 0) { radix.push_back(2); m /= 2; }
         for (int p = 3; m > 1; p += 2)
             while (m % p == 0) { radix.push_back(p); m /= p; }
         root.resize(n);
-        for (int k = 0; k < n; ++k) {
-            const long double a = 2.0L * 3.141592653589793238462643383279502884L *
-                                  static_cast<long double>(k) / static_cast<long double>(n);
-            root[k] = cd(static_cast<double>(std::cos(a)),
-                         static_cast<double>(sign * std::sin(a)));
+        for (int k = 0; k < n; ++k) root[k] = polar_exact(k, n, sign);
+        for (int R = 3; R < 16; R += 2)
+            for (int q = 0; q < R; ++q) {
+                const cd w = polar_exact(q, R, 1);
+                cs[R][q] = w.real();
+                sn[R][q] = w.imag();
+            }
+        int ns = 1;
+        for (int R : radix) {
+            Pass p;
+            p.R = R;
+            p.ns = ns;
+            p.m = n / R;
+            p.tw.resize(static_cast<size_t>(ns) * (R - 1));
+            for (int k = 0; k < ns; ++k)
+                for (int q = 1; q < R; ++q)
+                    p.tw[static_cast<size_t>(k) * (R - 1) + q - 1] =
+                        polar_exact(static_cast<long double>(q) * k, static_cast<long double>(ns) * R, sign);
+            pass.push_back(std::move(p));
+            ns *= R;
         }
+    }
+
+    template <int R>
+    void run_pass(const Pass &p, const cd *src, cd *dst) const {
+        const int m = p.m, ns = p.ns;
+        cd v[R > 0 ? R : 1];
+        for (int j0 = 0; j0 < m; j0 += ns) {
+            for (int k = 0; k < ns; ++k) {
+                const int j = j0 + k;
+                const cd *tw = p.tw.data() + static_cast<size_t>(k) * (R - 1);
+                v[0] = src[j];
+                for (int q = 1; q < R; ++q) v[q] = src[j + q * m] * tw[q - 1];
+                if (R == 2) {
+                    const cd a = v[0], b = v[1];
+                    v[0] = a + b;
+                    v[1] = a - b;
+                } else if (R == 4) {
+                    const cd a = v[0] + v[2], b = v[0] - v[2];
+                    const cd c = v[1] + v[3], d = v[1] - v[3];
+                    const cd di = sign < 0 ? cd(d.imag(), -d.real()) : cd(-d.imag(), d.real());
+                    v[0] = a + c;
+                    v[1] = b + di;
+                    v[2] = a - c;
+                    v[3] = b - di;
+                } else {
+                    bfly_odd<R>(v, cs[R], sn[R], sign);
+                }
+                cd *o = dst + j0 * R + k;
+                for (int q = 0; q < R; ++q) o[q * ns] = v[q];
+            }
+        }
+    }
+
+    void run_generic(const Pass &p, const cd *src, cd *dst) const {
+        const int R = p.R, m = p.m, ns = p.ns;
+        std::vector<cd> v(R), out(R);
+        for (int j0 = 0; j0 < m; j0 += ns)
+            for (int k = 0; k < ns; ++k) {
+                const int j = j0 + k;
+                const cd *tw = p.tw.data() + static_cast<size_t>(k) * (R - 1);
+                v[0] = src[j];
+                for (int q = 1; q < R; ++q) v[q] = src[j + q * m] * tw[q - 1];
+                for (int q = 0; q < R; ++q) {
+                    cd s = v[0];
+                    for (int t = 1; t < R; ++t)
+                        s += v[t] * root[(static_cast<long>(t) * q % R) * (n / R)];
+                    out[q] = s;
+                }
+                cd *o = dst + j0 * R + k;
+                for (int q = 0; q < R; ++q) o[q * ns] = out[q];
+            }
     }
 
     // Result in `data`; `work` has n elements of scratch.
     void run(cd *data, cd *work) const {
         if (n <= 1) return;
         cd *src = data, *dst = work;
-        int ns = 1;
-        cd vbuf[64], obuf[64];
-        std::vector<cd> big;
-        for (int r : radix) {
-            cd *vv = vbuf, *out = obuf;
-            if (r > 64) { big.resize(2 * static_cast<size_t>(r)); vv = big.data(); out = vv + r; }
-            const int m = n / r;
-            const int tstep = n / (ns * r);
-            for (int j = 0; j < m; ++j) {
-                const int k = j % ns;
-                for (int q = 0; q < r; ++q) {
-                    cd x = src[j + q * m];
-                    if (k) x *= root[(static_cast<long>(q) * k * tstep) % n];
-                    vv[q] = x;
-                }
-                if (r == 2) {
-                    out[0] = vv[0] + vv[1];
-                    out[1] = vv[0] - vv[1];
-                } else if (r == 4) {
-                    const cd a = vv[0] + vv[2], b = vv[0] - vv[2];
-                    const cd c = vv[1] + vv[3], d = vv[1] - vv[3];
-                    const cd di = sign < 0 ? cd(d.imag(), -d.real()) : cd(-d.imag(), d.real());
-                    out[0] = a + c;
-                    out[1] = b + di;
-                    out[2] = a - c;
-                    out[3] = b - di;
-                } else {
-                    const int step = n / r;
-                    for (int q = 0; q < r; ++q) {
-                        cd s = vv[0];
-                        for (int t = 1; t < r; ++t)
-                            s += vv[t] * root[(static_cast<long>(t) * q % r) * step];
-                        out[q] = s;
-                    }
-                }
-                const int base = (j / ns) * ns * r + k;
-                for (int q = 0; q < r; ++q) dst[base + q * ns] = out[q];
+        for (const Pass &p : pass) {
+            switch (p.R) {
+            case 2: run_pass<2>(p, src, dst); break;
+            case 3: run_pass<3>(p, src, dst); break;
+            case 4: run_pass<4>(p, src, dst); break;
+            case 5: run_pass<5>(p, src, dst); break;
+            case 7: run_pass<7>(p, src, dst); break;
+            case 11: run_pass<11>(p, src, dst); break;
+            case 13: run_pass<13>(p, src, dst); break;
+            default: run_generic(p, src, dst); break;
             }
             std::swap(src, dst);
-            ns *= r;
         }
         if (src != data) std::memcpy(data, src, sizeof(cd) * n);
     }
