@@ -72,6 +72,7 @@ _SIGNATURES = {
     "cdns_stage_name": [ctypes.c_int],
     "cdns_device_bytes": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t)],
     "cdns_get_stream": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)],
+    "cdns_debug_copy": [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t],
     "cdns_last_error": [ctypes.c_char_p, ctypes.c_size_t],
     "cdns_version": [],
 }
@@ -301,6 +302,17 @@ class Context:
         _check(lib().cdns_profile_end(self._h, _ptr(ms), ctypes.byref(steps)))
         names = [lib().cdns_stage_name(i).decode() for i in range(n)]
         return dict(zip(names, ms.tolist())), steps.value
+
+    def debug_buffer(self, which: int) -> np.ndarray:
+        """Stage buffer of the last nonlinear evaluation (see cdns_debug_copy)."""
+        m = self.mesh
+        nkz, ncy, nkx = m.spectral_shape
+        ny2 = m.NY2 + 1
+        shapes = {0: (6, ny2, nkz, nkx), 1: (6, ny2, m.NZ2, nkx), 2: (3, ny2, m.NZ2, nkx),
+                  3: (2, nkz, nkx)}
+        out = np.empty(shapes[which], dtype=np.complex128)
+        _check(lib().cdns_debug_copy(self._h, which, _ptr(out), out.size * 2))
+        return out
 
     def stream_ptr(self) -> int:
         s = ctypes.c_void_p()

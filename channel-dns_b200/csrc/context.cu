@@ -612,6 +612,25 @@ int cdns_profile_end(cdns_ctx *c, double *stage_ms, int *nsteps) {
 int cdns_stage_count(void) { return kStages; }
 const char *cdns_stage_name(int s) { return (s >= 0 && s < kStages) ? kStageNames[s] : ""; }
 
+int cdns_debug_copy(cdns_ctx *c, int which, double *out, size_t count) {
+    if (!c || !out) return fail(CDNS_ERR_ARG, "null argument");
+    DeviceGuard guard(c->device);
+    const Dims &d = c->d;
+    const void *src = nullptr;
+    size_t n = 0;
+    switch (which) {
+    case 0: src = c->F; n = 6 * (size_t)d.ny2 * d.ncol; break;
+    case 1: src = c->G; n = 6 * (size_t)d.ny2 * d.NZ2 * d.nkx; break;
+    case 2: src = c->H; n = 3 * (size_t)d.ny2 * d.NZ2 * d.nkx; break;
+    case 3: src = c->bw; n = 2 * (size_t)d.ncol; break;
+    default: return fail(CDNS_ERR_ARG, "unknown debug buffer");
+    }
+    if (count < 2 * n) return fail(CDNS_ERR_ARG, "debug buffer too small");
+    CK(cudaMemcpyAsync(out, src, n * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return CDNS_OK;
+}
+
 int cdns_get_stream(cdns_ctx *c, void **stream) {
     if (!c || !stream) return fail(CDNS_ERR_ARG, "null argument");
     *stream = (void *)c->stream;

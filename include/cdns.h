@@ -142,6 +142,14 @@ const char *cdns_stage_name(int stage);
  * own work or CUDA events against the step. */
 int cdns_get_stream(cdns_ctx *ctx, void **stream);
 
+/* Copy an intermediate stage buffer of the last nonlinear evaluation to the
+ * host, for stage-by-stage validation: which = 0 Chebyshev-synthesised
+ * fields [6][NY2+1][2*NZS+1][NXS+1], 1 z-physical fields
+ * [6][NY2+1][NZ2][NXS+1], 2 x-analysed products [3][NY2+1][NZ2][NXS+1]
+ * (complex), 3 vorticity wall sums [2][2*NZS+1][NXS+1].  `count` is the
+ * number of doubles the host buffer holds. */
+int cdns_debug_copy(cdns_ctx *ctx, int which, double *out, size_t count);
+
 /* Number of bytes of device memory the context holds. */
 int cdns_device_bytes(cdns_ctx *ctx, size_t *bytes);
 
