@@ -234,27 +234,30 @@ k_x_cross(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 *_
     __syncthreads();
     double2 *res = fft_lines<+1>(a, b, L, P, s_root);
     double2 *oth = (res == a) ? b : a;
-    // products, packed into 3 lines per pair of rows: (N0+iN1)_r, (N0+iN1)_{r+1}, (N2_r + i N2_{r+1})
-    const int L2 = 3 * ((RW + 1) / 2);
-    for (int i = threadIdx.x; i < n * RW; i += blockDim.x) {
-        const int x = i / RW, r = i - (i / RW) * RW;
-        const double2 p0 = res[x * L + 3 * r];
-        const double2 p1 = res[x * L + 3 * r + 1];
-        const double2 p2 = res[x * L + 3 * r + 2];
-        const double uu = p0.x, vv = p0.y, ww = p1.x, ox = p1.y, oy = p2.x, oz = p2.y;
-        const double n0 = vv * oz - ww * oy;
-        const double n1 = ww * ox - uu * oz;
-        const double n2 = uu * oy - vv * ox;
-        const int pr = r >> 1, odd = r & 1;
-        oth[x * L2 + 3 * pr + odd] = mk(n0, n1);
-        if (odd) oth[x * L2 + 3 * pr + 2].y = n2;
-        else oth[x * L2 + 3 * pr + 2].x = n2;
-    }
-    if (RW & 1) {  // odd row count: the last N2 line has no partner
-        for (int x = threadIdx.x; x < n; x += blockDim.x) {
-            oth[x * L2 + 3 * (RW / 2) + 1] = mk(0, 0);
-            oth[x * L2 + 3 * (RW / 2) + 2].y = 0.0;
+    // products, packed into 3 lines per pair of rows:
+    // (N0 + i N1)_r, (N0 + i N1)_{r+1}, (N2_r + i N2_{r+1}); one thread per
+    // (point, row pair) so every shared-memory element has a single writer.
+    const int npair = (RW + 1) / 2;
+    const int L2 = 3 * npair;
+    for (int i = threadIdx.x; i < n * npair; i += blockDim.x) {
+        const int x = i / npair, pr = i - (i / npair) * npair;
+        double n2[2] = {0.0, 0.0};
+        for (int odd = 0; odd < 2; ++odd) {
+            const int r = 2 * pr + odd;
+            if (r >= RW) {
+                oth[x * L2 + 3 * pr + odd] = mk(0, 0);
+                continue;
+            }
+            const double2 p0 = res[x * L + 3 * r];
+            const double2 p1 = res[x * L + 3 * r + 1];
+            const double2 p2 = res[x * L + 3 * r + 2];
+            const double uu = p0.x, vv = p0.y, ww = p1.x, ox = p1.y, oy = p2.x, oz = p2.y;
+            const double n0 = vv * oz - ww * oy;
+            const double n1 = ww * ox - uu * oz;
+            n2[odd] = uu * oy - vv * ox;
+            oth[x * L2 + 3 * pr + odd] = mk(n0, n1);
         }
+        oth[x * L2 + 3 * pr + 2] = mk(n2[0], n2[1]);
     }
     __syncthreads();
     double2 *res2 = fft_lines<-1>(oth, res, L2, P, s_root);

@@ -227,3 +227,23 @@ def test_bad_mesh_is_rejected():
     with pytest.raises(cdns.CdnsError) as e:
         cdns.Context(cdns.Mesh(16, 16, 16, 8, 14, 8, 12, 16, 24, 1.0, 1.0), cdns.Params(Re=1.0, DT=1e-3))
     assert e.value.code == 1
+
+
+def test_bitwise_determinism():
+    """Two evaluations of the same input are bit-identical (no kernel reads
+    stale or racing data): nonlinear term and three time steps."""
+    m, p = channel_case(32)
+    u0 = divergence_free_field(m, p, seed=2, amp=0.1, spectrum="k53", mean="loglaw")
+    c = ctx_for(m, p)
+    u = np.stack(u0, axis=-1)
+    N1, B1 = c.nonlinear(u)
+    for _ in range(3):
+        N2, B2 = c.nonlinear(u)
+        assert np.array_equal(N1, N2) and np.array_equal(B1, B2)
+    outs = []
+    for _ in range(2):
+        c.set_velocity(u)
+        c.run(1, 3)
+        c.synchronize()
+        outs.append((c.get_velocity(), c.get_pressure()))
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
