@@ -42,7 +42,9 @@ def build(verbose: bool = False, extra=None) -> str:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
         objs.append(obj)
-    cmd = [NVCC, *ARCH, "-shared", "-o", OUT, *objs, "-lcudart"]
+    # the CUDA runtime is linked statically: the library always runs on the
+    # runtime it was compiled against, whatever libcudart the host process loads
+    cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", "-o", OUT, *objs]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

@@ -308,6 +308,10 @@ class Context:
         m = self.mesh
         nkz, ncy, nkx = m.spectral_shape
         ny2 = m.NY2 + 1
+        if which == 4:
+            out = np.zeros(7)
+            _check(lib().cdns_debug_copy(self._h, 4, _ptr(out), 7))
+            return out
         shapes = {0: (6, ny2, nkz, nkx), 1: (6, ny2, m.NZ2, nkx), 2: (3, ny2, m.NZ2, nkx),
                   3: (2, nkz, nkx)}
         out = np.empty(shapes[which], dtype=np.complex128)

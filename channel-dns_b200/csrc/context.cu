@@ -623,6 +623,27 @@ int cdns_debug_copy(cdns_ctx *c, int which, double *out, size_t count) {
     case 1: src = c->G; n = 6 * (size_t)d.ny2 * d.NZ2 * d.nkx; break;
     case 2: src = c->H; n = 3 * (size_t)d.ny2 * d.NZ2 * d.nkx; break;
     case 3: src = c->bw; n = 2 * (size_t)d.ncol; break;
+    case 4: {
+        if (count < 7) return fail(CDNS_ERR_ARG, "debug buffer too small");
+        CK(cudaStreamSynchronize(c->stream));
+        auto nonfinite = [&](const void *p, size_t ndbl, double &out) -> int {
+            std::vector<double> h(ndbl);
+            CK(cudaMemcpy(h.data(), p, ndbl * sizeof(double), cudaMemcpyDeviceToHost));
+            size_t k = 0;
+            for (double v : h) k += !std::isfinite(v);
+            out = (double)k;
+            return CDNS_OK;
+        };
+        const SolverState &st = c->st;
+        const size_t Ns = (size_t)d.Ns, nc = d.ncol;
+        int r;
+        if ((r = nonfinite(st.ad_p, Ns, out[0])) || (r = nonfinite(st.ad_v, Ns, out[1])) ||
+            (r = nonfinite(st.inf_div, 8 * nc, out[2])) || (r = nonfinite(st.sigma0, 4 * nc, out[3])) ||
+            (r = nonfinite(st.p_inf, 4 * Ns, out[4])) || (r = nonfinite(st.v_b, 6 * Ns, out[5])) ||
+            (r = nonfinite(st.unit, 2 * (size_t)d.ncy + 2, out[6])))
+            return r;
+        return CDNS_OK;
+    }
     default: return fail(CDNS_ERR_ARG, "unknown debug buffer");
     }
     if (count < 2 * n) return fail(CDNS_ERR_ARG, "debug buffer too small");

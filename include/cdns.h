@@ -146,8 +146,10 @@ int cdns_get_stream(cdns_ctx *ctx, void **stream);
  * host, for stage-by-stage validation: which = 0 Chebyshev-synthesised
  * fields [6][NY2+1][2*NZS+1][NXS+1], 1 z-physical fields
  * [6][NY2+1][NZ2][NXS+1], 2 x-analysed products [3][NY2+1][NZ2][NXS+1]
- * (complex), 3 vorticity wall sums [2][2*NZS+1][NXS+1].  `count` is the
- * number of doubles the host buffer holds. */
+ * (complex), 3 vorticity wall sums [2][2*NZS+1][NXS+1], 4 solver state
+ * summary: per-array count of non-finite values (ad_p, ad_v, influence
+ * divergence, sigma0, influence fields, B-problem fields, unit responses)
+ * as 7 doubles.  `count` is the number of doubles the host buffer holds. */
 int cdns_debug_copy(cdns_ctx *ctx, int which, double *out, size_t count);
 
 /* Number of bytes of device memory the context holds. */
