@@ -73,6 +73,8 @@ _SIGNATURES = {
     "cdns_device_bytes": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t)],
     "cdns_get_stream": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)],
     "cdns_debug_copy": [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t],
+    "cdns_transform_fine_backward_noalloc": [ctypes.POINTER(MeshDesc), ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_void_p],
     "cdns_last_error": [ctypes.c_char_p, ctypes.c_size_t],
     "cdns_version": [],
 }
@@ -327,6 +329,15 @@ class Context:
         b = ctypes.c_size_t(0)
         _check(lib().cdns_device_bytes(self._h, ctypes.byref(b)))
         return int(b.value)
+
+
+def fine_backward_noalloc(mesh: Mesh, spectral_ptr: int, physical_ptr: int, stream: int = 0) -> None:
+    """Allocation-free fine backward transform on caller-owned device buffers
+    (cdns_transform_fine_backward_noalloc); queued on ``stream``, not waited for."""
+    md = mesh.desc()
+    _check(lib().cdns_transform_fine_backward_noalloc(ctypes.byref(md), ctypes.c_void_p(spectral_ptr),
+                                                      ctypes.c_void_p(physical_ptr),
+                                                      ctypes.c_void_p(stream)))
 
 
 def version() -> str:

@@ -69,6 +69,9 @@ cudaError_t configure_solver_kernels(const Dims &d);
 void launch_pressure_bc(const Dims &d, const double2 *N, const double2 *bw, double2 *B,
                         cudaStream_t s);
 
+// ---- context.cu ----
+int record_error(int code, const char *msg);
+
 // ---- layout.cu ----
 void launch_deinterleave(const double2 *src, double2 *dst, long long n, int nc, cudaStream_t s);
 void launch_interleave(const double2 *src, double2 *dst, long long n, int nc, cudaStream_t s);

@@ -21,6 +21,18 @@ int fail(int code, const std::string &msg) {
     g_error = msg;
     return code;
 }
+}  // namespace
+
+namespace cdns {
+// Records the calling thread's last error for cdns_last_error (used by
+// entry points defined in other translation units).
+int record_error(int code, const char *msg) {
+    g_error = msg ? msg : "";
+    return code;
+}
+}  // namespace cdns
+
+namespace {
 
 #define CK(call)                                                                          \
     do {                                                                                  \

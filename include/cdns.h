@@ -120,6 +120,24 @@ int cdns_nonlinear(cdns_ctx *ctx, const double *velocity, double *nonlinear, dou
  * 'F': physical -> spectral. */
 int cdns_transform_fine(cdns_ctx *ctx, int direction, const double *in, double *out);
 
+/* The fine-grid backward transform of cdns_transform_fine ('B': spectral ->
+ * physical, one scalar field) for callers that cannot allocate device
+ * memory -- code that runs under a caller-owned memory pool or inside an
+ * embedding framework that forbids or intercepts cudaMalloc.  No counterpart
+ * in the reference.  `spectral` [2*NZS+1][NYS+1][NXS+1] (complex) and
+ * `physical` [NZ2][NY2+1][NX2] are device pointers on the current device;
+ * the work is queued on `stream` (a cudaStream_t, NULL for the default
+ * stream) and the call returns without waiting.  No context is needed.
+ * Intermediate buffers and tables live in one 32 MiB array in device memory
+ * that the library holds on every GPU that loads it (product grids up to
+ * about 96^3); larger meshes are rejected with CDNS_ERR_ARG.  The first call
+ * on each device looks up that array's address, so make it before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * (different streams, threads or devices' streams running at once on one
+ * device) race and must be serialised by the caller. */
+int cdns_transform_fine_backward_noalloc(const cdns_mesh_desc *mesh, const double *spectral,
+                                         double *physical, void *stream);
+
 /* EqSolvePV::setup(g) followed by the fused solve (solve_modes with fused
  * RHS divergence and sigma correction, src/solver/eqsolve_pv.cpp:311-450)
  * of a given velocity RHS [..][3], pressure wall data [..][2][..] and velocity
