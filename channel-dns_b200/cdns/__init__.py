@@ -314,8 +314,13 @@ class Context:
             out = np.zeros(7)
             _check(lib().cdns_debug_copy(self._h, 4, _ptr(out), 7))
             return out
+        if which == 9:
+            out = np.zeros((2, nkz, nkx))
+            _check(lib().cdns_debug_copy(self._h, 9, _ptr(out), out.size * 2))
+            return out
         shapes = {0: (6, ny2, nkz, nkx), 1: (6, ny2, m.NZ2, nkx), 2: (3, ny2, m.NZ2, nkx),
-                  3: (2, nkz, nkx)}
+                  3: (2, nkz, nkx), 5: (2, 2, nkz, nkx), 6: (2, 3, nkz, ncy, nkx),
+                  7: (2, nkz, ncy, nkx), 8: (2, nkz, nkx)}
         out = np.empty(shapes[which], dtype=np.complex128)
         _check(lib().cdns_debug_copy(self._h, which, _ptr(out), out.size * 2))
         return out

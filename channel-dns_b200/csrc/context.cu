@@ -656,9 +656,20 @@ int cdns_debug_copy(cdns_ctx *c, int which, double *out, size_t count) {
             return r;
         return CDNS_OK;
     }
+    case 5: src = c->st.inf_div; n = 4 * (size_t)d.ncol; break;
+    case 6: src = c->st.v_inf; n = 6 * (size_t)d.Ns; break;
+    case 7: src = c->st.p_inf; n = 2 * (size_t)d.Ns; break;
+    case 8: src = c->st.sigma0; n = 2 * (size_t)d.ncol; break;
+    case 9: src = c->st.wn_p; n = (size_t)d.ncol; break;   // wn_p then wn_v as [2][ncol] doubles
     default: return fail(CDNS_ERR_ARG, "unknown debug buffer");
     }
     if (count < 2 * n) return fail(CDNS_ERR_ARG, "debug buffer too small");
+    if (which == 9) {
+        CK(cudaMemcpyAsync(out, c->st.wn_p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(out + n, c->st.wn_v, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        return CDNS_OK;
+    }
     CK(cudaMemcpyAsync(out, src, n * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return CDNS_OK;

@@ -167,7 +167,11 @@ int cdns_get_stream(cdns_ctx *ctx, void **stream);
  * (complex), 3 vorticity wall sums [2][2*NZS+1][NXS+1], 4 solver state
  * summary: per-array count of non-finite values (ad_p, ad_v, influence
  * divergence, sigma0, influence fields, B-problem fields, unit responses)
- * as 7 doubles.  `count` is the number of doubles the host buffer holds. */
+ * as 7 doubles, 5 normalised influence divergence [2][2][2*NZS+1][NXS+1], 6
+ * influence velocities [2][3][..spectral..], 7 influence pressures
+ * [2][..spectral..], 8 sigma0 [2][2*NZS+1][NXS+1] (complex), 9 the diagonals
+ * wn of the pressure and velocity problems [2][2*NZS+1][NXS+1] (real).
+ * `count` is the number of doubles the host buffer holds. */
 int cdns_debug_copy(cdns_ctx *ctx, int which, double *out, size_t count);
 
 /* Number of bytes of device memory the context holds. */
