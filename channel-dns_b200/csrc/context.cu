@@ -100,7 +100,10 @@ struct cdns_ctx {
         const size_t b = sizeof(T) * (count ? count : 1);
         cudaError_t e = cudaMalloc(&p, b);
         if (e != cudaSuccess) return fail(CDNS_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-        e = cudaMemset(p, 0, b);
+        // Zero on the context stream: a cudaMemset on the legacy default stream
+        // is not ordered against this non-blocking stream and could land after
+        // the kernels that fill the buffer.
+        e = cudaMemsetAsync(p, 0, b, stream);
         if (e != cudaSuccess) return fail(CDNS_ERR_CUDA, cudaGetErrorString(e));
         allocs.push_back(p);
         bytes += b;
@@ -472,9 +475,11 @@ int cdns_synchronize(cdns_ctx *c) {
     DeviceGuard guard(c->device);
     CK(cudaStreamSynchronize(c->stream));
     unsigned e = 0;
-    CK(cudaMemcpy(&e, c->err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpyAsync(&e, c->err, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
     if (e) {
-        CK(cudaMemset(c->err, 0, sizeof(unsigned)));
+        CK(cudaMemsetAsync(c->err, 0, sizeof(unsigned), c->stream));
+        CK(cudaStreamSynchronize(c->stream));
         if (e & ERR_NONFINITE) return fail(CDNS_ERR_NONFINITE, "non-finite value in the step output");
         return fail(CDNS_ERR_PIVOT, "zero or non-finite tau pivot or flow response");
     }
@@ -640,7 +645,8 @@ int cdns_debug_copy(cdns_ctx *c, int which, double *out, size_t count) {
         CK(cudaStreamSynchronize(c->stream));
         auto nonfinite = [&](const void *p, size_t ndbl, double &out) -> int {
             std::vector<double> h(ndbl);
-            CK(cudaMemcpy(h.data(), p, ndbl * sizeof(double), cudaMemcpyDeviceToHost));
+            CK(cudaMemcpyAsync(h.data(), p, ndbl * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaStreamSynchronize(c->stream));
             size_t k = 0;
             for (double v : h) k += !std::isfinite(v);
             out = (double)k;
