@@ -1,11 +1,17 @@
-// Batched complex FFT of interleaved lines in shared memory.
+// Batched complex FFT of interleaved lines for sm_100a.
 //
 // L lines of length n are stored interleaved: element (pos, line) sits at
 // buf[pos*L + line], so a warp's lanes touch consecutive 16-byte words in
-// every pass (no bank conflicts).  The transform is an iterative mixed-radix
-// Stockham autosort FFT (radix 4, 2, 3, 5, 7, and a direct DFT for other
-// small primes) that ping-pongs between two buffers; it is unnormalised with
-// the FFTW sign convention: SIGN=-1 forward, SIGN=+1 backward.
+// every pass.  The transform is an iterative mixed-radix Stockham autosort
+// FFT, unnormalised, with the FFTW sign convention (SIGN=-1 forward, +1
+// backward).  Every pass is instantiated for its radix at compile time
+// (radix 2, 3, 4, 5, 7 with literal twiddle constants; other odd radices up
+// to 13 from the root table), so the R values of a butterfly stay in
+// registers.  Two drivers:
+//   fft_lines  shared memory in, shared memory out (ping-pong buffers);
+//   fft_run    the first pass reads through a source functor and the last
+//              pass writes through a destination functor (global memory),
+//              middle passes ping-pong in shared memory.
 #pragma once
 
 #include "cdns_common.cuh"
@@ -15,101 +21,182 @@ namespace cdns {
 constexpr int kMaxRadix = 16;
 
 // roots[k] = exp(-2 pi i k / n); SIGN=+1 uses the conjugate.
-template <int SIGN> __device__ inline double2 root_of(const double2 *roots, int k) {
+template <int SIGN> __device__ __forceinline__ double2 root_of(const double2 *roots, int k) {
     const double2 r = roots[k];
     return SIGN < 0 ? r : mk(r.x, -r.y);
 }
 
-template <int SIGN>
-__device__ inline void dft_small(double2 *v, int R, const double2 *roots, int n) {
-    if (R == 2) {
+// cos / sin (2 pi i / R) for 0 <= i < R, folded to literals after unrolling.
+template <int R> __device__ __forceinline__ double kcos(int i);
+template <int R> __device__ __forceinline__ double ksin(int i);
+template <> __device__ __forceinline__ double kcos<3>(int i) { return i == 0 ? 1.0 : -0.5; }
+template <> __device__ __forceinline__ double ksin<3>(int i) {
+    return i == 0 ? 0.0 : (i == 1 ? 0.8660254037844386 : -0.8660254037844386);
+}
+template <> __device__ __forceinline__ double kcos<5>(int i) {
+    const int a = i <= 2 ? i : 5 - i;
+    return a == 0 ? 1.0 : (a == 1 ? 0.30901699437494745 : -0.8090169943749475);
+}
+template <> __device__ __forceinline__ double ksin<5>(int i) {
+    const int a = i <= 2 ? i : 5 - i;
+    const double s = a == 0 ? 0.0 : (a == 1 ? 0.9510565162951535 : 0.5877852522924731);
+    return i <= 2 ? s : -s;
+}
+template <> __device__ __forceinline__ double kcos<7>(int i) {
+    const int a = i <= 3 ? i : 7 - i;
+    return a == 0 ? 1.0 : (a == 1 ? 0.6234898018587335 : (a == 2 ? -0.2225209339563144 : -0.9009688679024191));
+}
+template <> __device__ __forceinline__ double ksin<7>(int i) {
+    const int a = i <= 3 ? i : 7 - i;
+    const double s = a == 0 ? 0.0 : (a == 1 ? 0.7818314824680298 : (a == 2 ? 0.9749279121818236 : 0.4338837391175581));
+    return i <= 3 ? s : -s;
+}
+
+// Odd radix by symmetric pairs: with s_t = x_t + x_{R-t}, d_t = x_t - x_{R-t},
+// y_q = x_0 + sum_t s_t cos(2 pi t q/R) + SIGN i sum_t d_t sin(2 pi t q/R),
+// y_{R-q} the same with the sine term negated.
+template <int R, int SIGN, bool TABLE>
+__device__ __forceinline__ void bfly_odd(double2 (&v)[R], const double2 *roots, int n) {
+    constexpr int h = R / 2;
+    double2 s[h + 1], d[h + 1];
+#pragma unroll
+    for (int t = 1; t <= h; ++t) {
+        s[t] = cadd(v[t], v[R - t]);
+        d[t] = csub(v[t], v[R - t]);
+    }
+    double2 out[R];
+    double2 y0 = v[0];
+#pragma unroll
+    for (int t = 1; t <= h; ++t) y0 = cadd(y0, s[t]);
+    out[0] = y0;
+#pragma unroll
+    for (int q = 1; q <= h; ++q) {
+        double2 re = v[0], im = mk(0.0, 0.0);
+#pragma unroll
+        for (int t = 1; t <= h; ++t) {
+            const int i = (t * q) % R;
+            double c, sn;
+            if constexpr (TABLE) {
+                const double2 w = roots[i * (n / R)];  // exp(-2 pi i i/R)
+                c = w.x;
+                sn = -w.y;
+            } else {
+                c = kcos<R>(i);
+                sn = ksin<R>(i);
+            }
+            re.x += c * s[t].x;
+            re.y += c * s[t].y;
+            im.x += sn * d[t].x;
+            im.y += sn * d[t].y;
+        }
+        const double2 iim = SIGN < 0 ? mk(im.y, -im.x) : mk(-im.y, im.x);
+        out[q] = cadd(re, iim);
+        out[R - q] = csub(re, iim);
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) v[q] = out[q];
+}
+
+template <int R, int SIGN>
+__device__ __forceinline__ void bfly(double2 (&v)[R], const double2 *roots, int n) {
+    if constexpr (R == 1) {
+        return;
+    } else if constexpr (R == 2) {
         const double2 a = v[0], b = v[1];
         v[0] = cadd(a, b);
         v[1] = csub(a, b);
-        return;
-    }
-    if (R == 4) {
+    } else if constexpr (R == 4) {
         const double2 a = cadd(v[0], v[2]), b = csub(v[0], v[2]);
         const double2 c = cadd(v[1], v[3]), d = csub(v[1], v[3]);
-        // SIGN*i*d
-        const double2 di = SIGN < 0 ? mk(d.y, -d.x) : mk(-d.y, d.x);
+        const double2 di = SIGN < 0 ? mk(d.y, -d.x) : mk(-d.y, d.x);  // SIGN i d
         v[0] = cadd(a, c);
         v[1] = cadd(b, di);
         v[2] = csub(a, c);
         v[3] = csub(b, di);
-        return;
+    } else if constexpr (R == 3 || R == 5 || R == 7) {
+        bfly_odd<R, SIGN, false>(v, roots, n);
+    } else {
+        bfly_odd<R, SIGN, true>(v, roots, n);
     }
-    if (R == 3) {
-        // y0 = a+b+c ; y1,2 = a - (b+c)/2 +- SIGN*i*(sqrt3/2)(b-c)
-        const double s3 = 0.86602540378443864676;
-        const double2 t = cadd(v[1], v[2]);
-        const double2 d = csub(v[1], v[2]);
-        const double2 m = mk(v[0].x - 0.5 * t.x, v[0].y - 0.5 * t.y);
-        const double2 r = SIGN < 0 ? mk(s3 * d.y, -s3 * d.x) : mk(-s3 * d.y, s3 * d.x);
-        v[0] = cadd(v[0], t);
-        v[1] = cadd(m, r);
-        v[2] = csub(m, r);
-        return;
-    }
-    // Odd R: pair terms t and R-t (real parts share cosines, imaginary parts
-    // share sines), halving the multiplications of a direct DFT.
-    double2 out[kMaxRadix];
-    const int step = n / R;
-    const int h = R / 2;
-    double2 s[kMaxRadix / 2 + 1], dd[kMaxRadix / 2 + 1];
-    for (int t = 1; t <= h; ++t) {
-        s[t] = cadd(v[t], v[R - t]);
-        dd[t] = csub(v[t], v[R - t]);
-    }
-    double2 y0 = v[0];
-    for (int t = 1; t <= h; ++t) y0 = cadd(y0, s[t]);
-    out[0] = y0;
-    for (int q = 1; q <= h; ++q) {
-        double2 re = v[0];
-        double2 im = mk(0.0, 0.0);
-        for (int t = 1; t <= h; ++t) {
-            const double2 w = roots[((t * q) % R) * step];  // exp(-2 pi i tq/R)
-            re.x += w.x * s[t].x;
-            re.y += w.x * s[t].y;
-            im.x += w.y * dd[t].x;
-            im.y += w.y * dd[t].y;
-        }
-        // forward: y_q = re + i*im_part, where sum w.y*dd carries sin(-..)
-        // term i*(w.y)*dd ; backward flips the sign of the sine.
-        const double2 iim = SIGN < 0 ? mk(-im.y, im.x) : mk(im.y, -im.x);
-        out[q] = cadd(re, iim);
-        out[R - q] = csub(re, iim);
-    }
-    for (int q = 0; q < R; ++q) v[q] = out[q];
 }
 
-// Runs all passes; returns the buffer holding the result (a or b).  Every
-// thread of the block must call it (it synchronises between passes).
+// Source / destination functors over interleaved shared-memory lines.
+struct SmemSrc {
+    const double2 *buf;
+    int L;
+    __device__ __forceinline__ double2 operator()(int pos, int line) const { return buf[pos * L + line]; }
+};
+struct SmemDst {
+    double2 *buf;
+    int L;
+    __device__ __forceinline__ void operator()(int pos, int line, double2 v) const { buf[pos * L + line] = v; }
+};
+
+// One Stockham pass of radix R over L lines: span ns (product of the radices
+// already applied).  Each work item (j, line) reads R inputs at stride n/R,
+// twiddles them by w^(q k), k = j mod ns, and writes R outputs at stride ns.
+template <int R, int SIGN, class Src, class Dst>
+__device__ __forceinline__ void pass_ct(int n, int L, int ns, const double2 *roots, const Src &src,
+                                        const Dst &dst) {
+    const int m = n / R;
+    const int tstep = n / (ns * R);
+    const int total = m * L;
+    for (int w = threadIdx.x; w < total; w += blockDim.x) {
+        const int j = w / L;
+        const int line = w - j * L;
+        const int k = j % ns;
+        double2 v[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) v[q] = src(j + q * m, line);
+        if (k) {
+#pragma unroll
+            for (int q = 1; q < R; ++q) v[q] = cmul(v[q], root_of<SIGN>(roots, q * k * tstep));
+        }
+        bfly<R, SIGN>(v, roots, n);
+        const int base = (j / ns) * ns * R + k;
+#pragma unroll
+        for (int q = 0; q < R; ++q) dst(base + q * ns, line, v[q]);
+    }
+}
+
+// Radices 9, 11 and 13 (meshes outside the usual 2^a 3^b 5^c 7^d sizes) run in
+// a separate non-inlined function so that they do not raise the register
+// budget of the kernels that use the common radices.
+template <int SIGN, class Src, class Dst>
+__device__ __noinline__ void pass_rare(int R, int n, int L, int ns, const double2 *roots,
+                                       const Src &src, const Dst &dst) {
+    switch (R) {
+    case 9: pass_ct<9, SIGN>(n, L, ns, roots, src, dst); break;
+    case 11: pass_ct<11, SIGN>(n, L, ns, roots, src, dst); break;
+    case 13: pass_ct<13, SIGN>(n, L, ns, roots, src, dst); break;
+    default: break;  // plans only hold radices 2, 3, 4, 5, 7, 9, 11, 13
+    }
+}
+
+template <int SIGN, class Src, class Dst>
+__device__ __forceinline__ void pass_dispatch(int R, int n, int L, int ns, const double2 *roots,
+                                              const Src &src, const Dst &dst) {
+    switch (R) {
+    case 1: pass_ct<1, SIGN>(n, L, ns, roots, src, dst); break;
+    case 2: pass_ct<2, SIGN>(n, L, ns, roots, src, dst); break;
+    case 3: pass_ct<3, SIGN>(n, L, ns, roots, src, dst); break;
+    case 4: pass_ct<4, SIGN>(n, L, ns, roots, src, dst); break;
+    case 5: pass_ct<5, SIGN>(n, L, ns, roots, src, dst); break;
+    case 7: pass_ct<7, SIGN>(n, L, ns, roots, src, dst); break;
+    default: pass_rare<SIGN>(R, n, L, ns, roots, src, dst); break;
+    }
+}
+
+// Shared memory in and out; returns the buffer holding the result (a or b).
+// Every thread of the block must call it (it synchronises between passes).
 template <int SIGN>
-__device__ double2 *fft_lines(double2 *a, double2 *b, int L, const FftPlan &P,
-                              const double2 *roots) {
+__device__ double2 *fft_lines(double2 *a, double2 *b, int L, const FftPlan &P, const double2 *roots) {
     const int n = P.n;
     double2 *src = a, *dst = b;
     int ns = 1;
     for (int p = 0; p < P.nrad; ++p) {
         const int R = P.radix[p];
-        const int m = n / R;
-        const int tstep = n / (ns * R);
-        const int work = m * L;
-        for (int w = threadIdx.x; w < work; w += blockDim.x) {
-            const int line = w % L;
-            const int j = w / L;
-            const int k = j % ns;
-            double2 v[kMaxRadix];
-            for (int q = 0; q < R; ++q) {
-                double2 x = src[(j + q * m) * L + line];
-                if (k) x = cmul(x, root_of<SIGN>(roots, q * k * tstep));
-                v[q] = x;
-            }
-            dft_small<SIGN>(v, R, roots, n);
-            const int base = (j / ns) * ns * R + k;
-            for (int q = 0; q < R; ++q) dst[(base + q * ns) * L + line] = v[q];
-        }
+        pass_dispatch<SIGN>(R, n, L, ns, roots, SmemSrc{src, L}, SmemDst{dst, L});
         __syncthreads();
         double2 *t = src;
         src = dst;
@@ -117,6 +204,32 @@ __device__ double2 *fft_lines(double2 *a, double2 *b, int L, const FftPlan &P,
         ns *= R;
     }
     return src;
+}
+
+// First pass reads through `gsrc(pos, line)`, last pass writes through
+// `gdst(pos, line, value)`; middle passes ping-pong between a and b.
+template <int SIGN, class GSrc, class GDst>
+__device__ void fft_run(double2 *a, double2 *b, int L, const FftPlan &P, const double2 *roots,
+                        const GSrc &gsrc, const GDst &gdst) {
+    const int n = P.n;
+    if (P.nrad <= 1) {
+        pass_dispatch<SIGN>(P.nrad == 1 ? P.radix[0] : 1, n, L, 1, roots, gsrc, gdst);
+        return;
+    }
+    int ns = 1;
+    pass_dispatch<SIGN>(P.radix[0], n, L, ns, roots, gsrc, SmemDst{a, L});
+    __syncthreads();
+    ns *= P.radix[0];
+    double2 *cur = a, *oth = b;
+    for (int p = 1; p < P.nrad - 1; ++p) {
+        pass_dispatch<SIGN>(P.radix[p], n, L, ns, roots, SmemSrc{cur, L}, SmemDst{oth, L});
+        __syncthreads();
+        double2 *t = cur;
+        cur = oth;
+        oth = t;
+        ns *= P.radix[p];
+    }
+    pass_dispatch<SIGN>(P.radix[P.nrad - 1], n, L, ns, roots, SmemSrc{cur, L}, gdst);
 }
 
 }  // namespace cdns

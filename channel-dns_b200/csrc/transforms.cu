@@ -145,10 +145,55 @@ k_curl_ysynth(Dims d, Tables t, const double2 *__restrict__ u, double2 *__restri
 
 // ---------------------------------------------------------------------------
 // K2: inverse z FFT.  Block = one (field, y point) plane x TL kx lines.  The
-// kz in [-NZS, NZS] coefficients are expanded into the NZ2 slots (negative
-// Nyquist slot wins at a full z spectrum, src/fft/transforms.cpp:715-732).
+// first Stockham pass reads the kz in [-NZS, NZS] coefficients straight from
+// HBM into the NZ2 slots (negative Nyquist slot wins at a full z spectrum,
+// src/fft/transforms.cpp:715-732); the last pass writes z-physical rows.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128)
+struct ZExpandSrc {
+    const double2 *Fp;   // one (field, y point) plane [kz][kx]
+    int nkx, kx0, NZS, n;
+    __device__ __forceinline__ double2 operator()(int z, int line) const {
+        const int kx = kx0 + line;
+        if (kx >= nkx) return mk(0, 0);
+        int kz;
+        if (z <= NZS) kz = (z == n - NZS) ? -NZS : z;
+        else if (z >= n - NZS) kz = z - n;
+        else return mk(0, 0);
+        return Fp[(kz + NZS) * nkx + kx];
+    }
+};
+struct RowDst {
+    double2 *p;   // [pos][kx]
+    int nkx, kx0;
+    __device__ __forceinline__ void operator()(int pos, int line, double2 v) const {
+        const int kx = kx0 + line;
+        if (kx < nkx) p[(long long)pos * nkx + kx] = v;
+    }
+};
+struct RowSrc {
+    const double2 *p;
+    int nkx, kx0;
+    __device__ __forceinline__ double2 operator()(int pos, int line) const {
+        const int kx = kx0 + line;
+        return kx < nkx ? p[(long long)pos * nkx + kx] : mk(0, 0);
+    }
+};
+// Forward z: keep kz in [-NZS, NZS] scaled by 1/NZ2 (src/fft/transforms.cpp:658-665);
+// at a full z spectrum slot NZS feeds both kz = +NZS and kz = -NZS.
+struct ZTruncDst {
+    double2 *Fp;
+    int nkx, kx0, NZS, n;
+    double invn;
+    __device__ __forceinline__ void operator()(int z, int line, double2 v) const {
+        const int kx = kx0 + line;
+        if (kx >= nkx) return;
+        const double2 s = cscale(invn, v);
+        if (z <= NZS) Fp[(z + NZS) * nkx + kx] = s;
+        if (z >= n - NZS) Fp[(z - n + NZS) * nkx + kx] = s;
+    }
+};
+
+__global__ void __launch_bounds__(256, 2)
 k_z_backward(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 *__restrict__ F,
              double2 *__restrict__ G, int TL) {
     extern __shared__ double2 sm[];
@@ -158,35 +203,26 @@ k_z_backward(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2
     double2 *b = a + n * TL;
     const int f = blockIdx.z, j = blockIdx.y, kx0 = blockIdx.x * TL;
     for (int i = threadIdx.x; i < n; i += blockDim.x) s_root[i] = roots[i];
-    const double2 *Fp = F + ((long long)f * d.ny2 + j) * d.ncol;
-    for (int i = threadIdx.x; i < n * TL; i += blockDim.x) {
-        const int z = i / TL, line = i - (i / TL) * TL;
-        const int kx = kx0 + line;
-        int kz;
-        bool keep;
-        if (z <= d.NZS) {
-            kz = z;
-            keep = true;
-            if (z == n - d.NZS) kz = -d.NZS;  // full z spectrum: negative Nyquist wins
-        } else if (z >= n - d.NZS) {
-            kz = z - n;
-            keep = true;
-        } else {
-            kz = 0;
-            keep = false;
-        }
-        double2 v = mk(0, 0);
-        if (keep && kx < d.nkx) v = Fp[(kz + d.NZS) * d.nkx + kx];
-        a[i] = v;
-    }
     __syncthreads();
-    const double2 *res = fft_lines<+1>(a, b, TL, P, s_root);
-    double2 *Gp = G + ((long long)f * d.ny2 + j) * (long long)n * d.nkx;
-    for (int i = threadIdx.x; i < n * TL; i += blockDim.x) {
-        const int z = i / TL, line = i - (i / TL) * TL;
-        const int kx = kx0 + line;
-        if (kx < d.nkx) Gp[(long long)z * d.nkx + kx] = res[i];
-    }
+    const ZExpandSrc src{F + ((long long)f * d.ny2 + j) * d.ncol, d.nkx, kx0, d.NZS, n};
+    const RowDst dst{G + ((long long)f * d.ny2 + j) * (long long)n * d.nkx, d.nkx, kx0};
+    fft_run<+1>(a, b, TL, P, s_root, src, dst);
+}
+
+__global__ void __launch_bounds__(256, 2)
+k_z_forward(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 *__restrict__ H,
+            double2 *__restrict__ F, int TL) {
+    extern __shared__ double2 sm[];
+    const int n = d.NZ2;
+    double2 *s_root = sm;
+    double2 *a = sm + n;
+    double2 *b = a + n * TL;
+    const int f = blockIdx.z, j = blockIdx.y, kx0 = blockIdx.x * TL;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s_root[i] = roots[i];
+    __syncthreads();
+    const RowSrc src{H + ((long long)f * d.ny2 + j) * (long long)n * d.nkx, d.nkx, kx0};
+    const ZTruncDst dst{F + ((long long)f * d.ny2 + j) * d.ncol, d.nkx, kx0, d.NZS, n, 1.0 / (double)n};
+    fft_run<-1>(a, b, TL, P, s_root, src, dst);
 }
 
 // ---------------------------------------------------------------------------
@@ -194,9 +230,10 @@ k_z_backward(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2
 // products.  Block = RW rows (z, j); real rows are packed in pairs into one
 // complex line (a + i b); c2r drops the imaginary parts of the DC and Nyquist
 // bins as FFTW does.  Products: N = u x omega (src/solver/vector_ops.cpp:263-269),
-// packed as (N0 + i N1) and (N2 of row r + i N2 of row r+1).
+// packed as (N0 + i N1) and (N2 of row r + i N2 of row r+1).  Loads and stores
+// run along kx so that a warp touches contiguous HBM.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 2)
 k_x_cross(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 *__restrict__ G,
           double2 *__restrict__ H, int RW) {
     extern __shared__ double2 sm[];
@@ -210,32 +247,35 @@ k_x_cross(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 *_
     const long long fstride = (long long)d.ny2 * d.NZ2 * d.nkx;
     const double2 *Gj = G + (long long)j * d.NZ2 * d.nkx;
     const int nyq = (n % 2 == 0) ? n / 2 : -1;
-    for (int i = threadIdx.x; i < n * L; i += blockDim.x) {
-        const int k = i / L, line = i - (i / L) * L;
+    const int nkx = d.nkx;
+    // zero band between the retained modes and their mirrors
+    const int zlo = d.NXS + 1, zhi = n - d.NXS;  // slots [zlo, zhi) are zero
+    for (int i = threadIdx.x; i < (zhi - zlo) * L; i += blockDim.x) {
+        const int k = zlo + i / L, line = i - (i / L) * L;
+        a[k * L + line] = mk(0, 0);
+    }
+    // retained modes and their Hermitian mirrors, one (row, pair, kx) per thread
+    for (int i = threadIdx.x; i < L * nkx; i += blockDim.x) {
+        const int line = i / nkx, m = i - (i / nkx) * nkx;
         const int r = line / 3, p = line - (line / 3) * 3;
         const int z = z0 + r;
-        double2 v = mk(0, 0);
+        double2 A = mk(0, 0), B = mk(0, 0);
         if (z < d.NZ2) {
-            int m;
-            bool mirror;
-            if (k <= d.NXS) { m = k; mirror = false; }
-            else if (k >= n - d.NXS && k != nyq) { m = n - k; mirror = true; }
-            else { m = -1; mirror = false; }
-            if (m >= 0) {
-                const double2 *row = Gj + (long long)z * d.nkx + m;
-                double2 A = row[(2 * p) * fstride];
-                double2 B = row[(2 * p + 1) * fstride];
-                if (m == 0 || m == nyq) { A.y = 0.0; B.y = 0.0; }
-                v = mirror ? mk(A.x + B.y, B.x - A.y) : mk(A.x - B.y, A.y + B.x);
-            }
+            const double2 *row = Gj + (long long)z * nkx + m;
+            A = row[(2 * p) * fstride];
+            B = row[(2 * p + 1) * fstride];
         }
-        a[i] = v;
+        if (m == 0 || m == nyq) {
+            A.y = 0.0;
+            B.y = 0.0;
+        }
+        a[m * L + line] = mk(A.x - B.y, A.y + B.x);
+        if (m != 0 && m != nyq) a[(n - m) * L + line] = mk(A.x + B.y, B.x - A.y);
     }
     __syncthreads();
     double2 *res = fft_lines<+1>(a, b, L, P, s_root);
     double2 *oth = (res == a) ? b : a;
-    // products, packed into 3 lines per pair of rows:
-    // (N0 + i N1)_r, (N0 + i N1)_{r+1}, (N2_r + i N2_{r+1}); one thread per
+    // products, packed into 3 lines per pair of rows; one thread per
     // (point, row pair) so every shared-memory element has a single writer.
     const int npair = (RW + 1) / 2;
     const int L2 = 3 * npair;
@@ -262,10 +302,9 @@ k_x_cross(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 *_
     __syncthreads();
     double2 *res2 = fft_lines<-1>(oth, res, L2, P, s_root);
     const double invn = 1.0 / (double)n;
-    for (int i = threadIdx.x; i < d.nkx * RW * 3; i += blockDim.x) {
-        const int k = i / (RW * 3);
-        const int rem = i - k * (RW * 3);
-        const int r = rem / 3, f = rem - (rem / 3) * 3;
+    for (int i = threadIdx.x; i < RW * 3 * nkx; i += blockDim.x) {
+        const int rf = i / nkx, k = i - (i / nkx) * nkx;
+        const int r = rf / 3, f = rf - (rf / 3) * 3;
         const int z = z0 + r;
         if (z >= d.NZ2) continue;
         const int km = (n - k) % n;
@@ -273,45 +312,11 @@ k_x_cross(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 *_
         const int line = (f < 2) ? 3 * pr + odd : 3 * pr + 2;
         const double2 P0 = res2[k * L2 + line];
         const double2 Pm = res2[km * L2 + line];
-        double2 out;
         // unpack: A = (P + conj Pm)/2, B = (P - conj Pm)/(2i)
         const bool takeA = (f == 0) || (f == 2 && !odd);
-        if (takeA) out = mk(0.5 * (P0.x + Pm.x), 0.5 * (P0.y - Pm.y));
-        else out = mk(0.5 * (P0.y + Pm.y), -0.5 * (P0.x - Pm.x));
-        H[(long long)f * fstride + ((long long)j * d.NZ2 + z) * d.nkx + k] = cscale(invn, out);
-    }
-}
-
-// ---------------------------------------------------------------------------
-// K4: forward z FFT, keep |kz| <= NZS, x1/NZ2 (src/fft/transforms.cpp:658-665).
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128)
-k_z_forward(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 *__restrict__ H,
-            double2 *__restrict__ F, int TL) {
-    extern __shared__ double2 sm[];
-    const int n = d.NZ2;
-    double2 *s_root = sm;
-    double2 *a = sm + n;
-    double2 *b = a + n * TL;
-    const int f = blockIdx.z, j = blockIdx.y, kx0 = blockIdx.x * TL;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) s_root[i] = roots[i];
-    const double2 *Hp = H + ((long long)f * d.ny2 + j) * (long long)n * d.nkx;
-    for (int i = threadIdx.x; i < n * TL; i += blockDim.x) {
-        const int z = i / TL, line = i - (i / TL) * TL;
-        const int kx = kx0 + line;
-        a[i] = kx < d.nkx ? Hp[(long long)z * d.nkx + kx] : mk(0, 0);
-    }
-    __syncthreads();
-    const double2 *res = fft_lines<-1>(a, b, TL, P, s_root);
-    const double invn = 1.0 / (double)n;
-    double2 *Fp = F + ((long long)f * d.ny2 + j) * d.ncol;
-    for (int i = threadIdx.x; i < d.nkz * TL; i += blockDim.x) {
-        const int kzi = i / TL, line = i - (i / TL) * TL;
-        const int kx = kx0 + line;
-        if (kx >= d.nkx) continue;
-        const int kz = kzi - d.NZS;
-        const int slot = kz >= 0 ? kz : n + kz;
-        Fp[kzi * d.nkx + kx] = cscale(invn, res[slot * TL + line]);
+        const double2 out = takeA ? mk(0.5 * (P0.x + Pm.x), 0.5 * (P0.y - Pm.y))
+                                  : mk(0.5 * (P0.y + Pm.y), -0.5 * (P0.x - Pm.x));
+        H[(long long)f * fstride + ((long long)j * d.NZ2 + z) * nkx + k] = cscale(invn, out);
     }
 }
 
@@ -456,12 +461,22 @@ k_x_r2c(Dims d, FftPlan P, const double2 *__restrict__ roots, const double *__re
 namespace {
 constexpr int kJT = 2;
 constexpr int kKT = 8;
-constexpr int kTL = 16;
 constexpr int kRW = 4;
 constexpr int kRWs = 8;
 }  // namespace
 
-size_t smem_zfft(const Dims &d) { return sizeof(double2) * (size_t)d.NZ2 * (1 + 2 * kTL); }
+// Lines per z-FFT block: the width in [8, 17] that tiles NXS+1 with the least
+// padding (13 for 65 modes).
+int z_lines(const Dims &d) {
+    int best = 16, waste = 1 << 30;
+    for (int tl = 17; tl >= 8; --tl) {
+        const int w = ((d.nkx + tl - 1) / tl) * tl - d.nkx;
+        if (w < waste) { waste = w; best = tl; }
+    }
+    return best;
+}
+
+size_t smem_zfft(const Dims &d) { return sizeof(double2) * (size_t)d.NZ2 * (1 + 2 * z_lines(d)); }
 size_t smem_xcross(const Dims &d) { return sizeof(double2) * (size_t)d.NX2 * (1 + 2 * 3 * kRW); }
 size_t smem_xsingle(const Dims &d) {
     return sizeof(double2) * (size_t)d.NX2 * (1 + 2 * ((kRWs + 1) / 2));
@@ -498,8 +513,9 @@ void launch_curl_ysynth(const Dims &d, const Tables &t, const double2 *u, double
 
 void launch_z_backward(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *F,
                        double2 *G, int nf, cudaStream_t s) {
-    dim3 grid((d.nkx + kTL - 1) / kTL, d.ny2, nf);
-    k_z_backward<<<grid, 128, smem_zfft(d), s>>>(d, P, roots, F, G, kTL);
+    const int tl = z_lines(d);
+    dim3 grid((d.nkx + tl - 1) / tl, d.ny2, nf);
+    k_z_backward<<<grid, 256, smem_zfft(d), s>>>(d, P, roots, F, G, tl);
 }
 
 void launch_x_cross(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G,
@@ -510,8 +526,9 @@ void launch_x_cross(const Dims &d, const FftPlan &P, const double2 *roots, const
 
 void launch_z_forward(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *H,
                       double2 *F, int nf, cudaStream_t s) {
-    dim3 grid((d.nkx + kTL - 1) / kTL, d.ny2, nf);
-    k_z_forward<<<grid, 128, smem_zfft(d), s>>>(d, P, roots, H, F, kTL);
+    const int tl = z_lines(d);
+    dim3 grid((d.nkx + tl - 1) / tl, d.ny2, nf);
+    k_z_forward<<<grid, 256, smem_zfft(d), s>>>(d, P, roots, H, F, tl);
 }
 
 void launch_y_analysis(const Dims &d, const Tables &t, const double2 *F, double2 *S, int nf,

@@ -54,6 +54,43 @@ def test_fine_transforms(case):
     assert np.abs(back - U).max() <= 1e-12 * np.abs(U).max()   # round trip (band-limited)
 
 
+ODD_RADIX_MESHES = {
+    # NX2 / NZ2 factorisations: 20 = 4*5, 40 = 4*2*5; 22 = 2*11, 36 = 4*9; 26 = 2*13, 52 = 4*13
+    "r5": (8, 14, 8, 20, 16, 40),
+    "r9_11": (8, 14, 8, 22, 16, 36),
+    "r13": (10, 14, 12, 26, 16, 52),
+}
+
+
+def odd_radix_case(key):
+    nxs, nys, nzs, nx2, ny2, nz2 = ODD_RADIX_MESHES[key]
+    m = orc.Mesh(2 * nxs, nys + 2, 2 * nzs, nxs, nys, nzs, nx2, ny2, nz2, 4 * np.pi, 2 * np.pi)
+    _, p = channel_case(16)
+    return m, p
+
+
+@pytest.mark.parametrize("key", sorted(ODD_RADIX_MESHES))
+def test_fine_transforms_odd_radices(key):
+    """FFT lengths with radix 5, 9, 11 and 13 passes, against the oracle."""
+    m, p = odd_radix_case(key)
+    U = band_spectrum(m, 23)
+    c = ctx_for(m, p)
+    phys_ref = orc.fine_backward(m, U)
+    assert rel_max(c.transform_fine("B", U), phys_ref) <= 1e-12
+    assert rel_max(c.transform_fine("F", phys_ref), orc.fine_forward(m, phys_ref)) <= 1e-12
+
+
+@pytest.mark.parametrize("key", sorted(ODD_RADIX_MESHES))
+def test_nonlinear_term_odd_radices(key):
+    m, p = odd_radix_case(key)
+    u = divergence_free_field(m, p, seed=4, amp=0.1, spectrum="k53", mean="loglaw")
+    cst = orc.make_constants(m, p.Re)
+    N_ref, _, B_ref = orc.nonlinear_term(m, cst, u)
+    N, B = ctx_for(m, p).nonlinear(np.stack(u, axis=-1))
+    for k in range(3):
+        assert rel_max(N[..., k], N_ref[k]) <= 1e-12
+
+
 def test_fine_forward_analytic_nyquist_peak():
     """tests/test_xyzfft.cpp:323-353: a fine-grid Nyquist mode has peak 1.0."""
     m, p = example_case()
