@@ -11,15 +11,15 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "cdns", "libcdns_cuda.so")
-SOURCES = ["context.cu", "transforms.cu", "solver.cu", "layout.cu", "noalloc.cu"]
+SOURCES = ["context.cu", "transforms.cu", "solver.cu", "solver_setup.cu", "layout.cu", "noalloc.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
-# Per-file nvcc flags.  The tau solver is latency-bound: it keeps the
-# reference's rounding (no FMA contraction), which matters for columns whose
-# solve amplifies rounding differences.
-FILE_FLAGS = {"solver.cu": ["-fmad=false"]}
+# Per-file nvcc flags.  The column solver keeps the reference's rounding of
+# each operation (no FMA contraction): its setup feeds differences that cancel
+# to 1e-6 of their terms.
+FILE_FLAGS = {"solver.cu": ["-fmad=false"], "solver_setup.cu": ["-fmad=false"]}
 
 
 def build(verbose: bool = False, extra=None) -> str:

@@ -27,12 +27,13 @@ void launch_x_r2c(const Dims &d, const FftPlan &P, const double2 *roots, const d
 // Precomputed solver state (EqSolvePV members, src/solver/eqsolve_pv.hpp:60-76).
 struct SolverState {
     double *wn_p, *wn_v;        // [ncol]
-    double *ad_p, *ad_v;        // [nkz][ncy][nkx]
-    double2 *p_inf;             // [2][Ns]
-    double2 *v_inf;             // [2][3][Ns]
+    // pivots and solution fields are column-major: [..][col][y]
+    double *ad_p, *ad_v;        // [ncol][ncy]
+    double2 *p_inf;             // [2][ncol][ncy]
+    double2 *v_inf;             // [2][3][ncol][ncy]
     double2 *inf_div;           // [2 (response)][2 (wall)][ncol]
-    double2 *p_b;               // [Ns]
-    double2 *v_b;               // [3][Ns]
+    double2 *p_b;               // [ncol][ncy]
+    double2 *v_b;               // [3][ncol][ncy]
     double2 *sigma0;            // [2][ncol]
     double *unit;               // [2][ncy] u_dpdx_unit, w_dpdz_unit ; [2*ncy..] qx, qz
 };
@@ -60,8 +61,12 @@ struct StepArgs {
     int solve_only;             // 1: solve_modes alone (no zero-mode / flow correction)
 };
 
+// ---- solver_setup.cu ----
+cudaError_t configure_setup_kernels(const Dims &d);
 void setup_solver(const Dims &d, const Tables &t, const PhysParams &pp, double g_v,
                   SolverState &st, double2 *scratch, cudaStream_t s);
+
+// ---- solver.cu ----
 void launch_step_solve(const Dims &d, const Tables &t, const PhysParams &pp, double g_v,
                        const SolverState &st, const StepArgs &a, cudaStream_t s);
 cudaError_t configure_solver_kernels(const Dims &d);

@@ -1,469 +1,570 @@
 // Per-(kz, kx) Chebyshev-tau pressure/velocity solve of the channel-dns step
 // (EqSolvePV, src/solver/eqsolve_pv.cpp) for sm_100a.
 //
-// One block owns TC consecutive spectral columns.  Coalesced block-wide
-// passes stage each column's inputs in shared memory ([y][column] layout)
-// and stream the precomputed influence / B-problem fields on write-back; the
-// sequential y recurrences run two threads per column, because every tau
-// recurrence (src/solver/eqsolve_pv.cpp:64-128) and every Chebyshev
-// derivative recurrence (src/solver/vector_ops.cpp:17-25) couples only
-// coefficients of one parity.  All arithmetic is FP64 in the reference's
-// operation order.
+// One warp owns one spectral column (kz, kx) and keeps all its y coefficients
+// in registers.  Lane L = 2h + p holds, for every field, the coefficients of
+// parity p at y = 2(E h + e) + p, e = 0..E-1 (E = ceil((NYS+1)/32) rounded up
+// to 1, 2, 4 or 8).  Every tau recurrence (src/solver/eqsolve_pv.cpp:64-128)
+// and every Chebyshev derivative recurrence (src/solver/vector_ops.cpp:17-25)
+// couples only coefficients of one parity, so each becomes a first-order
+// affine recurrence along the 16 lanes of that parity: a sequential pass over
+// a lane's E coefficients, a 4-level shuffle scan over the lanes, and a
+// carry-in.  Wall sums are shuffle reductions.  This reassociates the
+// reference's sequential sums and recurrences; the results agree with the
+// sequential order to round-off (tested against the oracle at 1e-10).
+//
+// The step solve reads and writes the spectral state in its planar
+// [kz][y][kx] layout through swizzled shared-memory tiles (a block of TC
+// warps owns TC consecutive columns, so every global access is a coalesced
+// row of TC columns).  The precomputed influence and B-problem fields and the
+// tau pivots (solver_setup.cu) are stored column-major ([col][y]) and read by
+// each warp directly.
 #include "cdns_kernels.cuh"
 
 namespace cdns {
 
 namespace {
-constexpr int TC = 8;          // spectral columns per block
-constexpr int kThreads = 128;
-
-enum Mode { MODE_STEP = 0, MODE_BASE = 1, MODE_COUPLED = 2 };
+constexpr int TC = 8;                 // columns (warps) per block
+constexpr int kThreads = 32 * TC;
+constexpr unsigned kFull = 0xffffffffu;
 
 struct SolveArgs {
     double p_a, p_b;           // pressure wall condition a P + b dP/dn
-    double2 bcp_top, bcp_bot;  // constant pressure wall data (setup problems)
-    double2 *p_out;            // [Ns]
-    double2 *v_out;            // [3][Ns]
-    double2 *divb_out;         // [2][ncol] raw wall divergence (MODE_BASE)
-    StepArgs step;             // MODE_STEP only
+    double2 *p_out;            // [Ns] planar
+    double2 *v_out;            // [3][Ns] planar
+    StepArgs step;
 };
 
-__device__ inline double tau_func(double a, double b, int y) {
+// ---- warp primitives -------------------------------------------------------
+__device__ __forceinline__ double2 shfl2(double2 v, int src) {
+    return mk(__shfl_sync(kFull, v.x, src), __shfl_sync(kFull, v.y, src));
+}
+__device__ __forceinline__ double2 shfl2_up(double2 v, int d) {
+    return mk(__shfl_up_sync(kFull, v.x, d), __shfl_up_sync(kFull, v.y, d));
+}
+__device__ __forceinline__ double2 shfl2_down(double2 v, int d) {
+    return mk(__shfl_down_sync(kFull, v.x, d), __shfl_down_sync(kFull, v.y, d));
+}
+__device__ __forceinline__ double2 shfl2_xor(double2 v, int m) {
+    return mk(__shfl_xor_sync(kFull, v.x, m), __shfl_xor_sync(kFull, v.y, m));
+}
+// Sum over the 16 lanes of one parity; every lane of the parity gets the
+// same value (IEEE addition commutes).
+__device__ __forceinline__ double2 sum_parity(double2 v) {
+#pragma unroll
+    for (int m = 2; m < 32; m <<= 1) v = cadd(v, shfl2_xor(v, m));
+    return v;
+}
+__device__ __forceinline__ double2 sum_warp(double2 v) {
+#pragma unroll
+    for (int m = 1; m < 32; m <<= 1) v = cadd(v, shfl2_xor(v, m));
+    return v;
+}
+__device__ __forceinline__ double sum_warp(double v) {
+#pragma unroll
+    for (int m = 1; m < 32; m <<= 1) v += __shfl_xor_sync(kFull, v, m);
+    return v;
+}
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+// y of element e in this lane.
+template <int E> __device__ __forceinline__ int ycoef(int e) {
+    const int L = lane_id();
+    return 2 * (E * (L >> 1) + e) + (L & 1);
+}
+
+// Value of coefficient y (uniform across the warp) broadcast to all lanes.
+template <int E> __device__ __forceinline__ double2 elem(const double2 (&x)[E], int y) {
+    const int m = y >> 1, h = m / E, e = m - h * E;
+    double2 v = x[0];
+#pragma unroll
+    for (int k = 1; k < E; ++k)
+        if (k == e) v = x[k];
+    return shfl2(v, 2 * h + (y & 1));
+}
+
+// In-place solution of X_y = B_y + A_y X_{y+2} (suffix direction, per parity);
+// elements beyond the chain carry A = 0, B = 0.
+template <int E> __device__ __forceinline__ void affine_suffix(double (&A)[E], double2 (&B)[E]) {
+    const int L = lane_id();
+#pragma unroll
+    for (int e = E - 2; e >= 0; --e) {
+        B[e] = cadd(B[e], cscale(A[e], B[e + 1]));
+        A[e] = A[e] * A[e + 1];
+    }
+    double a = A[0];
+    double2 b = B[0];
+#pragma unroll
+    for (int d = 2; d < 32; d <<= 1) {
+        const double a2 = __shfl_down_sync(kFull, a, d);
+        const double2 b2 = shfl2_down(b, d);
+        if (L + d < 32) {
+            b = cadd(b, cscale(a, b2));
+            a = a * a2;
+        }
+    }
+    double2 carry = shfl2_down(b, 2);
+    if (L + 2 >= 32) carry = mk(0.0, 0.0);
+#pragma unroll
+    for (int e = 0; e < E; ++e) B[e] = cadd(B[e], cscale(A[e], carry));
+}
+template <int E> __device__ __forceinline__ void affine_suffix(double (&A)[E], double (&B)[E]) {
+    const int L = lane_id();
+#pragma unroll
+    for (int e = E - 2; e >= 0; --e) {
+        B[e] = B[e] + A[e] * B[e + 1];
+        A[e] = A[e] * A[e + 1];
+    }
+    double a = A[0], b = B[0];
+#pragma unroll
+    for (int d = 2; d < 32; d <<= 1) {
+        const double a2 = __shfl_down_sync(kFull, a, d);
+        const double b2 = __shfl_down_sync(kFull, b, d);
+        if (L + d < 32) {
+            b = b + a * b2;
+            a = a * a2;
+        }
+    }
+    double carry = __shfl_down_sync(kFull, b, 2);
+    if (L + 2 >= 32) carry = 0.0;
+#pragma unroll
+    for (int e = 0; e < E; ++e) B[e] = B[e] + A[e] * carry;
+}
+// In-place solution of Z_y = B_y + A_y Z_{y-2} (prefix direction, per parity).
+template <int E> __device__ __forceinline__ void affine_prefix(double (&A)[E], double2 (&B)[E]) {
+    const int L = lane_id();
+#pragma unroll
+    for (int e = 1; e < E; ++e) {
+        B[e] = cadd(B[e], cscale(A[e], B[e - 1]));
+        A[e] = A[e] * A[e - 1];
+    }
+    double a = A[E - 1];
+    double2 b = B[E - 1];
+#pragma unroll
+    for (int d = 2; d < 32; d <<= 1) {
+        const double a2 = __shfl_up_sync(kFull, a, d);
+        const double2 b2 = shfl2_up(b, d);
+        if (L >= d) {
+            b = cadd(b, cscale(a, b2));
+            a = a * a2;
+        }
+    }
+    double2 carry = shfl2_up(b, 2);
+    if (L < 2) carry = mk(0.0, 0.0);
+#pragma unroll
+    for (int e = 0; e < E; ++e) B[e] = cadd(B[e], cscale(A[e], carry));
+}
+// In-place suffix sums S_y = sum_{j >= y, j = y mod 2} S_j.
+template <int E> __device__ __forceinline__ void suffix_sum(double2 (&S)[E]) {
+    const int L = lane_id();
+#pragma unroll
+    for (int e = E - 2; e >= 0; --e) S[e] = cadd(S[e + 1], S[e]);
+    double2 b = S[0];
+#pragma unroll
+    for (int d = 2; d < 32; d <<= 1) {
+        const double2 t = shfl2_down(b, d);
+        if (L + d < 32) b = cadd(t, b);
+    }
+    double2 carry = shfl2_down(b, 2);
+    if (L + 2 >= 32) carry = mk(0.0, 0.0);
+#pragma unroll
+    for (int e = 0; e < E; ++e) S[e] = cadd(carry, S[e]);
+}
+
+__device__ __forceinline__ double tau_func(double a, double b, int y) {
     const int q = y & 1;
     if (a == 0.0 && b == 0.0) return (double)((1 - q) * y * y + q);
     return a + b * y * y;
 }
 
-// Chebyshev derivative coefficients of parity `par`:
-// d_k = d_{k+2} + 2(k+1) f_{k+1}, d_NYS = 0, d_0 halved.
-__device__ void deriv_chain(int par, int ny, const double2 *f, double2 *dout, int st) {
-    int k = ((ny & 1) == par) ? ny : ny - 1;
-    double2 dd = mk(0.0, 0.0);
-    if (k == ny) {
-        dout[(long long)ny * st] = dd;
-        k -= 2;
+// Chebyshev derivative (src/solver/vector_ops.cpp:17-25):
+// d_k = sum_{j > k, j = k+1 mod 2} 2 j f_j, d_0 halved.  f is zero beyond ny.
+template <int E> __device__ __forceinline__ void deriv_warp(int ny, const double2 (&f)[E], double2 (&d)[E]) {
+    const int L = lane_id(), p = L & 1;
+    double2 S[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int y = ycoef<E>(e);
+        S[e] = (y <= ny) ? cscale((double)(2 * y), f[e]) : mk(0.0, 0.0);
     }
-    for (; k >= 0; k -= 2) {
-        dd = cadd(dd, cscale((double)(2 * (k + 1)), f[(long long)(k + 1) * st]));
-        if (k == 0) dd = cscale(0.5, dd);
-        dout[(long long)k * st] = dd;
+    suffix_sum<E>(S);
+    // d(y) = S(y + 1): the neighbour of opposite parity
+    double2 a[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) a[e] = shfl2_xor(S[e], 1);
+    double2 c = shfl2_down(S[0], 1);
+    if (L == 31) c = mk(0.0, 0.0);
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int y = ycoef<E>(e);
+        const double2 nx = (p == 0) ? a[e] : (e + 1 < E ? a[(e + 1) % E] : c);
+        d[e] = (y < ny) ? nx : mk(0.0, 0.0);
+        if (y == 0) d[e] = cscale(0.5, d[e]);
     }
 }
 
-// One parity of the column tau solve of (D^2 - k^2 - g) f = r with
-// a f + b f' = (lower, upper) at y = (+1, -1)  (src/solver/eqsolve_pv.cpp:64-128).
-// Returns false if a pivot is zero or not finite.
-__device__ bool tau_chain(int par, int ny, double g, double a, double b, bool zero_col,
-                          double2 lower, double2 upper, double w, const double2 *r, double2 *out,
-                          const double *ad, int st, const double *WL, const double *WD,
-                          const double *WR) {
+// Tau solve of (D^2 - k^2 - g) f = r with a f + b f' = (lower, upper) at
+// y = (+1, -1), both parities at once (src/solver/eqsolve_pv.cpp:64-128).
+// r must be zero beyond ny.  Returns false in a lane whose parity's pivot is
+// zero or not finite.
+template <int E>
+__device__ bool tau_warp(int ny, double g, double a, double b, bool zero_col, double2 lower,
+                         double2 upper, double w, const double2 (&r)[E], double2 (&out)[E],
+                         const double (&ad)[E], const double *__restrict__ WL,
+                         const double *__restrict__ WD, const double *__restrict__ WR) {
+    const int L = lane_id(), p = L & 1;
     const bool normalize = g == 0.0 && a == 0.0 && zero_col;
-    double2 r0 = r[0];
-    if (normalize && par == 0) {
-        double2 corr = mk(0.0, 0.0);
-        for (int y = 2; y <= ny; y += 2) corr = cadd(corr, cdivr(r[(long long)y * st], (double)(y * y - 1)));
-        if (b != 0.0) corr = cadd(corr, cdivr(cadd(lower, upper), 2.0 * b));
-        r0 = corr;
+    const int top = ((ny & 1) == p) ? ny : ny - 1;
+    double2 rr[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) rr[e] = r[e];
+    if (normalize) {
+        // the even chain of the singular zero column is closed by the mean
+        // (eqsolve_pv.cpp:71-79): r_0 <- sum_{y>=2 even} r_y/(y^2-1) + (lo+up)/(2b)
+        double2 part = mk(0.0, 0.0);
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int y = ycoef<E>(e);
+            if (p == 0 && y >= 2 && y <= ny) part = cadd(part, cdivr(r[e], (double)(y * y - 1)));
+        }
+        part = sum_parity(part);
+        if (b != 0.0) part = cadd(part, cdivr(cadd(lower, upper), 2.0 * b));
+        if (L == 0) rr[0] = part;
     }
-#define RR(yy) ((yy) == 0 ? r0 : r[(long long)(yy) * st])
-#define OUT(yy) out[(long long)(yy) * st]
-#define AD(yy) ad[(long long)(yy) * st]
-    if (par == 0) OUT(0) = cdivr(cadd(lower, upper), 2.0);
-    else OUT(1) = cdivr(csub(lower, upper), 2.0);
-    for (int y = 2 + par; y <= ny - 2; y += 2)
-        OUT(y) = cadd(cadd(cscale(WL[y], RR(y - 2)), cscale(WD[y], RR(y))), cscale(WR[y], RR(y + 2)));
-    if (((ny - 1) & 1) == par) OUT(ny - 1) = cadd(cscale(WL[ny - 1], RR(ny - 3)), cscale(WD[ny - 1], RR(ny - 1)));
-    if ((ny & 1) == par) OUT(ny) = cadd(cscale(WL[ny], RR(ny - 2)), cscale(WD[ny], RR(ny)));
-    int ys = ny - 2;
-    if ((ys & 1) != par) ys -= 1;
-    for (int y = ys; y >= 2; y -= 2) OUT(y) = csub(OUT(y), cscale((WR[y] * w) * AD(y + 2), OUT(y + 2)));
-    double ad01 = tau_func(a, b, ((ny & 1) == par) ? ny : ny - 1);
-    double2 o0 = OUT(par);
-    for (int y = ys; y >= par; y -= 2) {
-        o0 = csub(o0, cscale(ad01 * AD(y + 2), OUT(y + 2)));
-        ad01 = tau_func(a, b, y) - ((WL[y + 2] * w) * ad01) * AD(y + 2);
+    // three-term combination of the rhs
+    double2 rm2_0 = shfl2_up(rr[E - 1], 2);
+    double2 rp2_l = shfl2_down(rr[0], 2);
+    if (L + 2 >= 32) rp2_l = mk(0.0, 0.0);
+    double2 X[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int y = ycoef<E>(e);
+        const double2 rm2 = e > 0 ? rr[(e + E - 1) % E] : rm2_0;
+        const double2 rp2 = e + 1 < E ? rr[(e + 1) % E] : rp2_l;
+        if (y > ny) X[e] = mk(0.0, 0.0);
+        else if (y == p) X[e] = (p == 0) ? cdivr(cadd(lower, upper), 2.0) : cdivr(csub(lower, upper), 2.0);
+        else if (y >= ny - 1) X[e] = cadd(cscale(WL[y], rm2), cscale(WD[y], rr[e]));
+        else X[e] = cadd(cadd(cscale(WL[y], rm2), cscale(WD[y], rr[e])), cscale(WR[y], rp2));
     }
-    if (normalize && par == 0) {
+    // pivots one step up the chain, AD(y + 2)
+    double adn_l = __shfl_down_sync(kFull, ad[0], 2);
+    if (L + 2 >= 32) adn_l = 0.0;
+    // backward sweep X_y -= (WR_y w AD_{y+2}) X_{y+2} for 2 <= y <= top - 2
+    double A[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int y = ycoef<E>(e);
+        const double adn = e + 1 < E ? ad[(e + 1) % E] : adn_l;
+        A[e] = (y >= 2 && y <= top - 2) ? -((WR[y] * w) * adn) : 0.0;
+    }
+    affine_suffix<E>(A, X);
+    // pivot chain ad01_j = tau(j) - (WL_{j+2} w ad01_{j+2}) AD_{j+2}, ad01_top = tau(top)
+    double Aa[E], Ba[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int y = ycoef<E>(e);
+        const double adn = e + 1 < E ? ad[(e + 1) % E] : adn_l;
+        if (y > top) {
+            Aa[e] = 0.0;
+            Ba[e] = 0.0;
+        } else if (y == top) {
+            Aa[e] = 0.0;
+            Ba[e] = tau_func(a, b, y);
+        } else {
+            Aa[e] = -((WL[y + 2] * w) * adn);
+            Ba[e] = tau_func(a, b, y);
+        }
+    }
+    affine_suffix<E>(Aa, Ba);
+    // o0 = X_par - sum_{j = par+2..top} ad01_j AD_j X_j ; pivot ad01_par
+    double2 s = mk(0.0, 0.0);
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int y = ycoef<E>(e);
+        if (y >= p + 2 && y <= top) s = cadd(s, cscale(Ba[e] * ad[e], X[e]));
+    }
+    s = sum_parity(s);
+    double2 o0 = csub(shfl2(X[0], p), s);
+    double piv = __shfl_sync(kFull, Ba[0], p);
+    if (normalize && p == 0) {
         o0 = mk(0.0, 0.0);
-        ad01 = 1.0;
+        piv = 1.0;
     }
-    const bool ok = isfinite(ad01) && ad01 != 0.0;
-    OUT(par) = cdivr(o0, ad01);
-    for (int y = 2 + par; y <= ny; y += 2) OUT(y) = cscale(AD(y), csub(OUT(y), cscale(WL[y] * w, OUT(y - 2))));
-#undef RR
-#undef OUT
-#undef AD
+    const bool ok = isfinite(piv) && piv != 0.0;
+    const double2 zpar = cdivr(o0, piv);
+    // forward sweep Z_y = AD_y (X_y - WL_y w Z_{y-2})
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int y = ycoef<E>(e);
+        if (y == p) {
+            A[e] = 0.0;
+            X[e] = zpar;
+        } else if (y <= ny) {
+            A[e] = -(ad[e] * (WL[y] * w));
+            X[e] = cscale(ad[e], X[e]);
+        } else {
+            A[e] = 0.0;
+            X[e] = mk(0.0, 0.0);
+        }
+    }
+    affine_prefix<E>(A, X);
+#pragma unroll
+    for (int e = 0; e < E; ++e) out[e] = ycoef<E>(e) <= ny ? X[e] : mk(0.0, 0.0);
     return ok;
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(kThreads)
-k_solve(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, SolveArgs A) {
-    extern __shared__ double2 sm2[];
-    const int ncy = d.ncy, ny = d.NYS, nkx = d.nkx;
-    const int S = ncy * TC;
-    double2 *rv = sm2;            // [3][ncy][TC]
-    double2 *pc = rv + 3 * S;     // [ncy][TC]
-    double2 *dyb = pc + S;
-    double2 *fo = dyb + S;
-    double *adp = reinterpret_cast<double *>(fo + S);
-    double *adv = adp + S;
-    double *sWL = adv + S;
-    double *sWD = sWL + ncy;
-    double *sWR = sWD + ncy;
-    __shared__ double2 s_lo[TC], s_up[TC], s_c0[TC], s_c1[TC], s_sig[2][TC];
-    __shared__ double s_dp[2];
+// Shared-memory tile [ncy][TC] of complex values with the column slot
+// swizzled by y, so that both a row of TC columns (staging) and the E-strided
+// y coefficients of one column (a warp) are free of bank conflicts.
+template <int E> __device__ __forceinline__ int tile_slot(int y, int l) {
+    const int g = (2 * (y / (2 * E)) + (y & 1)) & (TC - 1);
+    return y * TC + (l ^ g);
+}
 
+template <int E>
+__global__ void __launch_bounds__(kThreads, E <= 4 ? 2 : 1)
+k_solve(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, SolveArgs A) {
+    extern __shared__ double2 tile[];   // [4][ncy][TC]
+    const int ncy = d.ncy, ny = d.NYS, nkx = d.nkx, ncol = d.ncol;
+    const int S = ncy * TC;
     const int col0 = blockIdx.x * TC;
     const int tid = threadIdx.x;
-    for (int i = tid; i < ncy; i += blockDim.x) {
-        sWL[i] = t.WL[i];
-        sWD[i] = t.WD[i];
-        sWR[i] = t.WR[i];
-    }
-    // ---- phase A: stage inputs -------------------------------------------
-    for (int i = tid; i < S; i += blockDim.x) {
+    const int w = tid >> 5;
+    const int L = tid & 31, p = L & 1;
+    const int col = col0 + w;
+    const StepArgs &s = A.step;
+
+    // ---- stage R = a0 u + a1 u_prev + b0 N + b1 N_prev and N_y -------------
+#pragma unroll 2
+    for (int i = tid; i < S; i += kThreads) {
         const int y = i / TC, l = i - (i / TC) * TC;
-        const int col = col0 + l;
-        if (col < d.ncol) {
-            const int kzi = col / nkx, kx = col - (col / nkx) * nkx;
+        const int c2 = col0 + l;
+        if (c2 < ncol) {
+            const int kzi = c2 / nkx, kx = c2 - (c2 / nkx) * nkx;
             const long long off = ((long long)kzi * ncy + y) * nkx + kx;
-            adp[i] = st.ad_p[off];
-            adv[i] = st.ad_v[off];
-            if (MODE == MODE_STEP) {
-                const StepArgs &s = A.step;
-                for (int c = 0; c < 3; ++c) {
-                    const long long o = c * d.Ns + off;
-                    // R = a0 u + a1 u_prev + b0 N + b1 N_prev (src/sim/simulation.cpp:151-158)
-                    const double2 R = cadd(cadd(cadd(cscale(s.a0, s.u[o]), cscale(s.a1, s.u_prev[o])),
-                                                cscale(s.b0, s.N[o])),
-                                           cscale(s.b1, s.N_prev[o]));
-                    rv[c * S + i] = R;
-                }
-                fo[i] = s.N[d.Ns + off];
-            } else {
-                for (int c = 0; c < 3; ++c) rv[c * S + i] = mk(0, 0);
-                double rp = 0.0;
-                if (MODE == MODE_COUPLED) {
-                    // B-problem pressure RHS (src/solver/eqsolve_pv.cpp:452-461)
-                    if (y == 0) rp = (double)(ny - 1);
-                    else if (y < ny) rp = (double)(2 * (ny - ((y + 1) % 2)));
-                }
-                dyb[i] = mk(rp, 0.0);
+            const int sl = tile_slot<E>(y, l);
+            double2 nv[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const long long o = c * d.Ns + off;
+                nv[c] = s.N[o];
+                // R (src/sim/simulation.cpp:151-158)
+                tile[c * S + sl] = cadd(cadd(cadd(cscale(s.a0, s.u[o]), cscale(s.a1, s.u_prev[o])),
+                                             cscale(s.b0, nv[c])),
+                                        cscale(s.b1, s.N_prev[o]));
             }
-        } else {
-            adp[i] = 1.0;
-            adv[i] = 1.0;
-            for (int c = 0; c < 3; ++c) rv[c * S + i] = mk(0, 0);
-            dyb[i] = mk(0, 0);
-            fo[i] = mk(0, 0);
+            tile[3 * S + sl] = nv[1];
         }
-        pc[i] = mk(0, 0);
     }
     __syncthreads();
 
-    // ---- phase B: recurrences, two threads (parities) per column ----------
-    if (tid < 2 * TC) {
-        const unsigned mask = 0x0000ffffu;
-        const int l = tid >> 1, par = tid & 1;
-        const int col = col0 + l;
-        const bool active = col < d.ncol;
-        const int kzi = active ? col / nkx : 0;
-        const int kx = active ? col - kzi * nkx : 0;
+    if (col < ncol) {
+        const int kzi = col / nkx, kx = col - kzi * nkx;
         const double ax = t.wavx[kx], az = t.wavz[kzi];
-        const bool zero_col = active && kzi == d.NZS && kx == 0;
-        double2 tail0 = mk(0, 0), tail1 = mk(0, 0);
-        bool ok = true;
-        if (active && par == 0) {
-            if (MODE == MODE_STEP && A.step.bc_p) {
-                s_lo[l] = A.step.bc_p[col];
-                s_up[l] = A.step.bc_p[d.ncol + col];
-            } else if (MODE == MODE_STEP) {
-                const StepArgs &s = A.step;
-                double2 st_ = mk(0, 0), sb_ = mk(0, 0);
-                for (int y = 0; y <= ny; ++y) {
-                    const double2 n1 = fo[y * TC + l];
-                    st_ = cadd(st_, n1);
-                    sb_ = (y & 1) ? cadd(sb_, n1) : csub(sb_, n1);
-                }
-                const double2 bt = cadd(s.bw[col], st_);
-                const double2 bb = cadd(s.bw[d.ncol + col], sb_);
+        const bool zero_col = kzi == d.NZS && kx == 0;
+        const long long cm = (long long)col * ncy;   // column-major base
+        bool bad = false, pivot_fail = false;
+        double2 pv[E], v0[E], v1[E], v2[E], dy[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int y = ycoef<E>(e);
+            if (y <= ny) {
+                const int sl = tile_slot<E>(y, w);
+                v0[e] = tile[sl];
+                v1[e] = tile[S + sl];
+                v2[e] = tile[2 * S + sl];
+                dy[e] = tile[3 * S + sl];
+            } else {
+                v0[e] = v1[e] = v2[e] = dy[e] = mk(0.0, 0.0);
+            }
+        }
+        double2 lower, upper;
+        if (s.bc_p) {
+            lower = s.bc_p[col];
+            upper = s.bc_p[ncol + col];
+        } else {
+            // pressure wall data (src/solver/eqsolve_pv.cpp:322-337)
+            double2 st_ = mk(0, 0), sb_ = mk(0, 0);
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                st_ = cadd(st_, dy[e]);
+                sb_ = p ? cadd(sb_, dy[e]) : csub(sb_, dy[e]);
+            }
+            st_ = sum_warp(st_);
+            sb_ = sum_warp(sb_);
+            const double2 bt = cadd(s.bw[col], st_);
+            const double2 bb = cadd(s.bw[ncol + col], sb_);
+            if (L == 0) {
                 s.B_new[col] = bt;
-                s.B_new[d.ncol + col] = bb;
-                // combined wall data b0 B + b1 B_prev (src/sim/simulation.cpp:146-150)
-                s_lo[l] = cadd(cscale(s.b0, bt), cscale(s.b1, s.B_prev[col]));
-                s_up[l] = cadd(cscale(s.b0, bb), cscale(s.b1, s.B_prev[d.ncol + col]));
-            } else {
-                s_lo[l] = A.bcp_top;
-                s_up[l] = A.bcp_bot;
+                s.B_new[ncol + col] = bb;
             }
+            // combined wall data b0 B + b1 B_prev (src/sim/simulation.cpp:146-150)
+            lower = cadd(cscale(s.b0, bt), cscale(s.b1, s.B_prev[col]));
+            upper = cadd(cscale(s.b0, bb), cscale(s.b1, s.B_prev[ncol + col]));
         }
-        __syncwarp(mask);
-        const double2 lower = s_lo[l], upper = s_up[l];
-        if (MODE == MODE_STEP && active) {
-            // fused divergence of the RHS (src/solver/eqsolve_pv.cpp:340-357)
-            deriv_chain(par, ny, rv + S + l, dyb + l, TC);
-            for (int y = par; y <= ny; y += 2) {
-                const int k = y * TC + l;
-                dyb[k] = cadd(cadd(fderiv(ax, rv[k]), dyb[k]), fderiv(az, rv[2 * S + k]));
+        // divergence of R (src/solver/eqsolve_pv.cpp:340-357)
+        deriv_warp<E>(ny, v1, dy);
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+            if (ycoef<E>(e) <= ny) dy[e] = cadd(cadd(fderiv(ax, v0[e]), dy[e]), fderiv(az, v2[e]));
+        // pressure
+        double ad[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int y = ycoef<E>(e);
+            ad[e] = y <= ny ? st.ad_p[cm + y] : 0.0;
+        }
+        pivot_fail |= !tau_warp<E>(ny, pp.G_pre, A.p_a, A.p_b, zero_col, lower, upper, st.wn_p[col], dy, pv,
+                                   ad, t.WL, t.WD, t.WR);
+        const double2 tail0 = elem<E>(v1, ny), tail1 = elem<E>(v1, ny - 1);
+        // velocity: Re (grad P - R) (src/solver/eqsolve_pv.cpp:359-395)
+        deriv_warp<E>(ny, pv, dy);
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int y = ycoef<E>(e);
+            ad[e] = y <= ny ? st.ad_v[cm + y] : 0.0;
+        }
+        const double wv = st.wn_v[col];
+        auto velocity = [&](int c, double2(&vc)[E]) {
+            double2 f[E];
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const double2 grad = (c == 0) ? fderiv(ax, pv[e]) : (c == 1) ? dy[e] : fderiv(az, pv[e]);
+                f[e] = ycoef<E>(e) <= ny ? cscale(pp.Re, csub(grad, vc[e])) : mk(0.0, 0.0);
             }
+            const double2 blo = s.bc_v[(2 * c) * ncol + col], bup = s.bc_v[(2 * c + 1) * ncol + col];
+            pivot_fail |= !tau_warp<E>(ny, g_v, pp.a_V[c], pp.b_V[c], zero_col, blo, bup, wv, f, vc, ad,
+                                       t.WL, t.WD, t.WR);
+        };
+        velocity(0, v0);
+        velocity(1, v1);
+        velocity(2, v2);
+        // wall divergence by endpoint sums (src/solver/eqsolve_pv.cpp:397-406)
+        double2 div0 = mk(0, 0), div1 = mk(0, 0);
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int y = ycoef<E>(e);
+            const double2 tang = cadd(fderiv(ax, v0[e]), fderiv(az, v2[e]));
+            const double2 nrm = cscale((double)(y * y), v1[e]);
+            div0 = cadd(div0, cadd(tang, nrm));
+            div1 = p ? cadd(div1, cadd(mk(-tang.x, -tang.y), nrm)) : cadd(div1, csub(tang, nrm));
         }
-        __syncwarp(mask);
-        if (active) {
-            ok &= tau_chain(par, ny, pp.G_pre, A.p_a, A.p_b, zero_col, lower, upper,
-                            st.wn_p[col], dyb + l, pc + l, adp + l, TC, sWL, sWD, sWR);
+        div0 = sum_warp(div0);
+        div1 = sum_warp(div1);
+        // influence correction (src/solver/eqsolve_pv.cpp:408-411)
+        const double2 i00 = st.inf_div[col], i01 = st.inf_div[ncol + col];
+        const double2 i10 = st.inf_div[2 * ncol + col], i11 = st.inf_div[3 * ncol + col];
+        const double2 c0 = csub(cmul(div1, i10), cmul(div0, i11));
+        const double2 c1 = csub(cmul(div0, i01), cmul(div1, i00));
+        const double2 *PI0 = st.p_inf + cm, *PI1 = st.p_inf + d.Ns + cm;
+        const double2 *VI0 = st.v_inf + cm, *VI1 = st.v_inf + 3 * d.Ns + cm;
+        // sigma correction (src/solver/eqsolve_pv.cpp:413-429)
+        const double2 ptop = cadd(elem<E>(pv, ny), cadd(cmul(c0, PI0[ny]), cmul(c1, PI1[ny])));
+        const double2 vt0 = cadd(elem<E>(v1, ny), cadd(cmul(c0, VI0[d.Ns + ny]), cmul(c1, VI1[d.Ns + ny])));
+        const double2 vt1 =
+            cadd(elem<E>(v1, ny - 1), cadd(cmul(c0, VI0[d.Ns + ny - 1]), cmul(c1, VI1[d.Ns + ny - 1])));
+        const double2 n0 = csub(cscale(-wv, vt0), cscale(pp.Re, tail0));
+        const double2 n1 = cadd(cscale(-wv, vt1), cscale(pp.Re, csub(cscale(2.0 * ny, ptop), tail1)));
+        const double2 sg0 = cdiv(n0, st.sigma0[col]);
+        const double2 sg1 = cdiv(n1, st.sigma0[ncol + col]);
+        // odd-y coefficients take sigma_0 for p, u, w and sigma_1 for v; even-y the reverse
+        const double2 sq = p ? sg0 : sg1, sv = p ? sg1 : sg0;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int y = ycoef<E>(e);
+            if (y > ny) continue;
+            pv[e] = cadd(pv[e], cadd(cmul(c0, PI0[y]), cmul(c1, PI1[y])));
+            pv[e] = cadd(pv[e], cmul(sq, st.p_b[cm + y]));
+            auto correct = [&](int c, double2 &vc) {
+                vc = cadd(vc, cadd(cmul(c0, VI0[c * d.Ns + y]), cmul(c1, VI1[c * d.Ns + y])));
+                vc = cadd(vc, cmul(c == 1 ? sv : sq, st.v_b[c * d.Ns + cm + y]));
+            };
+            correct(0, v0[e]);
+            correct(1, v1[e]);
+            correct(2, v2[e]);
         }
-        __syncwarp(mask);
-        if (active) {
-            if (par == 0) {
-                tail0 = rv[S + ny * TC + l];
-                tail1 = rv[S + (ny - 1) * TC + l];
-            }
-            deriv_chain(par, ny, pc + l, dyb + l, TC);
-        }
-        __syncwarp(mask);
-        if (active) {
-            const double wv = st.wn_v[col];
-            for (int c = 0; c < 3; ++c) {
-                double2 *rc = rv + c * S + l;
-                for (int y = par; y <= ny; y += 2) {
-                    const int k = y * TC;
-                    const double2 grad = (c == 0) ? fderiv(ax, pc[k + l])
-                                         : (c == 1) ? dyb[k + l] : fderiv(az, pc[k + l]);
-                    fo[k + l] = cscale(pp.Re, csub(grad, rc[k]));
-                }
-                double2 blo = mk(0, 0), bup = mk(0, 0);
-                if (MODE == MODE_STEP) {
-                    blo = A.step.bc_v[(2 * c) * d.ncol + col];
-                    bup = A.step.bc_v[(2 * c + 1) * d.ncol + col];
-                }
-                ok &= tau_chain(par, ny, g_v, pp.a_V[c], pp.b_V[c], zero_col, blo, bup, wv,
-                                fo + l, rc, adv + l, TC, sWL, sWD, sWR);
-            }
-        }
-        __syncwarp(mask);
-        if (active && par == 0) {
-            // wall divergence by endpoint sums (src/solver/eqsolve_pv.cpp:397-406)
-            double2 div0 = mk(0, 0), div1 = mk(0, 0);
-            for (int y = 0; y <= ny; ++y) {
-                const int k = y * TC + l;
-                const double2 tang = cadd(fderiv(ax, rv[k]), fderiv(az, rv[2 * S + k]));
-                const double2 nrm = cscale((double)(y * y), rv[S + k]);
-                div0 = cadd(div0, cadd(tang, nrm));
-                div1 = (y & 1) ? cadd(div1, cadd(mk(-tang.x, -tang.y), nrm)) : cadd(div1, csub(tang, nrm));
-            }
-            if (MODE == MODE_BASE) {
-                A.divb_out[col] = div0;
-                A.divb_out[d.ncol + col] = div1;
-                s_c0[l] = mk(0, 0);
-                s_c1[l] = mk(0, 0);
-            } else {
-                const double2 i00 = st.inf_div[col], i01 = st.inf_div[d.ncol + col];
-                const double2 i10 = st.inf_div[2 * d.ncol + col], i11 = st.inf_div[3 * d.ncol + col];
-                const double2 c0 = csub(cmul(div1, i10), cmul(div0, i11));
-                const double2 c1 = csub(cmul(div0, i01), cmul(div1, i00));
-                s_c0[l] = c0;
-                s_c1[l] = c1;
-                if (MODE == MODE_STEP) {
-                    // sigma correction (src/solver/eqsolve_pv.cpp:413-429)
-                    const long long base = (long long)kzi * ncy * nkx + kx;
-                    const long long oN = base + (long long)ny * nkx;
-                    const long long oN1 = base + (long long)(ny - 1) * nkx;
-                    const double2 *PI0 = st.p_inf, *PI1 = st.p_inf + d.Ns;
-                    const double2 *VI0 = st.v_inf + d.Ns, *VI1 = st.v_inf + 4 * d.Ns;  // component 1
-                    const double2 ptop = cadd(pc[ny * TC + l], cadd(cmul(c0, PI0[oN]), cmul(c1, PI1[oN])));
-                    const double2 vt0 = cadd(rv[S + ny * TC + l], cadd(cmul(c0, VI0[oN]), cmul(c1, VI1[oN])));
-                    const double2 vt1 = cadd(rv[S + (ny - 1) * TC + l], cadd(cmul(c0, VI0[oN1]), cmul(c1, VI1[oN1])));
-                    const double wv = st.wn_v[col];
-                    const double2 n0 = csub(cscale(-wv, vt0), cscale(pp.Re, tail0));
-                    const double2 n1 = cadd(cscale(-wv, vt1),
-                                            cscale(pp.Re, csub(cscale(2.0 * ny, ptop), tail1)));
-                    s_sig[0][l] = cdiv(n0, st.sigma0[col]);
-                    s_sig[1][l] = cdiv(n1, st.sigma0[d.ncol + col]);
-                }
-            }
-        }
-        if (!ok && active) {
-            unsigned *err = (MODE == MODE_STEP) ? A.step.err : nullptr;
-            if (err) atomicOr(err, ERR_PIVOT);
-        }
-    }
-    __syncthreads();
-
-    // ---- phase C: corrections and single write-back -----------------------
-    const int zero_col = d.NZS * nkx;
-    bool bad = false;
-    for (int i = tid; i < S; i += blockDim.x) {
-        const int y = i / TC, l = i - (i / TC) * TC;
-        const int col = col0 + l;
-        if (col >= d.ncol) continue;
-        const int kzi = col / nkx, kx = col - (col / nkx) * nkx;
-        const long long off = ((long long)kzi * ncy + y) * nkx + kx;
-        const int q = (y + 1) & 1;
-        double2 p = pc[i];
-        double2 v[3] = {rv[i], rv[S + i], rv[2 * S + i]};
-        if (MODE != MODE_BASE) {
-            const double2 c0 = s_c0[l], c1 = s_c1[l];
-            p = cadd(p, cadd(cmul(c0, st.p_inf[off]), cmul(c1, st.p_inf[d.Ns + off])));
-            if (MODE == MODE_STEP) p = cadd(p, cmul(s_sig[q][l], st.p_b[off]));
-            for (int c = 0; c < 3; ++c) {
-                v[c] = cadd(v[c], cadd(cmul(c0, st.v_inf[c * d.Ns + off]),
-                                       cmul(c1, st.v_inf[(3 + c) * d.Ns + off])));
-                if (MODE == MODE_STEP)
-                    v[c] = cadd(v[c], cmul(s_sig[c == 1 ? 1 - q : q][l], st.v_b[c * d.Ns + off]));
-            }
-        }
-        if (MODE == MODE_STEP && !A.step.solve_only && col == zero_col) {
+        if (!s.solve_only && zero_col) {
             // correct_zero_mode (src/solver/timestepper.cpp:60-68)
-            v[1] = (y == 0) ? cscale(0.5, cadd(A.step.bc_v[2 * d.ncol + col], A.step.bc_v[3 * d.ncol + col]))
-                            : mk(0.0, 0.0);
-        }
-        if (MODE == MODE_STEP) {
-            bad |= !(isfinite(p.x) && isfinite(p.y));
-            for (int c = 0; c < 3; ++c) bad |= !(isfinite(v[c].x) && isfinite(v[c].y));
-        }
-        A.p_out[off] = p;
-        for (int c = 0; c < 3; ++c) A.v_out[c * d.Ns + off] = v[c];
-    }
-    if (MODE == MODE_STEP && bad) atomicOr(A.step.err, ERR_NONFINITE);
-    if (MODE == MODE_STEP && !A.step.solve_only && zero_col >= col0 && zero_col < col0 + TC) {
-        // correct_flow (src/sim/simulation.cpp:111-140), single-rank branch
-        __syncthreads();
-        const long long zoff = (long long)d.NZS * ncy * nkx;  // (kz=0, y=0, kx=0)
-        if (tid == 0) {
+            const double2 v1w = cscale(0.5, cadd(s.bc_v[2 * ncol + col], s.bc_v[3 * ncol + col]));
+#pragma unroll
+            for (int e = 0; e < E; ++e) v1[e] = ycoef<E>(e) == 0 ? v1w : mk(0.0, 0.0);
+            // correct_flow (src/sim/simulation.cpp:111-140), single-rank branch
             const double *uu = st.unit;
-            const double qxu = uu[2 * ncy], qzu = uu[2 * ncy + 1];
             double dpdx, dpdz;
             if (pp.grad_pre == 1) {
                 dpdx = pp.gx;
                 dpdz = pp.gz;
             } else {
                 double qx = 0.0, qz = 0.0;
-                for (int y = 0; y <= ny; y += 2) {
-                    qx -= A.v_out[zoff + (long long)y * nkx].x / (double)(y * y - 1);
-                    qz -= A.v_out[2 * d.Ns + zoff + (long long)y * nkx].x / (double)(y * y - 1);
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const int y = ycoef<E>(e);
+                    if (p == 0 && y <= ny) {
+                        qx += v0[e].x / (double)(y * y - 1);
+                        qz += v2[e].x / (double)(y * y - 1);
+                    }
                 }
-                if (!isfinite(qxu) || qxu == 0.0 || !isfinite(qzu) || qzu == 0.0)
-                    atomicOr(A.step.err, ERR_PIVOT);
+                qx = -sum_warp(qx);
+                qz = -sum_warp(qz);
+                const double qxu = uu[2 * ncy], qzu = uu[2 * ncy + 1];
+                if (!isfinite(qxu) || qxu == 0.0 || !isfinite(qzu) || qzu == 0.0) pivot_fail = true;
                 dpdx = (pp.qxm - qx) / qxu;
                 dpdz = (pp.qzm - qz) / qzu;
             }
-            s_dp[0] = dpdx;
-            s_dp[1] = dpdz;
-            A.step.dpdx[0] = dpdx;
-            A.step.dpdx[1] = dpdz;
+            if (L == 0) {
+                s.dpdx[0] = dpdx;
+                s.dpdx[1] = dpdz;
+            }
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const int y = ycoef<E>(e);
+                if (y <= ny) {
+                    v0[e].x += dpdx * uu[y];
+                    v2[e].x += dpdz * uu[ncy + y];
+                }
+            }
         }
-        __syncthreads();
-        for (int y = tid; y <= ny; y += blockDim.x) {
-            A.v_out[zoff + (long long)y * nkx].x += s_dp[0] * st.unit[y];
-            A.v_out[2 * d.Ns + zoff + (long long)y * nkx].x += s_dp[1] * st.unit[ncy + y];
+        // results into the tile (each warp rewrites only its own column's slots)
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int y = ycoef<E>(e);
+            if (y > ny) continue;
+            bad |= !(isfinite(pv[e].x) && isfinite(pv[e].y) && isfinite(v0[e].x) && isfinite(v0[e].y) &&
+                     isfinite(v1[e].x) && isfinite(v1[e].y) && isfinite(v2[e].x) && isfinite(v2[e].y));
+            const int sl = tile_slot<E>(y, w);
+            tile[sl] = pv[e];
+            tile[S + sl] = v0[e];
+            tile[2 * S + sl] = v1[e];
+            tile[3 * S + sl] = v2[e];
         }
-    }
-}
-
-size_t solve_smem(const Dims &d) {
-    const size_t S = (size_t)d.ncy * TC;
-    return sizeof(double2) * 6 * S + sizeof(double) * (2 * S + 3 * (size_t)d.ncy);
-}
-
-// EqSolvePV::build_wn_ad (src/solver/eqsolve_pv.cpp:148-168), one thread per column.
-__global__ void k_wn_ad(Dims d, Tables t, double g, double *wn, double *ad) {
-    const int col = blockIdx.x * blockDim.x + threadIdx.x;
-    if (col >= d.ncol) return;
-    const int kzi = col / d.nkx, kx = col - (col / d.nkx) * d.nkx;
-    const double ax = t.wavx[kx], az = t.wavz[kzi];
-    const double w = -((ax * ax + az * az) + g);
-    wn[col] = w;
-    const int n = d.NYS;
-    double *A = ad + (long long)kzi * d.ncy * d.nkx + kx;
-    const long long s = d.nkx;
-    A[0] = 0.0;
-    A[s] = 0.0;
-    A[n * s] = 1.0 / (1.0 + t.WD[n] * w);
-    A[(n - 1) * s] = 1.0 / (1.0 + t.WD[n - 1] * w);
-    for (int y = n - 2; y >= 2; --y) {
-        const double fc = t.WR[y] * t.WL[y + 2];
-        const double den = 1.0 + (t.WD[y] - (fc * w) * A[(y + 2) * s]) * w;
-        A[y * s] = 1.0 / den;
-    }
-}
-
-// Influence normalisation (src/solver/eqsolve_pv.cpp:282-302).
-__global__ void k_inf_normalize(Dims d, double a_v1, double2 *inf_div) {
-    const int col = blockIdx.x * blockDim.x + threadIdx.x;
-    if (col >= d.ncol) return;
-    double2 *I = inf_div;
-    const int nc = d.ncol;
-    const double2 i00 = I[col], i01 = I[nc + col], i10 = I[2 * nc + col], i11 = I[3 * nc + col];
-    double2 den = csub(cmul(i00, i11), cmul(i01, i10));
-    const bool root = (col == d.NZS * d.nkx);
-    if (root) den = (a_v1 == 0.0) ? mk(1.0, 0.0) : cdiv(mk(0.25, 0.0), i00);
-    if (root) {
-        I[col] = den;
-        I[nc + col] = mk(0, 0);
-        I[2 * nc + col] = den;
-        I[3 * nc + col] = mk(0, 0);
-    } else {
-        I[col] = cdiv(i00, den);
-        I[nc + col] = cdiv(i01, den);
-        I[2 * nc + col] = cdiv(i10, den);
-        I[3 * nc + col] = cdiv(i11, den);
-    }
-}
-
-// sigma0 denominators (src/solver/eqsolve_pv.cpp:466-476).
-__global__ void k_sigma0(Dims d, double re, const double *wn_v, const double2 *p_b,
-                         const double2 *v_b, double2 *sigma0) {
-    const int col = blockIdx.x * blockDim.x + threadIdx.x;
-    if (col >= d.ncol) return;
-    const int kzi = col / d.nkx, kx = col - (col / d.nkx) * d.nkx;
-    const long long base = (long long)kzi * d.ncy * d.nkx + kx;
-    const int n = d.NYS;
-    const double w = wn_v[col];
-    const double2 vbn = v_b[d.Ns + base + (long long)n * d.nkx];
-    const double2 vbn1 = v_b[d.Ns + base + (long long)(n - 1) * d.nkx];
-    const double2 pbn = p_b[base + (long long)n * d.nkx];
-    sigma0[col] = mk(re + w * vbn.x, w * vbn.y);
-    double2 s1 = csub(mk(re + w * vbn1.x, w * vbn1.y), cscale(re * (2.0 * n), pbn));
-    if (col == d.NZS * d.nkx) s1 = mk(1.0, 0.0);
-    sigma0[d.ncol + col] = s1;
-}
-
-// Unit pressure-gradient responses of the zero mode
-// (src/solver/eqsolve_pv.cpp:479-493): two threads (parities), one column.
-__global__ void k_unit_response(Dims d, Tables t, PhysParams pp, double g_v, const double *ad_v,
-                                double *unit) {
-    extern __shared__ double2 su[];
-    const int ncy = d.ncy, ny = d.NYS;
-    double2 *r = su;
-    double2 *o = r + ncy;
-    double *ad = reinterpret_cast<double *>(o + ncy);
-    double *WL = ad + ncy, *WD = WL + ncy, *WR = WD + ncy;
-    const int par = threadIdx.x;
-    const long long zc = (long long)d.NZS * ncy * d.nkx;
-    for (int y = par; y < ncy; y += 2) {
-        r[y] = mk(y == 0 ? pp.Re : 0.0, 0.0);
-        ad[y] = ad_v[zc + (long long)y * d.nkx];
-        WL[y] = t.WL[y];
-        WD[y] = t.WD[y];
-        WR[y] = t.WR[y];
+        const unsigned flags = (__any_sync(kFull, bad) ? ERR_NONFINITE : 0u) |
+                               (__any_sync(kFull, pivot_fail) ? ERR_PIVOT : 0u);
+        if (flags && L == 0) atomicOr(s.err, flags);
     }
     __syncthreads();
-    const double w = -((0.0 + 0.0) + g_v);
-    for (int pass = 0; pass < 2; ++pass) {
-        const int c = pass == 0 ? 0 : 2;
-        tau_chain(par, ny, g_v, pp.a_V[c], pp.b_V[c], true, mk(0, 0), mk(0, 0), w, r, o, ad, 1, WL,
-                  WD, WR);
-        __syncthreads();
-        if (par == 0) {
-            double q = 0.0;
-            for (int y = 0; y <= ny; y += 2) q -= o[y].x / (double)(y * y - 1);
-            unit[2 * ncy + pass] = q;
-            for (int y = 0; y <= ny; ++y) unit[pass * ncy + y] = o[y].x;
-        }
-        __syncthreads();
+    for (int i = tid; i < S; i += kThreads) {
+        const int y = i / TC, l = i - (i / TC) * TC;
+        const int c2 = col0 + l;
+        if (c2 >= ncol) continue;
+        const int kzi = c2 / nkx, kx = c2 - (c2 / nkx) * nkx;
+        const long long off = ((long long)kzi * ncy + y) * nkx + kx;
+        const int sl = tile_slot<E>(y, l);
+        A.p_out[off] = tile[sl];
+        A.v_out[off] = tile[S + sl];
+        A.v_out[d.Ns + off] = tile[2 * S + sl];
+        A.v_out[2 * d.Ns + off] = tile[3 * S + sl];
     }
 }
+
+size_t solve_smem(const Dims &d) { return sizeof(double2) * 4 * (size_t)d.ncy * TC; }
+
+// Elements per lane for NYS + 1 coefficients (1, 2, 4 or 8; 0 if too many).
+int lane_elems(const Dims &d) {
+    const int e = (d.ncy + 31) / 32;
+    return e <= 1 ? 1 : e <= 2 ? 2 : e <= 4 ? 4 : e <= 8 ? 8 : 0;
+}
+
 __global__ void k_pressure_bc(Dims d, const double2 *N, const double2 *bw, double2 *B) {
     const int col = blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= d.ncol) return;
@@ -478,6 +579,18 @@ __global__ void k_pressure_bc(Dims d, const double2 *N, const double2 *bw, doubl
     B[col] = cadd(bw[col], st_);
     B[d.ncol + col] = cadd(bw[d.ncol + col], sb_);
 }
+
+template <int E>
+cudaError_t configure_e(const Dims &d) {
+    return cudaFuncSetAttribute(k_solve<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem(d));
+}
+
+template <int E>
+void step_e(const Dims &d, const Tables &t, const PhysParams &pp, double g_v, const SolverState &st,
+            const SolveArgs &A, cudaStream_t s) {
+    const int blocks = (d.ncol + TC - 1) / TC;
+    k_solve<E><<<blocks, kThreads, solve_smem(d), s>>>(d, t, pp, g_v, st, A);
+}
 }  // namespace
 
 void launch_pressure_bc(const Dims &d, const double2 *N, const double2 *bw, double2 *B,
@@ -486,45 +599,15 @@ void launch_pressure_bc(const Dims &d, const double2 *N, const double2 *bw, doub
 }
 
 cudaError_t configure_solver_kernels(const Dims &d) {
-    const int sm = (int)solve_smem(d);
-    cudaError_t e = cudaFuncSetAttribute(k_solve<MODE_STEP>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaError_t e = configure_setup_kernels(d);
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_solve<MODE_BASE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_solve<MODE_COUPLED>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-}
-
-void setup_solver(const Dims &d, const Tables &t, const PhysParams &pp, double g_v, SolverState &st,
-                  double2 *, cudaStream_t s) {
-    const int nb = (d.ncol + 127) / 128;
-    k_wn_ad<<<nb, 128, 0, s>>>(d, t, pp.G_pre, st.wn_p, st.ad_p);
-    k_wn_ad<<<nb, 128, 0, s>>>(d, t, g_v, st.wn_v, st.ad_v);
-    const int blocks = (d.ncol + TC - 1) / TC;
-    const size_t sm = solve_smem(d);
-    // influence responses: pressure Dirichlet data (1,0) and (0,1)
-    for (int i = 0; i < 2; ++i) {
-        SolveArgs A{};
-        A.p_a = 1.0;
-        A.p_b = 0.0;
-        A.bcp_top = mk((double)(1 - i), 0.0);
-        A.bcp_bot = mk((double)i, 0.0);
-        A.p_out = st.p_inf + (long long)i * d.Ns;
-        A.v_out = st.v_inf + (long long)i * 3 * d.Ns;
-        A.divb_out = st.inf_div + (long long)i * 2 * d.ncol;
-        k_solve<MODE_BASE><<<blocks, kThreads, sm, s>>>(d, t, pp, g_v, st, A);
+    switch (lane_elems(d)) {
+    case 1: return configure_e<1>(d);
+    case 2: return configure_e<2>(d);
+    case 4: return configure_e<4>(d);
+    case 8: return configure_e<8>(d);
+    default: return cudaErrorInvalidValue;   // more than 256 Chebyshev coefficients
     }
-    k_inf_normalize<<<nb, 128, 0, s>>>(d, pp.a_V[1], st.inf_div);
-    {
-        SolveArgs A{};
-        A.p_a = 1.0;
-        A.p_b = 0.0;
-        A.p_out = st.p_b;
-        A.v_out = st.v_b;
-        k_solve<MODE_COUPLED><<<blocks, kThreads, sm, s>>>(d, t, pp, g_v, st, A);
-    }
-    k_sigma0<<<nb, 128, 0, s>>>(d, pp.Re, st.wn_v, st.p_b, st.v_b, st.sigma0);
-    const size_t smu = sizeof(double2) * 2 * d.ncy + sizeof(double) * 4 * d.ncy;
-    k_unit_response<<<1, 2, smu, s>>>(d, t, pp, g_v, st.ad_v, st.unit);
 }
 
 void launch_step_solve(const Dims &d, const Tables &t, const PhysParams &pp, double g_v,
@@ -535,8 +618,13 @@ void launch_step_solve(const Dims &d, const Tables &t, const PhysParams &pp, dou
     A.p_out = a.p_out;
     A.v_out = a.u_out;
     A.step = a;
-    const int blocks = (d.ncol + TC - 1) / TC;
-    k_solve<MODE_STEP><<<blocks, kThreads, solve_smem(d), s>>>(d, t, pp, g_v, st, A);
+    switch (lane_elems(d)) {
+    case 1: step_e<1>(d, t, pp, g_v, st, A, s); break;
+    case 2: step_e<2>(d, t, pp, g_v, st, A, s); break;
+    case 4: step_e<4>(d, t, pp, g_v, st, A, s); break;
+    case 8: step_e<8>(d, t, pp, g_v, st, A, s); break;
+    default: break;
+    }
 }
 
 }  // namespace cdns
