@@ -28,6 +28,8 @@ struct Tables {
     const double *wavz;   // [nkz]  kz*2pi/ZL
     const double *WL, *WD, *WR;  // [ncy] Chebyshev integration weights
     const double *cosy;   // [2*NY2] cos(pi m / NY2)
+    const double *csyn;   // Chebyshev synthesis matrix (chebyshev.cu)
+    const double *cana;   // Chebyshev analysis matrix (chebyshev.cu)
     const double2 *root_x;  // [NX2] exp(-2 pi i k / NX2)
     const double2 *root_z;  // [NZ2] exp(-2 pi i k / NZ2)
 };

@@ -6,18 +6,27 @@
 
 namespace cdns {
 
+// ---- chebyshev.cu ----
+void cheb_table_sizes(const Dims &d, size_t *nsyn, size_t *nana);
+// cana may be null (synthesis matrix only)
+void launch_cheb_tables(const Dims &d, const double *cosy, double *csyn, double *cana, cudaStream_t s);
+cudaError_t configure_cheb_kernels(const Dims &d);
+// vorticity om[3][Ns] of u[3][Ns] and its pressure-wall sums bw[2][ncol] (bw may be null)
+void launch_curl(const Dims &d, const Tables &t, const double2 *u, double2 *om, double2 *bw, double re,
+                 cudaStream_t s);
+// F[f][j][col] of nf spectral fields: f < nsplit from src0, the others from src1
+void launch_ysynth(const Dims &d, const Tables &t, const double2 *src0, const double2 *src1, int nsplit,
+                   int nf, double2 *F, cudaStream_t s);
+void launch_yanalysis(const Dims &d, const Tables &t, const double2 *F, double2 *S, int nf, cudaStream_t s);
+
 // ---- transforms.cu ----
 cudaError_t configure_transform_kernels(const Dims &d);
-void launch_curl_ysynth(const Dims &d, const Tables &t, const double2 *u, double2 *F, double2 *bw,
-                        double re, bool curl, cudaStream_t s);
 void launch_z_backward(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *F,
                        double2 *G, int nf, cudaStream_t s);
 void launch_x_cross(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G,
                     double2 *H, cudaStream_t s);
 void launch_z_forward(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *H,
                       double2 *F, int nf, cudaStream_t s);
-void launch_y_analysis(const Dims &d, const Tables &t, const double2 *F, double2 *S, int nf,
-                       cudaStream_t s);
 void launch_x_c2r(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G,
                   double *phys, cudaStream_t s);
 void launch_x_r2c(const Dims &d, const FftPlan &P, const double2 *roots, const double *phys,

@@ -41,9 +41,9 @@ namespace {
             return fail(CDNS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
-constexpr int kStages = 6;
-const char *kStageNames[kStages] = {"curl_ysynth", "z_backward", "x_cross",
-                                    "z_forward",   "y_analysis", "solve"};
+constexpr int kStages = 7;
+const char *kStageNames[kStages] = {"curl", "y_synthesis", "z_backward", "x_cross",
+                                    "z_forward", "y_analysis", "solve"};
 constexpr int kMaxProfSteps = 256;
 
 bool plan_fft(int n, FftPlan &p) {
@@ -84,6 +84,7 @@ struct cdns_ctx {
     int cur = 0;                          // U[cur] = u, Nb[cur] = next N, Bb[cur] = next B
     double2 *p = nullptr, *bw = nullptr, *bc_v = nullptr, *bc_p = nullptr;
     double2 *F = nullptr, *G = nullptr, *H = nullptr, *aux = nullptr, *aux2 = nullptr, *zero3 = nullptr;
+    double2 *om = nullptr;                // vorticity of the velocity being transformed
     double *phys = nullptr;
     double *dpdx = nullptr;
     unsigned *err = nullptr;
@@ -137,16 +138,18 @@ void enqueue_nonlinear(cdns_ctx *c, const double2 *u, double2 *N, bool prof, int
         if (prof) cudaEventRecord(c->ev[(size_t)step_slot * (kStages + 1) + stage], s);
     };
     mark(0);
-    launch_curl_ysynth(d, c->t, u, c->F, c->bw, c->pp.Re, true, s);
+    launch_curl(d, c->t, u, c->om, c->bw, c->pp.Re, s);
     mark(1);
-    launch_z_backward(d, c->pz, c->t.root_z, c->F, c->G, 6, s);
+    launch_ysynth(d, c->t, u, c->om, 3, 6, c->F, s);
     mark(2);
-    launch_x_cross(d, c->px, c->t.root_x, c->G, c->H, s);
+    launch_z_backward(d, c->pz, c->t.root_z, c->F, c->G, 6, s);
     mark(3);
-    launch_z_forward(d, c->pz, c->t.root_z, c->H, c->F, 3, s);
+    launch_x_cross(d, c->px, c->t.root_x, c->G, c->H, s);
     mark(4);
-    launch_y_analysis(d, c->t, c->F, N, 3, s);
+    launch_z_forward(d, c->pz, c->t.root_z, c->H, c->F, 3, s);
     mark(5);
+    launch_yanalysis(d, c->t, c->F, N, 3, s);
+    mark(6);
 }
 
 void enqueue_step_body(cdns_ctx *c, double a0, double a1, double b0, double b1, double g_v,
@@ -336,6 +339,15 @@ int cdns_create(const cdns_mesh_desc *m, const cdns_params *p, int precision, in
     auto pzz = put(rz.data(), 2 * rz.size()); c->t.root_z = reinterpret_cast<const double2 *>(pzz.first);
     if (pw.second || pz.second || pl.second || pd.second || pr.second || pc.second || px.second || pzz.second)
         return bail(CDNS_ERR_CUDA);
+    {
+        size_t nsyn, nana;
+        cheb_table_sizes(d, &nsyn, &nana);
+        double *csyn = nullptr, *cana = nullptr;
+        if ((r = c->alloc(csyn, nsyn)) || (r = c->alloc(cana, nana))) return bail(r);
+        launch_cheb_tables(d, c->t.cosy, csyn, cana, c->stream);
+        c->t.csyn = csyn;
+        c->t.cana = cana;
+    }
     // ---- state and workspaces ----
     const size_t Ns = (size_t)d.Ns, nc = d.ncol;
     const size_t fbuf = 6 * (size_t)d.ny2 * nc;
@@ -347,7 +359,7 @@ int cdns_create(const cdns_mesh_desc *m, const cdns_params *p, int precision, in
         (r = c->alloc(c->p, Ns)) || (r = c->alloc(c->bw, 2 * nc)) || (r = c->alloc(c->bc_v, 6 * nc)) ||
         (r = c->alloc(c->bc_p, 2 * nc)) || (r = c->alloc(c->F, fbuf)) || (r = c->alloc(c->G, gbuf)) ||
         (r = c->alloc(c->H, hbuf)) || (r = c->alloc(c->aux, 3 * Ns)) || (r = c->alloc(c->aux2, 3 * Ns)) ||
-        (r = c->alloc(c->zero3, 3 * Ns)) ||
+        (r = c->alloc(c->zero3, 3 * Ns)) || (r = c->alloc(c->om, 3 * Ns)) ||
         (r = c->alloc(c->phys, (size_t)d.NZ2 * d.ny2 * d.NX2)) || (r = c->alloc(c->dpdx, 2)) ||
         (r = c->alloc(c->err, 1)))
         return bail(r);
@@ -358,6 +370,7 @@ int cdns_create(const cdns_mesh_desc *m, const cdns_params *p, int precision, in
         (r = c->alloc(st.sigma0, 2 * nc)) || (r = c->alloc(st.unit, 2 * (size_t)d.ncy + 2)))
         return bail(r);
     cudaError_t e = configure_transform_kernels(d);
+    if (e == cudaSuccess) e = configure_cheb_kernels(d);
     if (e == cudaSuccess) e = configure_solver_kernels(d);
     if (e != cudaSuccess) return bail(fail(CDNS_ERR_CUDA, cudaGetErrorString(e)));
     // velocity_boundary (src/sim/initial_bc.cpp:95-101): v = V_Microblow0 on the zero mode
@@ -527,7 +540,7 @@ int cdns_transform_fine(cdns_ctx *c, int dir, const double *in, double *out) {
     const size_t nphys = (size_t)d.NZ2 * d.ny2 * d.NX2;
     if (dir == 'B') {
         CK(cudaMemcpyAsync(c->aux, in, sizeof(double2) * d.Ns, cudaMemcpyHostToDevice, c->stream));
-        launch_curl_ysynth(d, c->t, c->aux, c->F, c->bw, c->pp.Re, false, c->stream);
+        launch_ysynth(d, c->t, c->aux, nullptr, 1, 1, c->F, c->stream);
         launch_z_backward(d, c->pz, c->t.root_z, c->F, c->G, 1, c->stream);
         launch_x_c2r(d, c->px, c->t.root_x, c->G, c->phys, c->stream);
         CK(cudaGetLastError());
@@ -536,7 +549,7 @@ int cdns_transform_fine(cdns_ctx *c, int dir, const double *in, double *out) {
         CK(cudaMemcpyAsync(c->phys, in, sizeof(double) * nphys, cudaMemcpyHostToDevice, c->stream));
         launch_x_r2c(d, c->px, c->t.root_x, c->phys, c->H, c->stream);
         launch_z_forward(d, c->pz, c->t.root_z, c->H, c->F, 1, c->stream);
-        launch_y_analysis(d, c->t, c->F, c->aux, 1, c->stream);
+        launch_yanalysis(d, c->t, c->F, c->aux, 1, c->stream);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(out, c->aux, sizeof(double2) * d.Ns, cudaMemcpyDeviceToHost, c->stream));
     } else {

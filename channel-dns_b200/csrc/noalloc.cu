@@ -120,9 +120,12 @@ extern "C" int cdns_transform_fine_backward_noalloc(const cdns_mesh_desc *m, con
     const size_t b_cos = align256(sizeof(double) * 2 * (size_t)d.NY2);
     const size_t b_rx = align256(sizeof(double2) * (size_t)d.NX2);
     const size_t b_rz = align256(sizeof(double2) * (size_t)d.NZ2);
+    size_t nsyn, nana;
+    cheb_table_sizes(d, &nsyn, &nana);
+    const size_t b_syn = align256(sizeof(double) * nsyn);
     const size_t b_F = align256(sizeof(double2) * (size_t)d.ny2 * d.ncol);
     const size_t b_G = align256(sizeof(double2) * (size_t)d.ny2 * d.NZ2 * d.nkx);
-    const size_t need = b_wavx + b_wavz + b_cos + b_rx + b_rz + b_F + b_G;
+    const size_t need = b_wavx + b_wavz + b_cos + b_rx + b_rz + b_syn + b_F + b_G;
     if (need > kScratchBytes) {
         char msg[200];
         std::snprintf(msg, sizeof msg,
@@ -141,6 +144,7 @@ extern "C" int cdns_transform_fine_backward_noalloc(const cdns_mesh_desc *m, con
     double *cosy = reinterpret_cast<double *>(p); p += b_cos;
     double2 *root_x = reinterpret_cast<double2 *>(p); p += b_rx;
     double2 *root_z = reinterpret_cast<double2 *>(p); p += b_rz;
+    double *csyn = reinterpret_cast<double *>(p); p += b_syn;
     double2 *F = reinterpret_cast<double2 *>(p); p += b_F;
     double2 *G = reinterpret_cast<double2 *>(p);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -148,7 +152,9 @@ extern "C" int cdns_transform_fine_backward_noalloc(const cdns_mesh_desc *m, con
     const int nt = std::max(std::max(d.nkx, d.nkz), std::max(2 * d.NY2, std::max(d.NX2, d.NZ2)));
     k_noalloc_tables<<<(nt + 127) / 128, 128, 0, s>>>(d, 2.0 * pi / m->XL, 2.0 * pi / m->ZL, wavx,
                                                        wavz, cosy, root_x, root_z);
+    launch_cheb_tables(d, cosy, csyn, nullptr, s);
     Tables t{};
+    t.csyn = csyn;
     t.wavx = wavx;
     t.wavz = wavz;
     t.cosy = cosy;
@@ -156,7 +162,7 @@ extern "C" int cdns_transform_fine_backward_noalloc(const cdns_mesh_desc *m, con
     t.root_z = root_z;
     // Every element of F and G is written before it is read, so nothing in
     // the scratch needs clearing between calls.
-    launch_curl_ysynth(d, t, reinterpret_cast<const double2 *>(spectral), F, nullptr, 1.0, false, s);
+    launch_ysynth(d, t, reinterpret_cast<const double2 *>(spectral), nullptr, 1, 1, F, s);
     launch_z_backward(d, pz, root_z, F, G, 1, s);
     launch_x_c2r(d, px, root_x, G, physical, s);
     e = cudaGetLastError();

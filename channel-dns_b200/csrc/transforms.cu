@@ -7,141 +7,13 @@
 //   Xspec      H[f][j][z][kx]           products after the forward x FFT
 //   Zspec      F[f][j][kz][kx]          after the forward z FFT
 //
-// Reference semantics (src/fft/transforms.cpp:615-741): the synthesis is the
-// unnormalised DCT-I of the zero-padded column with c_0 doubled, followed by
-// the 0.5 z-expansion factor; both factors are powers of two, so they are
-// folded into f_j = sum_k w_k c_k cos(pi j k / NY2) (w_k = 1, or 1/2 for
-// k = NY2).  The analysis keeps x1/NX2 before the z FFT, x1/NZ2 after it, and
-// DCT-I scaling 1/(2 NY2) at k=0, 1/NY2 otherwise.
+// The Chebyshev (y) synthesis and analysis live in chebyshev.cu; this file
+// holds the Fourier directions (src/fft/transforms.cpp:615-741): the analysis
+// keeps x1/NX2 before the z FFT and x1/NZ2 after it.
 #include "cdns_kernels.cuh"
 #include "fft_lines.cuh"
 
 namespace cdns {
-
-// ---------------------------------------------------------------------------
-// K1: curl + Chebyshev synthesis, one thread per (spectral column, JT point
-// pairs).  The even/odd split f_j = E_j + O_j, f_{NY2-j} = E_j - O_j halves
-// the multiply-adds.  The curl's y-derivative recurrence
-// (src/solver/vector_ops.cpp:17-25, :112-151) runs along the descending
-// coefficient loop in registers.  Row group 0 also accumulates the vorticity
-// part of the pressure wall condition (src/solver/timestepper.cpp:26-43).
-// ---------------------------------------------------------------------------
-template <int JT, bool CURL>
-__global__ void __launch_bounds__(128)
-k_curl_ysynth(Dims d, Tables t, const double2 *__restrict__ u, double2 *__restrict__ F,
-              double2 *__restrict__ bw, double inv_re_unused, double re) {
-    constexpr int NF = CURL ? 6 : 1;
-    extern __shared__ double s_cos[];
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    const int twoN = 2 * d.NY2;
-    for (int i = tid; i < twoN; i += blockDim.x * blockDim.y) s_cos[i] = t.cosy[i];
-    __syncthreads();
-    const int col = blockIdx.x * blockDim.x + threadIdx.x;
-    const int g = blockIdx.y * blockDim.y + threadIdx.y;
-    const int j0 = g * JT;
-    if (col >= d.ncol || j0 >= d.nyh) return;
-    const int kzi = col / d.nkx;
-    const int kx = col - kzi * d.nkx;
-    const double ax = t.wavx[kx], az = t.wavz[kzi];
-    const double2 *U = u + (long long)kzi * d.ncy * d.nkx + kx;
-    const double2 *V = U + d.Ns;
-    const double2 *W = V + d.Ns;
-    const int nys = d.NYS;
-    int idx[JT];
-#pragma unroll
-    for (int q = 0; q < JT; ++q) idx[q] = ((j0 + q) * nys) % twoN;
-    double2 accE[JT][NF], accO[JT][NF];
-#pragma unroll
-    for (int q = 0; q < JT; ++q)
-#pragma unroll
-        for (int f = 0; f < NF; ++f) accE[q][f] = accO[q][f] = mk(0.0, 0.0);
-    double2 u1 = mk(0, 0), w1 = mk(0, 0), du1 = mk(0, 0), du2 = mk(0, 0), dw1 = mk(0, 0),
-            dw2 = mk(0, 0);
-    double2 btop = mk(0, 0), bbot = mk(0, 0);
-    const bool wall_sums = CURL && g == 0;
-    const double axr = ax / re, azr = az / re;
-    for (int k = nys; k >= 0; --k) {
-        double2 fld[NF];
-        const double2 uk = U[(long long)k * d.nkx];
-        if (CURL) {
-            const double2 vk = V[(long long)k * d.nkx];
-            const double2 wk = W[(long long)k * d.nkx];
-            double2 duk, dwk;
-            if (k == nys) {
-                duk = mk(0, 0);
-                dwk = mk(0, 0);
-            } else {
-                const double s = (double)(2 * (k + 1));
-                duk = cadd(du2, cscale(s, u1));
-                dwk = cadd(dw2, cscale(s, w1));
-            }
-            if (k == 0) {
-                duk = cscale(0.5, duk);
-                dwk = cscale(0.5, dwk);
-            }
-            du2 = du1; du1 = duk; u1 = uk;
-            dw2 = dw1; dw1 = dwk; w1 = wk;
-            const double2 ox = csub(dwk, fderiv(az, vk));
-            const double2 oy = csub(fderiv(az, uk), fderiv(ax, wk));
-            const double2 oz = csub(fderiv(ax, vk), duk);
-            fld[0] = uk;
-            if (NF == 6) {
-                fld[1] = vk; fld[2] = wk; fld[3] = ox; fld[4] = oy; fld[5] = oz;
-            }
-            if (wall_sums) {
-                const double2 wall = csub(fderiv(axr, oz), fderiv(azr, ox));
-                btop = cadd(btop, wall);
-                bbot = (k & 1) ? cadd(bbot, wall) : csub(bbot, wall);
-            }
-        } else {
-            fld[0] = uk;
-        }
-        const double wgt = (k == d.NY2) ? 0.5 : 1.0;
-        if (k & 1) {
-#pragma unroll
-            for (int q = 0; q < JT; ++q) {
-                const double c = s_cos[idx[q]] * wgt;
-#pragma unroll
-                for (int f = 0; f < NF; ++f) {
-                    accO[q][f].x += c * fld[f].x;
-                    accO[q][f].y += c * fld[f].y;
-                }
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < JT; ++q) {
-                const double c = s_cos[idx[q]] * wgt;
-#pragma unroll
-                for (int f = 0; f < NF; ++f) {
-                    accE[q][f].x += c * fld[f].x;
-                    accE[q][f].y += c * fld[f].y;
-                }
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < JT; ++q) {
-            idx[q] -= j0 + q;
-            if (idx[q] < 0) idx[q] += twoN;
-        }
-    }
-    if (wall_sums) {
-        bw[col] = btop;
-        bw[d.ncol + col] = bbot;
-    }
-    const long long plane = (long long)d.ncol;
-#pragma unroll
-    for (int q = 0; q < JT; ++q) {
-        const int j = j0 + q;
-        if (j >= d.nyh) break;
-        const int jm = d.NY2 - j;
-#pragma unroll
-        for (int f = 0; f < NF; ++f) {
-            double2 *Ff = F + (long long)f * d.ny2 * plane;
-            Ff[(long long)j * plane + col] = cadd(accE[q][f], accO[q][f]);
-            if (jm != j) Ff[(long long)jm * plane + col] = csub(accE[q][f], accO[q][f]);
-        }
-    }
-}
 
 // ---------------------------------------------------------------------------
 // K2: inverse z FFT.  Block = one (field, y point) plane x TL kx lines.  The
@@ -321,63 +193,6 @@ k_x_cross(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 *_
 }
 
 // ---------------------------------------------------------------------------
-// K5a: Chebyshev analysis (DCT-I) of the products, keep k <= NYS.  One thread
-// per (spectral column, KT coefficients); symmetric pairs e_j = x_j + x_{N-j},
-// o_j = x_j - x_{N-j} feed the even / odd coefficients.
-// ---------------------------------------------------------------------------
-template <int KT>
-__global__ void __launch_bounds__(128)
-k_y_analysis(Dims d, Tables t, const double2 *__restrict__ F, double2 *__restrict__ S, int nf) {
-    extern __shared__ double s_cos[];
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    const int N = d.NY2, twoN = 2 * N;
-    for (int i = tid; i < twoN; i += blockDim.x * blockDim.y) s_cos[i] = t.cosy[i];
-    __syncthreads();
-    const int fc = blockIdx.x * blockDim.x + threadIdx.x;
-    const int g = blockIdx.y * blockDim.y + threadIdx.y;
-    const int k0 = g * KT;
-    if (fc >= nf * d.ncol || k0 > d.NYS) return;
-    const int f = fc / d.ncol, col = fc - (fc / d.ncol) * d.ncol;
-    const double2 *X = F + (long long)f * d.ny2 * d.ncol + col;
-    double2 acc[KT];
-    int idx[KT];
-#pragma unroll
-    for (int q = 0; q < KT; ++q) { acc[q] = mk(0, 0); idx[q] = 0; }
-    for (int j = 0; j < d.nyh; ++j) {
-        const double2 xa = X[(long long)j * d.ncol];
-        double2 e, o;
-        if (N - j == j) {
-            e = xa;
-            o = mk(0, 0);
-        } else {
-            const double2 xb = X[(long long)(N - j) * d.ncol];
-            e = cadd(xa, xb);
-            o = csub(xa, xb);
-        }
-        const double wgt = (j == 0) ? 1.0 : 2.0;
-#pragma unroll
-        for (int q = 0; q < KT; ++q) {
-            const int k = k0 + q;
-            const double c = s_cos[idx[q]] * wgt;
-            const double2 src = (k & 1) ? o : e;
-            acc[q].x += c * src.x;
-            acc[q].y += c * src.y;
-            idx[q] += k;
-            if (idx[q] >= twoN) idx[q] -= twoN;
-        }
-    }
-    const int kzi = col / d.nkx, kx = col - (col / d.nkx) * d.nkx;
-    double2 *Sf = S + (long long)f * d.Ns + (long long)kzi * d.ncy * d.nkx + kx;
-#pragma unroll
-    for (int q = 0; q < KT; ++q) {
-        const int k = k0 + q;
-        if (k > d.NYS) break;
-        const double s = (k == 0) ? 1.0 / (2.0 * N) : 1.0 / (double)N;
-        Sf[(long long)k * d.nkx] = cscale(s, acc[q]);
-    }
-}
-
-// ---------------------------------------------------------------------------
 // Single-field x transforms for the standalone fine transform (tests and
 // to-physical output): c2r / r2c of one real field [z][j][x].
 // ---------------------------------------------------------------------------
@@ -459,8 +274,6 @@ k_x_r2c(Dims d, FftPlan P, const double2 *__restrict__ roots, const double *__re
 // Host launchers
 // ---------------------------------------------------------------------------
 namespace {
-constexpr int kJT = 2;
-constexpr int kKT = 8;
 constexpr int kRW = 4;
 constexpr int kRWs = 8;
 }  // namespace
@@ -501,16 +314,6 @@ cudaError_t configure_transform_kernels(const Dims &d) {
     return e;
 }
 
-void launch_curl_ysynth(const Dims &d, const Tables &t, const double2 *u, double2 *F, double2 *bw,
-                        double re, bool curl, cudaStream_t s) {
-    dim3 block(32, 4);
-    const int groups = (d.nyh + kJT - 1) / kJT;
-    dim3 grid((d.ncol + 31) / 32, (groups + 3) / 4);
-    const size_t sm = sizeof(double) * 2 * d.NY2;
-    if (curl) k_curl_ysynth<kJT, true><<<grid, block, sm, s>>>(d, t, u, F, bw, 0.0, re);
-    else k_curl_ysynth<kJT, false><<<grid, block, sm, s>>>(d, t, u, F, bw, 0.0, re);
-}
-
 void launch_z_backward(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *F,
                        double2 *G, int nf, cudaStream_t s) {
     const int tl = z_lines(d);
@@ -529,14 +332,6 @@ void launch_z_forward(const Dims &d, const FftPlan &P, const double2 *roots, con
     const int tl = z_lines(d);
     dim3 grid((d.nkx + tl - 1) / tl, d.ny2, nf);
     k_z_forward<<<grid, 256, smem_zfft(d), s>>>(d, P, roots, H, F, tl);
-}
-
-void launch_y_analysis(const Dims &d, const Tables &t, const double2 *F, double2 *S, int nf,
-                       cudaStream_t s) {
-    dim3 block(32, 4);
-    const int groups = (d.ncy + kKT - 1) / kKT;
-    dim3 grid((nf * d.ncol + 31) / 32, (groups + 3) / 4);
-    k_y_analysis<kKT><<<grid, block, sizeof(double) * 2 * d.NY2, s>>>(d, t, F, S, nf);
 }
 
 void launch_x_c2r(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G,
