@@ -36,13 +36,12 @@ void launch_x_r2c(const Dims &d, const FftPlan &P, const double2 *roots, const d
 // Precomputed solver state (EqSolvePV members, src/solver/eqsolve_pv.hpp:60-76).
 struct SolverState {
     double *wn_p, *wn_v;        // [ncol]
-    // pivots and solution fields are column-major: [..][col][y]
-    double *ad_p, *ad_v;        // [ncol][ncy]
-    double2 *p_inf;             // [2][ncol][ncy]
-    double2 *v_inf;             // [2][3][ncol][ncy]
+    double *ad_p, *ad_v;        // [ncol][ncy] (column-major)
+    double2 *p_inf;             // [2][Ns] planar
+    double2 *v_inf;             // [2][3][Ns] planar
     double2 *inf_div;           // [2 (response)][2 (wall)][ncol]
-    double2 *p_b;               // [ncol][ncy]
-    double2 *v_b;               // [3][ncol][ncy]
+    double2 *p_b;               // [Ns] planar
+    double2 *v_b;               // [3][Ns] planar
     double2 *sigma0;            // [2][ncol]
     double *unit;               // [2][ncy] u_dpdx_unit, w_dpdz_unit ; [2*ncy..] qx, qz
 };

@@ -678,7 +678,7 @@ int cdns_debug_copy(cdns_ctx *c, int which, double *out, size_t count) {
         return CDNS_OK;
     }
     case 5: src = c->st.inf_div; n = 4 * (size_t)d.ncol; break;
-    case 6: src = c->st.v_inf; n = 6 * (size_t)d.Ns; break;   // column-major on the device
+    case 6: src = c->st.v_inf; n = 6 * (size_t)d.Ns; break;
     case 7: src = c->st.p_inf; n = 2 * (size_t)d.Ns; break;
     case 8: src = c->st.sigma0; n = 2 * (size_t)d.ncol; break;
     case 9: src = c->st.wn_p; n = (size_t)d.ncol; break;   // wn_p then wn_v as [2][ncol] doubles
@@ -689,21 +689,6 @@ int cdns_debug_copy(cdns_ctx *c, int which, double *out, size_t count) {
         CK(cudaMemcpyAsync(out, c->st.wn_p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         CK(cudaMemcpyAsync(out + n, c->st.wn_v, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
-        return CDNS_OK;
-    }
-    if (which == 6 || which == 7) {
-        // influence fields are stored [field][col][y]; return them [field][kz][y][kx]
-        std::vector<double2> h(n);
-        CK(cudaMemcpyAsync(h.data(), src, n * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
-        double2 *o = reinterpret_cast<double2 *>(out);
-        const size_t nf = n / (size_t)d.Ns;
-        for (size_t f = 0; f < nf; ++f)
-            for (int col = 0; col < d.ncol; ++col) {
-                const int kz = col / d.nkx, kx = col % d.nkx;
-                for (int y = 0; y < d.ncy; ++y)
-                    o[f * d.Ns + ((size_t)kz * d.ncy + y) * d.nkx + kx] = h[f * d.Ns + (size_t)col * d.ncy + y];
-            }
         return CDNS_OK;
     }
     CK(cudaMemcpyAsync(out, src, n * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));

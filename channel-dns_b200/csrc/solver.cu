@@ -13,12 +13,14 @@
 // reference's sequential sums and recurrences; the results agree with the
 // sequential order to round-off (tested against the oracle at 1e-10).
 //
-// The step solve reads and writes the spectral state in its planar
-// [kz][y][kx] layout through swizzled shared-memory tiles (a block of TC
-// warps owns TC consecutive columns, so every global access is a coalesced
-// row of TC columns).  The precomputed influence and B-problem fields and the
-// tau pivots (solver_setup.cu) are stored column-major ([col][y]) and read by
-// each warp directly.
+// The step solve reads the spectral state in its planar [kz][y][kx] layout
+// through swizzled shared-memory tiles (a block of TC warps owns TC
+// consecutive columns, so every global access is a coalesced row of TC
+// columns).  The warps leave the uncorrected solution in the tiles together
+// with four coefficients per column; the influence-matrix and sigma
+// corrections then run over the block as one coalesced elementwise pass over
+// the planar influence and B-problem fields (solver_setup.cu).  The tau
+// pivots are stored column-major ([col][y]) and read by each warp directly.
 #include "cdns_kernels.cuh"
 #include "warp_columns.cuh"
 
@@ -155,6 +157,7 @@ template <int E>
 __global__ void __launch_bounds__(kThreads, E <= 4 ? 2 : 1)
 k_solve(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, SolveArgs A) {
     extern __shared__ double2 tile[];   // [4][ncy][TC]
+    __shared__ double2 s_c0[TC], s_c1[TC], s_sg[2][TC];   // per-column correction coefficients
     const int ncy = d.ncy, ny = d.NYS, nkx = d.nkx, ncol = d.ncol;
     const int S = ncy * TC;
     const int col0 = blockIdx.x * TC;
@@ -193,7 +196,7 @@ k_solve(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, SolveArgs A
         const double ax = t.wavx[kx], az = t.wavz[kzi];
         const bool zero_col = kzi == d.NZS && kx == 0;
         const long long cm = (long long)col * ncy;   // column-major base
-        bool bad = false, pivot_fail = false;
+        bool pivot_fail = false;
         double2 pv[E], v0[E], v1[E], v2[E], dy[E];
 #pragma unroll
         for (int e = 0; e < E; ++e) {
@@ -281,46 +284,96 @@ k_solve(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, SolveArgs A
         }
         div0 = sum_warp(div0);
         div1 = sum_warp(div1);
-        // influence correction (src/solver/eqsolve_pv.cpp:408-411)
+        // influence and sigma coefficients (src/solver/eqsolve_pv.cpp:408-429)
         const double2 i00 = st.inf_div[col], i01 = st.inf_div[ncol + col];
         const double2 i10 = st.inf_div[2 * ncol + col], i11 = st.inf_div[3 * ncol + col];
         const double2 c0 = csub(cmul(div1, i10), cmul(div0, i11));
         const double2 c1 = csub(cmul(div0, i01), cmul(div1, i00));
-        const double2 *PI0 = st.p_inf + cm, *PI1 = st.p_inf + d.Ns + cm;
-        const double2 *VI0 = st.v_inf + cm, *VI1 = st.v_inf + 3 * d.Ns + cm;
-        // sigma correction (src/solver/eqsolve_pv.cpp:413-429)
-        const double2 ptop = cadd(elem<E>(pv, ny), cadd(cmul(c0, PI0[ny]), cmul(c1, PI1[ny])));
-        const double2 vt0 = cadd(elem<E>(v1, ny), cadd(cmul(c0, VI0[d.Ns + ny]), cmul(c1, VI1[d.Ns + ny])));
+        const long long o_n = ((long long)kzi * ncy + ny) * nkx + kx, o_n1 = o_n - nkx;
+        const double2 ptop = cadd(elem<E>(pv, ny), cadd(cmul(c0, st.p_inf[o_n]), cmul(c1, st.p_inf[d.Ns + o_n])));
+        const double2 vt0 =
+            cadd(elem<E>(v1, ny), cadd(cmul(c0, st.v_inf[d.Ns + o_n]), cmul(c1, st.v_inf[4 * d.Ns + o_n])));
         const double2 vt1 =
-            cadd(elem<E>(v1, ny - 1), cadd(cmul(c0, VI0[d.Ns + ny - 1]), cmul(c1, VI1[d.Ns + ny - 1])));
+            cadd(elem<E>(v1, ny - 1), cadd(cmul(c0, st.v_inf[d.Ns + o_n1]), cmul(c1, st.v_inf[4 * d.Ns + o_n1])));
         const double2 n0 = csub(cscale(-wv, vt0), cscale(pp.Re, tail0));
         const double2 n1 = cadd(cscale(-wv, vt1), cscale(pp.Re, csub(cscale(2.0 * ny, ptop), tail1)));
-        const double2 sg0 = cdiv(n0, st.sigma0[col]);
-        const double2 sg1 = cdiv(n1, st.sigma0[ncol + col]);
-        // odd-y coefficients take sigma_0 for p, u, w and sigma_1 for v; even-y the reverse
-        const double2 sq = p ? sg0 : sg1, sv = p ? sg1 : sg0;
+        if (L == 0) {
+            s_c0[w] = c0;
+            s_c1[w] = c1;
+            s_sg[0][w] = cdiv(n0, st.sigma0[col]);
+            s_sg[1][w] = cdiv(n1, st.sigma0[ncol + col]);
+        }
+        // uncorrected solution into the tile (each warp rewrites only its own column's slots)
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const int y = ycoef<E>(e);
             if (y > ny) continue;
-            pv[e] = cadd(pv[e], cadd(cmul(c0, PI0[y]), cmul(c1, PI1[y])));
-            pv[e] = cadd(pv[e], cmul(sq, st.p_b[cm + y]));
-            auto correct = [&](int c, double2 &vc) {
-                vc = cadd(vc, cadd(cmul(c0, VI0[c * d.Ns + y]), cmul(c1, VI1[c * d.Ns + y])));
-                vc = cadd(vc, cmul(c == 1 ? sv : sq, st.v_b[c * d.Ns + cm + y]));
-            };
-            correct(0, v0[e]);
-            correct(1, v1[e]);
-            correct(2, v2[e]);
+            const int sl = tile_slot<E>(y, w);
+            tile[sl] = pv[e];
+            tile[S + sl] = v0[e];
+            tile[2 * S + sl] = v1[e];
+            tile[3 * S + sl] = v2[e];
         }
-        if (!s.solve_only && zero_col) {
-            // correct_zero_mode (src/solver/timestepper.cpp:60-68)
-            const double2 v1w = cscale(0.5, cadd(s.bc_v[2 * ncol + col], s.bc_v[3 * ncol + col]));
+        if (__any_sync(kFull, pivot_fail) && L == 0) atomicOr(s.err, ERR_PIVOT);
+    }
+    __syncthreads();
+
+    // ---- influence and sigma corrections, coalesced over the block --------
+    // odd-y coefficients take sigma_0 for p, u, w and sigma_1 for v; even-y the reverse
+    const int zc = d.NZS * nkx;   // the (kz, kx) = (0, 0) column
+    const bool fix_zero = !s.solve_only && zc >= col0 && zc < col0 + TC;
+    bool bad = false;
+    for (int i = tid; i < S; i += kThreads) {
+        const int y = i / TC, l = i - (i / TC) * TC;
+        const int c2 = col0 + l;
+        if (c2 >= ncol) continue;
+        const int kzi = c2 / nkx, kx = c2 - (c2 / nkx) * nkx;
+        const long long off = ((long long)kzi * ncy + y) * nkx + kx;
+        const int sl = tile_slot<E>(y, l);
+        const double2 c0 = s_c0[l], c1 = s_c1[l];
+        const double2 sq = s_sg[(y + 1) & 1][l], sv = s_sg[y & 1][l];
+        double2 pr = cadd(tile[sl], cadd(cmul(c0, st.p_inf[off]), cmul(c1, st.p_inf[d.Ns + off])));
+        pr = cadd(pr, cmul(sq, st.p_b[off]));
+        double2 v[3];
 #pragma unroll
-            for (int e = 0; e < E; ++e) v1[e] = ycoef<E>(e) == 0 ? v1w : mk(0.0, 0.0);
+        for (int c = 0; c < 3; ++c) {
+            v[c] = cadd(tile[(1 + c) * S + sl],
+                        cadd(cmul(c0, st.v_inf[c * d.Ns + off]), cmul(c1, st.v_inf[(3 + c) * d.Ns + off])));
+            v[c] = cadd(v[c], cmul(c == 1 ? sv : sq, st.v_b[c * d.Ns + off]));
+        }
+        if (fix_zero && c2 == zc) {
+            tile[sl] = pr;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) tile[(1 + c) * S + sl] = v[c];
+            continue;
+        }
+        bad |= !(isfinite(pr.x) && isfinite(pr.y) && isfinite(v[0].x) && isfinite(v[0].y) && isfinite(v[1].x) &&
+                 isfinite(v[1].y) && isfinite(v[2].x) && isfinite(v[2].y));
+        A.p_out[off] = pr;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) A.v_out[c * d.Ns + off] = v[c];
+    }
+    if (fix_zero) {
+        __syncthreads();
+        if (w == zc - col0) {
+            const int kzi = d.NZS;
+            double2 pz[E], u0[E], u1[E], u2[E];
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const int y = ycoef<E>(e);
+                const int sl = tile_slot<E>(y <= ny ? y : 0, w);
+                pz[e] = tile[sl];
+                u0[e] = tile[S + sl];
+                u2[e] = tile[3 * S + sl];
+            }
+            // correct_zero_mode (src/solver/timestepper.cpp:60-68)
+            const double2 v1w = cscale(0.5, cadd(s.bc_v[2 * ncol + zc], s.bc_v[3 * ncol + zc]));
+#pragma unroll
+            for (int e = 0; e < E; ++e) u1[e] = ycoef<E>(e) == 0 ? v1w : mk(0.0, 0.0);
             // correct_flow (src/sim/simulation.cpp:111-140), single-rank branch
             const double *uu = st.unit;
             double dpdx, dpdz;
+            bool pfail = false;
             if (pp.grad_pre == 1) {
                 dpdx = pp.gx;
                 dpdz = pp.gz;
@@ -330,60 +383,39 @@ k_solve(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, SolveArgs A
                 for (int e = 0; e < E; ++e) {
                     const int y = ycoef<E>(e);
                     if (p == 0 && y <= ny) {
-                        qx += v0[e].x / (double)(y * y - 1);
-                        qz += v2[e].x / (double)(y * y - 1);
+                        qx += u0[e].x / (double)(y * y - 1);
+                        qz += u2[e].x / (double)(y * y - 1);
                     }
                 }
                 qx = -sum_warp(qx);
                 qz = -sum_warp(qz);
                 const double qxu = uu[2 * ncy], qzu = uu[2 * ncy + 1];
-                if (!isfinite(qxu) || qxu == 0.0 || !isfinite(qzu) || qzu == 0.0) pivot_fail = true;
+                pfail = !isfinite(qxu) || qxu == 0.0 || !isfinite(qzu) || qzu == 0.0;
                 dpdx = (pp.qxm - qx) / qxu;
                 dpdz = (pp.qzm - qz) / qzu;
             }
             if (L == 0) {
                 s.dpdx[0] = dpdx;
                 s.dpdx[1] = dpdz;
+                if (pfail) atomicOr(s.err, ERR_PIVOT);
             }
 #pragma unroll
             for (int e = 0; e < E; ++e) {
                 const int y = ycoef<E>(e);
-                if (y <= ny) {
-                    v0[e].x += dpdx * uu[y];
-                    v2[e].x += dpdz * uu[ncy + y];
-                }
+                if (y > ny) continue;
+                u0[e].x += dpdx * uu[y];
+                u2[e].x += dpdz * uu[ncy + y];
+                bad |= !(isfinite(pz[e].x) && isfinite(pz[e].y) && isfinite(u0[e].x) && isfinite(u0[e].y) &&
+                         isfinite(u1[e].x) && isfinite(u1[e].y) && isfinite(u2[e].x) && isfinite(u2[e].y));
+                const long long off = ((long long)kzi * ncy + y) * nkx;
+                A.p_out[off] = pz[e];
+                A.v_out[off] = u0[e];
+                A.v_out[d.Ns + off] = u1[e];
+                A.v_out[2 * d.Ns + off] = u2[e];
             }
         }
-        // results into the tile (each warp rewrites only its own column's slots)
-#pragma unroll
-        for (int e = 0; e < E; ++e) {
-            const int y = ycoef<E>(e);
-            if (y > ny) continue;
-            bad |= !(isfinite(pv[e].x) && isfinite(pv[e].y) && isfinite(v0[e].x) && isfinite(v0[e].y) &&
-                     isfinite(v1[e].x) && isfinite(v1[e].y) && isfinite(v2[e].x) && isfinite(v2[e].y));
-            const int sl = tile_slot<E>(y, w);
-            tile[sl] = pv[e];
-            tile[S + sl] = v0[e];
-            tile[2 * S + sl] = v1[e];
-            tile[3 * S + sl] = v2[e];
-        }
-        const unsigned flags = (__any_sync(kFull, bad) ? ERR_NONFINITE : 0u) |
-                               (__any_sync(kFull, pivot_fail) ? ERR_PIVOT : 0u);
-        if (flags && L == 0) atomicOr(s.err, flags);
     }
-    __syncthreads();
-    for (int i = tid; i < S; i += kThreads) {
-        const int y = i / TC, l = i - (i / TC) * TC;
-        const int c2 = col0 + l;
-        if (c2 >= ncol) continue;
-        const int kzi = c2 / nkx, kx = c2 - (c2 / nkx) * nkx;
-        const long long off = ((long long)kzi * ncy + y) * nkx + kx;
-        const int sl = tile_slot<E>(y, l);
-        A.p_out[off] = tile[sl];
-        A.v_out[off] = tile[S + sl];
-        A.v_out[d.Ns + off] = tile[2 * S + sl];
-        A.v_out[2 * d.Ns + off] = tile[3 * S + sl];
-    }
+    if (__any_sync(kFull, bad) && L == 0) atomicOr(s.err, ERR_NONFINITE);
 }
 
 size_t solve_smem(const Dims &d) { return sizeof(double2) * 4 * (size_t)d.ncy * TC; }

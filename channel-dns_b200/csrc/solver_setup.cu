@@ -9,8 +9,9 @@
 // reference's by 1e-9 relative after that cancellation unless the B-problem is
 // computed in the same order.  Setup runs at steps 1 and 2 only.
 //
-// Outputs: pivots ad_p, ad_v and the influence / B-problem fields are stored
-// column-major ([col][y]), the layout the step solve reads.
+// Outputs: the pivots ad_p, ad_v are stored column-major ([col][y]), read by
+// the step solve's column warps; the influence / B-problem fields are planar
+// ([kz][y][kx]), read by its coalesced correction pass.
 #include "cdns_kernels.cuh"
 
 namespace cdns {
@@ -23,8 +24,8 @@ enum SetupMode { MODE_BASE = 1, MODE_COUPLED = 2 };
 
 struct SetupArgs {
     double2 bcp_top, bcp_bot;  // constant pressure wall data
-    double2 *p_out;            // [Ns] column-major
-    double2 *v_out;            // [3][Ns] column-major
+    double2 *p_out;            // [Ns] planar
+    double2 *v_out;            // [3][Ns] planar
     double2 *divb_out;         // [2][ncol] raw wall divergence (MODE_BASE)
 };
 
@@ -207,7 +208,8 @@ k_setup_solve(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, Setup
         const int y = i / TC, l = i - (i / TC) * TC;
         const int col = col0 + l;
         if (col >= d.ncol) continue;
-        const long long cm = (long long)col * ncy + y;
+        const int kzi = col / nkx, kx = col - (col / nkx) * nkx;
+        const long long cm = ((long long)kzi * ncy + y) * nkx + kx;   // planar
         double2 p = pc[i];
         double2 v[3] = {rv[i], rv[S + i], rv[2 * S + i]};
         if (MODE == MODE_COUPLED) {
@@ -275,12 +277,13 @@ __global__ void k_sigma0(Dims d, double re, const double *wn_v, const double2 *p
                          const double2 *v_b, double2 *sigma0) {
     const int col = blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= d.ncol) return;
-    const long long base = (long long)col * d.ncy;
+    const int kzi = col / d.nkx, kx = col - (col / d.nkx) * d.nkx;
     const int n = d.NYS;
+    const long long on = ((long long)kzi * d.ncy + n) * d.nkx + kx;   // planar (kz, n, kx)
     const double w = wn_v[col];
-    const double2 vbn = v_b[d.Ns + base + n];
-    const double2 vbn1 = v_b[d.Ns + base + n - 1];
-    const double2 pbn = p_b[base + n];
+    const double2 vbn = v_b[d.Ns + on];
+    const double2 vbn1 = v_b[d.Ns + on - d.nkx];
+    const double2 pbn = p_b[on];
     sigma0[col] = mk(re + w * vbn.x, w * vbn.y);
     double2 s1 = csub(mk(re + w * vbn1.x, w * vbn1.y), cscale(re * (2.0 * n), pbn));
     if (col == d.NZS * d.nkx) s1 = mk(1.0, 0.0);

@@ -10,8 +10,11 @@
 // The Chebyshev (y) synthesis and analysis live in chebyshev.cu; this file
 // holds the Fourier directions (src/fft/transforms.cpp:615-741): the analysis
 // keeps x1/NX2 before the z FFT and x1/NZ2 after it.
+#include <type_traits>
+
 #include "cdns_kernels.cuh"
 #include "fft_lines.cuh"
+#include "reg_fft.cuh"
 
 namespace cdns {
 
@@ -193,6 +196,171 @@ k_x_cross(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 *_
 }
 
 // ---------------------------------------------------------------------------
+// K3, register form for NX2 = N1 x N2 (N1, N2 <= 16): the same transform with
+// every length-NX2 FFT done as two in-register DFT steps and one shared-memory
+// exchange.  16 lanes per line (a half-warp), RW rows per block, RW even.
+//   phase 1  lanes (line, n2): gather the Hermitian spectrum slots
+//            m = n2 + N2 n1 from HBM, N1-point DFT, twiddle -> S
+//   phase 2  lanes (line, k1): N2-point DFT -> physical rows P[line][x]
+//   phase 3  lanes (out line, n2): products at x = n2 + N2 n1 from P,
+//            N1-point DFT, twiddle -> S
+//   phase 4  lanes (out line, k1): N2-point DFT, Hermitian unpack with the
+//            partner lane (k1' = N1 - k1) by shuffle, modes k <= NXS -> HBM
+// S and P share one buffer; every phase reads into registers before a
+// barrier and writes after it.
+// ---------------------------------------------------------------------------
+template <int N1, int N2>
+__global__ void __launch_bounds__(16 * 3 * 4)
+k_x_cross_r(Dims d, const double2 *__restrict__ roots, const double2 *__restrict__ G,
+            double2 *__restrict__ H, int RW) {
+    constexpr int n = N1 * N2;
+    constexpr int SP = N2 + 1;   // padded row of the step-1 output
+    extern __shared__ double2 sm[];
+    double2 *s_root = sm;
+    double2 *buf = sm + n;
+    const int L = 3 * RW, L2 = 3 * (RW / 2);
+    const int slot = threadIdx.x >> 4, sub = threadIdx.x & 15;
+    const int j = blockIdx.y, z0 = blockIdx.x * RW;
+    const int nkx = d.nkx, nxs = d.NXS;
+    const long long fstride = (long long)d.ny2 * d.NZ2 * nkx;
+    const double2 *Gj = G + (long long)j * d.NZ2 * nkx;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s_root[i] = roots[i];
+    const int nyq = (n % 2 == 0) ? n / 2 : -1;
+    double2 v[N1 > N2 ? N1 : N2];
+
+    // ---- phase 1: spectrum gather, N1-point DFTs over n1 (backward) --------
+    const bool act1 = slot < L && sub < N2;
+    if (act1) {
+        const int r = slot / 3, pl = slot - (slot / 3) * 3;
+        const int z = z0 + r;
+        const double2 *rowA = Gj + (long long)z * nkx + (2 * pl) * fstride;
+        const double2 *rowB = rowA + fstride;
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) {
+            const int m = sub + N2 * n1;
+            double2 x = mk(0.0, 0.0);
+            if (z < d.NZ2) {
+                if (m <= nxs) {
+                    double2 A = rowA[m], B = rowB[m];
+                    if (m == 0 || m == nyq) {
+                        A.y = 0.0;
+                        B.y = 0.0;
+                    }
+                    x = mk(A.x - B.y, A.y + B.x);
+                } else if (m >= n - nxs && m != nyq) {
+                    const double2 A = rowA[n - m], B = rowB[n - m];
+                    x = mk(A.x + B.y, B.x - A.y);
+                }
+            }
+            v[n1] = x;
+        }
+    }
+    __syncthreads();   // s_root complete
+    if (act1) {
+        double2(&w)[N1] = reinterpret_cast<double2(&)[N1]>(v);
+        dft_reg<N1, +1>(w, s_root, N2);
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) {
+            const double2 t = (k1 == 0 || sub == 0) ? w[k1] : cmul(w[k1], root_of<+1>(s_root, sub * k1));
+            buf[(slot * N1 + k1) * SP + sub] = t;
+        }
+    }
+    __syncthreads();
+    // ---- phase 2: N2-point DFTs over n2 -> physical rows ------------------
+    const bool act2 = slot < L && sub < N1;
+    if (act2) {
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) v[n2] = buf[(slot * N1 + sub) * SP + n2];
+    }
+    __syncthreads();
+    if (act2) {
+        double2(&w)[N2] = reinterpret_cast<double2(&)[N2]>(v);
+        dft_reg<N2, +1>(w, s_root, N1);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) buf[slot * n + sub + N1 * k2] = w[k2];
+    }
+    __syncthreads();
+    // ---- phase 3: products u x omega, N1-point DFTs (forward) -------------
+    // out lines per row pair (r, r+1): (N0 + i N1)(r), (N0 + i N1)(r+1), N2(r) + i N2(r+1)
+    const bool act3 = slot < L2 && sub < N2;
+    if (act3) {
+        const int pr = slot / 3, kind = slot - (slot / 3) * 3;
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) {
+            const int x = sub + N2 * n1;
+            auto prod = [&](int r, double &n0, double &n1v, double &n2v) {
+                const double2 p0 = buf[(3 * r) * n + x];
+                const double2 p1 = buf[(3 * r + 1) * n + x];
+                const double2 p2 = buf[(3 * r + 2) * n + x];
+                const double uu = p0.x, vv = p0.y, ww = p1.x, ox = p1.y, oy = p2.x, oz = p2.y;
+                n0 = vv * oz - ww * oy;
+                n1v = ww * ox - uu * oz;
+                n2v = uu * oy - vv * ox;
+            };
+            double a0, a1, a2, b0, b1, b2;
+            if (kind < 2) {
+                prod(2 * pr + kind, a0, a1, a2);
+                v[n1] = mk(a0, a1);
+            } else {
+                prod(2 * pr, a0, a1, a2);
+                prod(2 * pr + 1, b0, b1, b2);
+                v[n1] = mk(a2, b2);
+            }
+        }
+    }
+    __syncthreads();
+    if (act3) {
+        double2(&w)[N1] = reinterpret_cast<double2(&)[N1]>(v);
+        dft_reg<N1, -1>(w, s_root, N2);
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) {
+            const double2 t = (k1 == 0 || sub == 0) ? w[k1] : cmul(w[k1], root_of<-1>(s_root, sub * k1));
+            buf[(slot * N1 + k1) * SP + sub] = t;
+        }
+    }
+    __syncthreads();
+    // ---- phase 4: N2-point DFTs, unpack, modes k <= NXS -------------------
+    const bool act4 = slot < L2 && sub < N1;
+    if (act4) {
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) v[n2] = buf[(slot * N1 + sub) * SP + n2];
+        double2(&w)[N2] = reinterpret_cast<double2(&)[N2]>(v);
+        dft_reg<N2, -1>(w, s_root, N1);
+    }
+    // partner of frequency k1 + N1 k2 is n - k = k1' + N1 k2' with
+    // k1' = (N1 - k1) mod N1, k2' = N2 - 1 - k2 (k1 > 0) or (N2 - k2) mod N2 (k1 = 0)
+    const int lane = threadIdx.x & 31;
+    const int partner = (lane & 16) + (sub < N1 ? (N1 - sub) % N1 : sub);
+    const int pr = slot / 3, kind = slot - (slot / 3) * 3;
+    const double invn = 1.0 / (double)n;
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) {
+        double2 pm;
+        pm.x = __shfl_sync(0xffffffffu, v[N2 - 1 - k2].x, partner);
+        pm.y = __shfl_sync(0xffffffffu, v[N2 - 1 - k2].y, partner);
+        const int k = sub + N1 * k2;
+        if (!act4 || k > nxs) continue;
+        if (sub == 0) pm = v[(N2 - k2) % N2];
+        const double2 p0 = v[k2];
+        const double2 outA = cscale(invn, mk(0.5 * (p0.x + pm.x), 0.5 * (p0.y - pm.y)));
+        const double2 outB = cscale(invn, mk(0.5 * (p0.y + pm.y), -0.5 * (p0.x - pm.x)));
+        if (kind < 2) {
+            const int z = z0 + 2 * pr + kind;
+            if (z < d.NZ2) {
+                double2 *h = H + ((long long)j * d.NZ2 + z) * nkx + k;
+                h[0] = outA;            // N0
+                h[fstride] = outB;      // N1
+            }
+        } else {
+            const int z = z0 + 2 * pr;
+            double2 *h = H + 2 * fstride + ((long long)j * d.NZ2 + z) * nkx + k;
+            if (z < d.NZ2) h[0] = outA;                 // N2 of row r
+            if (z + 1 < d.NZ2) h[nkx] = outB;           // N2 of row r+1
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Single-field x transforms for the standalone fine transform (tests and
 // to-physical output): c2r / r2c of one real field [z][j][x].
 // ---------------------------------------------------------------------------
@@ -295,8 +463,32 @@ size_t smem_xsingle(const Dims &d) {
     return sizeof(double2) * (size_t)d.NX2 * (1 + 2 * ((kRWs + 1) / 2));
 }
 
+// NX2 = N1 x N2 pairs with a register-form x kernel; others use the Stockham form.
+template <typename Fn> bool with_xsplit(int nx2, Fn &&fn) {
+    switch (nx2) {
+    case 48: fn(std::integral_constant<int, 6>{}, std::integral_constant<int, 8>{}); return true;
+    case 96: fn(std::integral_constant<int, 8>{}, std::integral_constant<int, 12>{}); return true;
+    case 144: fn(std::integral_constant<int, 12>{}, std::integral_constant<int, 12>{}); return true;
+    case 192: fn(std::integral_constant<int, 12>{}, std::integral_constant<int, 16>{}); return true;
+    case 196: fn(std::integral_constant<int, 14>{}, std::integral_constant<int, 14>{}); return true;
+    default: return false;
+    }
+}
+constexpr int kRWr = 4;
+size_t smem_xcross_r(int n1, int n2) {
+    const size_t L = 3 * kRWr;
+    const size_t s1 = L * n1 * (n2 + 1), s2 = L * n1 * n2;
+    return sizeof(double2) * ((size_t)n1 * n2 + (s1 > s2 ? s1 : s2));
+}
+
 cudaError_t configure_transform_kernels(const Dims &d) {
-    cudaError_t e;
+    cudaError_t e = cudaSuccess;
+    with_xsplit(d.NX2, [&](auto a, auto b) {
+        constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
+        e = cudaFuncSetAttribute(k_x_cross_r<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem_xcross_r(N1, N2));
+    });
+    if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_z_backward, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem_zfft(d));
     if (e != cudaSuccess) return e;
@@ -323,6 +515,12 @@ void launch_z_backward(const Dims &d, const FftPlan &P, const double2 *roots, co
 
 void launch_x_cross(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G,
                     double2 *H, cudaStream_t s) {
+    const bool done = with_xsplit(d.NX2, [&](auto a, auto b) {
+        constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
+        dim3 grid((d.NZ2 + kRWr - 1) / kRWr, d.ny2);
+        k_x_cross_r<N1, N2><<<grid, 16 * 3 * kRWr, smem_xcross_r(N1, N2), s>>>(d, roots, G, H, kRWr);
+    });
+    if (done) return;
     dim3 grid((d.NZ2 + kRW - 1) / kRW, d.ny2);
     k_x_cross<<<grid, 256, smem_xcross(d), s>>>(d, P, roots, G, H, kRW);
 }
