@@ -100,6 +100,72 @@ k_z_forward(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 
     fft_run<-1>(a, b, TL, P, s_root, src, dst);
 }
 
+// Register form of the z transforms for NZ2 = N1 x N2: threads t = n2 TL + l
+// (step 1) and t = k1 TL + l (step 2) over TL kx lines, one shared-memory
+// exchange S[k1][n2][l]; loads and stores run along kx.
+template <int N1, int N2, int SIGN, class Src, class Dst>
+__device__ __forceinline__ void fft2_lines(int TL, const double2 *s_root, double2 *S, const Src &src,
+                                           const Dst &dst) {
+    constexpr int NM = N1 > N2 ? N1 : N2;
+    const int t = threadIdx.x;
+    double2 v[NM];
+    const bool a1 = t < N2 * TL;
+    const int n2 = t / TL, l1 = t - (t / TL) * TL;
+    if (a1) {
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) v[n1] = src(n2 + N2 * n1, l1);
+    }
+    __syncthreads();   // s_root complete
+    if (a1) {
+        double2(&w)[N1] = reinterpret_cast<double2(&)[N1]>(v);
+        dft_reg<N1, SIGN>(w, s_root, N2);
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1)
+            S[(k1 * N2 + n2) * TL + l1] =
+                (k1 == 0 || n2 == 0) ? w[k1] : cmul(w[k1], root_of<SIGN>(s_root, n2 * k1));
+    }
+    __syncthreads();
+    if (t < N1 * TL) {
+        const int k1 = t / TL, l = t - (t / TL) * TL;
+#pragma unroll
+        for (int m = 0; m < N2; ++m) v[m] = S[(k1 * N2 + m) * TL + l];
+        double2(&w)[N2] = reinterpret_cast<double2(&)[N2]>(v);
+        dft_reg<N2, SIGN>(w, s_root, N1);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) dst(k1 + N1 * k2, l, w[k2]);
+    }
+}
+
+template <int N1, int N2>
+__global__ void __launch_bounds__(16 * 17)
+k_z_backward_r(Dims d, const double2 *__restrict__ roots, const double2 *__restrict__ F,
+               double2 *__restrict__ G, int TL) {
+    extern __shared__ double2 sm[];
+    constexpr int n = N1 * N2;
+    double2 *s_root = sm;
+    double2 *S = sm + n;
+    const int f = blockIdx.z, j = blockIdx.y, kx0 = blockIdx.x * TL;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s_root[i] = roots[i];
+    const ZExpandSrc src{F + ((long long)f * d.ny2 + j) * d.ncol, d.nkx, kx0, d.NZS, n};
+    const RowDst dst{G + ((long long)f * d.ny2 + j) * (long long)n * d.nkx, d.nkx, kx0};
+    fft2_lines<N1, N2, +1>(TL, s_root, S, src, dst);
+}
+
+template <int N1, int N2>
+__global__ void __launch_bounds__(16 * 17)
+k_z_forward_r(Dims d, const double2 *__restrict__ roots, const double2 *__restrict__ H,
+              double2 *__restrict__ F, int TL) {
+    extern __shared__ double2 sm[];
+    constexpr int n = N1 * N2;
+    double2 *s_root = sm;
+    double2 *S = sm + n;
+    const int f = blockIdx.z, j = blockIdx.y, kx0 = blockIdx.x * TL;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s_root[i] = roots[i];
+    const RowSrc src{H + ((long long)f * d.ny2 + j) * (long long)n * d.nkx, d.nkx, kx0};
+    const ZTruncDst dst{F + ((long long)f * d.ny2 + j) * d.ncol, d.nkx, kx0, d.NZS, n, 1.0 / (double)n};
+    fft2_lines<N1, N2, -1>(TL, s_root, S, src, dst);
+}
+
 // ---------------------------------------------------------------------------
 // K3: inverse x FFT of the six fields, u x omega, forward x FFT of the three
 // products.  Block = RW rows (z, j); real rows are packed in pairs into one
@@ -475,6 +541,9 @@ template <typename Fn> bool with_xsplit(int nx2, Fn &&fn) {
     }
 }
 constexpr int kRWr = 4;
+size_t smem_zfft_r(const Dims &d, int n1, int n2) {
+    return sizeof(double2) * ((size_t)n1 * n2 + (size_t)n1 * n2 * z_lines(d));
+}
 size_t smem_xcross_r(int n1, int n2) {
     const size_t L = 3 * kRWr;
     const size_t s1 = L * n1 * (n2 + 1), s2 = L * n1 * n2;
@@ -487,6 +556,14 @@ cudaError_t configure_transform_kernels(const Dims &d) {
         constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
         e = cudaFuncSetAttribute(k_x_cross_r<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem_xcross_r(N1, N2));
+    });
+    if (e != cudaSuccess) return e;
+    with_xsplit(d.NZ2, [&](auto a, auto b) {
+        constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
+        const int sm = (int)smem_zfft_r(d, N1, N2);
+        e = cudaFuncSetAttribute(k_z_backward_r<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_z_forward_r<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     });
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_z_backward, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -510,7 +587,11 @@ void launch_z_backward(const Dims &d, const FftPlan &P, const double2 *roots, co
                        double2 *G, int nf, cudaStream_t s) {
     const int tl = z_lines(d);
     dim3 grid((d.nkx + tl - 1) / tl, d.ny2, nf);
-    k_z_backward<<<grid, 256, smem_zfft(d), s>>>(d, P, roots, F, G, tl);
+    const bool done = with_xsplit(d.NZ2, [&](auto a, auto b) {
+        constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
+        k_z_backward_r<N1, N2><<<grid, (N1 > N2 ? N1 : N2) * tl, smem_zfft_r(d, N1, N2), s>>>(d, roots, F, G, tl);
+    });
+    if (!done) k_z_backward<<<grid, 256, smem_zfft(d), s>>>(d, P, roots, F, G, tl);
 }
 
 void launch_x_cross(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G,
@@ -529,7 +610,11 @@ void launch_z_forward(const Dims &d, const FftPlan &P, const double2 *roots, con
                       double2 *F, int nf, cudaStream_t s) {
     const int tl = z_lines(d);
     dim3 grid((d.nkx + tl - 1) / tl, d.ny2, nf);
-    k_z_forward<<<grid, 256, smem_zfft(d), s>>>(d, P, roots, H, F, tl);
+    const bool done = with_xsplit(d.NZ2, [&](auto a, auto b) {
+        constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
+        k_z_forward_r<N1, N2><<<grid, (N1 > N2 ? N1 : N2) * tl, smem_zfft_r(d, N1, N2), s>>>(d, roots, H, F, tl);
+    });
+    if (!done) k_z_forward<<<grid, 256, smem_zfft(d), s>>>(d, P, roots, H, F, tl);
 }
 
 void launch_x_c2r(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G,
