@@ -13,10 +13,9 @@
 //   analysis   S_k = s_k sum_{j <= N/2} A_jk (k even ? X_j + X_{N-j} : X_j - X_{N-j}),
 //              A_jk = v_j cos(pi j k / N), v_0 = 1, else 2 (the middle point
 //              j = N/2 enters once), s_0 = 1/(2N), s_k = 1/N.
-// One thread owns one spectral column and MR output rows of one field; the 32
-// lanes of a warp own 32 consecutive columns and read the same matrix entries
-// (one broadcast load per pair of rows), so the kernels run at the FP64 FMA
-// rate with coalesced column loads and stores.
+// A block owns 32 consecutive spectral columns of one field; its warps run
+// 8x8x4 FP64 MMA tiles (rows x real columns) of one parity each, with the
+// column data and cosine rows streamed through shared memory by cp.async.
 #include <algorithm>
 
 #include "cdns_kernels.cuh"
@@ -25,9 +24,9 @@
 namespace cdns {
 
 namespace {
-constexpr int kSynRows = 14;   // synthesis rows (j) per thread
-constexpr int kAnaRows = 16;   // analysis rows (k of one parity) per thread
-constexpr int kMaxGroups = 8;  // row groups per block (two warps each)
+constexpr int kSynRows = 16;   // synthesis rows (j) per warp
+constexpr int kAnaRows = 16;   // analysis rows (k of one parity) per warp
+constexpr int kMaxGroups = 8;  // row groups per block (two warps each); more go to grid.z
 
 // 16-byte asynchronous global -> shared copy; src_bytes = 0 writes zeros.
 __device__ __forceinline__ void cp_async16(void *dst, const void *src, int src_bytes) {
@@ -152,34 +151,54 @@ k_curl(Dims d, Tables t, const double2 *__restrict__ u, double2 *__restrict__ om
     }
 }
 
+// D (8x8) += A (8x4) B (4x8) on the FP64 tensor pipe.  Lane l = 4 g + t holds
+// A[g][t], B[t][g] and D[g][2t], D[g][2t+1].
+__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// Staged rows are padded so that the four k (or j) rows of one fragment load
+// fall on distinct bank quarters: complex rows of 32 columns take kXS = 34
+// slots; double rows are padded to a stride = 4 (mod 16) / 2 (mod 8).
+constexpr int kXS = 34;
+__host__ __device__ inline int syn_cs(int jp) { return jp + ((4 - jp % 16) + 16) % 16; }
+__host__ __device__ inline int ana_as(int kh) { return kh + ((2 - kh % 8) + 8) % 8; }
+
 // ---------------------------------------------------------------------------
 // Synthesis: F[f][j][col] for j = 0..NY2 from spectral fields
 // (fields f < nsplit from src0, the rest from src1).  Grid (column tiles of
-// 32, fields); block (32, 2 G): warp (g, p) accumulates the parity-p sum of
-// rows j = g MR .. g MR + MR - 1 for the 32 columns.  The coefficients flow
-// through shared memory in chunks of KC rows of k (descending, as the
-// reference's recurrences), the next chunk prefetched into registers while
-// the current one is multiplied; the cosine rows of the chunk ride along.
+// 32, fields); block (32, 2 G): warp (g, p) accumulates, with 8x8x4 FP64 MMA,
+// the parity-p sum of rows j = 16 g .. 16 g + 15 for the 32 columns (a 16 x 64
+// real tile).  Coefficients and cosine rows stream through shared memory in
+// chunks of KC rows of k (descending), split by parity, double-buffered with
+// cp.async; odd-parity warps hand their sums to the even ones at the end.
 // ---------------------------------------------------------------------------
 constexpr int kSynKC = 16;
+constexpr int kSynStages = 4;
+constexpr int kSynTiles = 4;   // 16-row tiles per block (two warps each); more go to grid.z
 
-template <int MR>
-__global__ void __launch_bounds__(32 * 2 * kMaxGroups)
+__global__ void __launch_bounds__(32 * 2 * kSynTiles, 2)
 k_ysynth(Dims d, const double *__restrict__ csyn, int jp, const double2 *__restrict__ src0,
          const double2 *__restrict__ src1, int nsplit, double2 *__restrict__ F) {
     extern __shared__ double2 sm[];
-    constexpr int KC = kSynKC;
-    double2 *xs = sm;                                            // [2][KC][32]
-    double *cs = reinterpret_cast<double *>(sm + 2 * KC * 32);   // [2][KC][jp]
+    constexpr int KC = kSynKC, KH = KC / 2;
+    constexpr int jw = kSynTiles * 16;   // cosine columns staged per block
+    const int CS = syn_cs(jw);
+    constexpr int NS = kSynStages;
+    double2 *xs = sm;                                                // [NS][2 par][KH][kXS]
+    double *cs = reinterpret_cast<double *>(sm + NS * 2 * KH * kXS); // [NS][2 par][KH][CS]
     const int lane = threadIdx.x, wy = threadIdx.y;
     const int tid = wy * 32 + lane, nthr = 32 * blockDim.y;
-    const int g = wy >> 1, par = wy & 1;
+    const int jt = blockIdx.z * kSynTiles + (wy >> 1), par = wy & 1;
+    const int jb = blockIdx.z * kSynTiles * 16;   // first row of this block
+    const int g = lane >> 2, t = lane & 3;
     const int f = blockIdx.y, col0 = blockIdx.x * 32;
     const int ncol = d.ncol, ny = d.NYS, N = d.NY2;
     const double2 *X = f < nsplit ? src0 + (long long)f * d.Ns : src1 + (long long)(f - nsplit) * d.Ns;
     const int nchunk = (d.ncy + KC - 1) / KC;
-    // staging of one chunk: X units (row r, lane l) and cosine double2 units
-    const int nxu = KC * 32, ncu = KC * jp / 2;
+    const int nxu = KC * 32, ncu = KC * (jw / 2);
     auto fetch = [&](int chunk, int buf) {
         const int khi = ny - chunk * KC;
         for (int u = tid; u < nxu + ncu; u += nthr) {
@@ -188,172 +207,194 @@ k_ysynth(Dims d, const double *__restrict__ csyn, int jp, const double2 *__restr
                 const int k = khi - r, col = col0 + l;
                 const bool ok = k >= 0 && col < ncol;
                 const int kzi = ok ? col / d.nkx : 0, kx = ok ? col - kzi * d.nkx : 0;
-                cp_async16(xs + buf * KC * 32 + u, X + ((long long)kzi * d.ncy + (ok ? k : 0)) * d.nkx + kx,
-                           ok ? 16 : 0);
+                cp_async16(xs + ((buf * 2 + (k & 1)) * KH + (r >> 1)) * kXS + l,
+                           X + ((long long)kzi * d.ncy + (ok ? k : 0)) * d.nkx + kx, ok ? 16 : 0);
             } else {
                 const int c = u - nxu;
-                const int r = c / (jp / 2), h = c - r * (jp / 2);
+                const int r = c / (jw / 2), h = c - r * (jw / 2);
                 const int k = khi - r;
-                cp_async16(reinterpret_cast<double2 *>(cs + buf * KC * jp) + c,
-                           reinterpret_cast<const double2 *>(csyn + (long long)(k >= 0 ? k : 0) * jp) + h,
-                           k >= 0 ? 16 : 0);
+                const bool ok = k >= 0 && jb + 2 * h < jp;
+                cp_async16(cs + ((buf * 2 + (k & 1)) * KH + (r >> 1)) * CS + 2 * h,
+                           csyn + (long long)(ok ? k : 0) * jp + (ok ? jb + 2 * h : 0), ok ? 16 : 0);
             }
         }
         cp_async_commit();
     };
-    double2 acc[MR];
+    double acc[2][8][2];
 #pragma unroll
-    for (int i = 0; i < MR; ++i) acc[i] = mk(0.0, 0.0);
-    const int j0 = g * MR;
-    fetch(0, 0);
+    for (int mr = 0; mr < 2; ++mr)
+#pragma unroll
+        for (int q = 0; q < 8; ++q) acc[mr][q][0] = acc[mr][q][1] = 0.0;
+    const int j0 = jt * 16;
+    const bool jok = j0 < jp;   // warps past the last row tile only stage data
+#pragma unroll
+    for (int c = 0; c < NS - 1; ++c) {
+        if (c < nchunk) fetch(c, c);
+        else cp_async_commit();
+    }
     for (int chunk = 0; chunk < nchunk; ++chunk) {
-        const int buf = chunk & 1;
-        if (chunk + 1 < nchunk) {
-            fetch(chunk + 1, buf ^ 1);
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
-        }
-        __syncthreads();
-        const int khi = ny - chunk * KC;
-        // rows r of this chunk whose k = khi - r has parity par
-        const int r0 = ((khi - par) & 1);
-        for (int r = r0; r < KC; r += 2) {
-            const double2 x = xs[(buf * KC + r) * 32 + lane];
-            const double2 *c2 = reinterpret_cast<const double2 *>(cs + (buf * KC + r) * jp + j0);
+        const int buf = chunk % NS;
+        cp_async_wait<NS - 2>();   // this chunk has landed
+        __syncthreads();           // ... for every thread; the buffer refilled next was consumed last iteration
+        if (chunk + NS - 1 < nchunk) fetch(chunk + NS - 1, (chunk + NS - 1) % NS);
+        else cp_async_commit();
+        const double *cb = cs + (buf * 2 + par) * KH * CS;
+        const double2 *xb = xs + (buf * 2 + par) * KH * kXS;
 #pragma unroll
-            for (int i = 0; i < MR / 2; ++i) {
-                const double2 c = c2[i];
-                acc[2 * i].x += c.x * x.x;
-                acc[2 * i].y += c.x * x.y;
-                acc[2 * i + 1].x += c.y * x.x;
-                acc[2 * i + 1].y += c.y * x.y;
+        for (int st = 0; st < (jok ? KH / 4 : 0); ++st) {
+            const int r = 4 * st + t;
+            const double a0 = cb[r * CS + j0 - jb + g], a1 = cb[r * CS + j0 - jb + 8 + g];
+            const double *xr = reinterpret_cast<const double *>(xb + r * kXS) + (g & 1);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const double bq = xr[2 * (4 * q + (g >> 1))];
+                dmma(acc[0][q][0], acc[0][q][1], a0, bq);
+                dmma(acc[1][q][0], acc[1][q][1], a1, bq);
             }
         }
-        __syncthreads();
     }
+    cp_async_wait<0>();
+    __syncthreads();
     // combine: odd-parity warps hand their sums to the even-parity warps
-    double2 *ex = sm;   // [G][MR][32]
-    if (par == 1) {
+    constexpr int kEXS = 36;
+    double2 *ex = sm;   // [16 * kSynTiles][kEXS], rows relative to this block's first tile
+    if (jok && par == 1) {
 #pragma unroll
-        for (int i = 0; i < MR; ++i) ex[(g * MR + i) * 32 + lane] = acc[i];
+        for (int mr = 0; mr < 2; ++mr)
+#pragma unroll
+            for (int q = 0; q < 8; ++q) ex[(j0 - jb + 8 * mr + g) * kEXS + 4 * q + t] = mk(acc[mr][q][0], acc[mr][q][1]);
     }
     __syncthreads();
-    const int col = col0 + lane;
-    if (par == 0 && col < ncol) {
-        double2 *Ff = F + (long long)f * d.ny2 * ncol + col;
+    if (jok && par == 0) {
+        double2 *Ff = F + (long long)f * d.ny2 * ncol + col0;
 #pragma unroll
-        for (int i = 0; i < MR; ++i) {
-            const int j = j0 + i;
-            if (j >= d.nyh) break;
-            const double2 o = ex[(g * MR + i) * 32 + lane];
-            Ff[(long long)j * ncol] = cadd(acc[i], o);
-            if (N - j != j) Ff[(long long)(N - j) * ncol] = csub(acc[i], o);
+        for (int mr = 0; mr < 2; ++mr) {
+            const int j = j0 + 8 * mr + g;
+            if (j >= d.nyh) continue;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int c = 4 * q + t;
+                if (col0 + c >= ncol) continue;
+                const double2 o = ex[(j0 - jb + 8 * mr + g) * kEXS + c];
+                const double2 e = mk(acc[mr][q][0], acc[mr][q][1]);
+                Ff[(long long)j * ncol + c] = cadd(e, o);
+                if (N - j != j) Ff[(long long)(N - j) * ncol + c] = csub(e, o);
+            }
         }
     }
 }
 
 // ---------------------------------------------------------------------------
 // Analysis: S[f][k][col] (spectral, planar) from F[f][j][col].  Grid (column
-// tiles of 32, fields); block (32, 2 G): warp (g, p) owns the MR coefficients
-// k = 2 (g MR + i) + p.  Chunks of JC points j (ascending) are folded into
-// e_j = X_j + X_{N-j}, o_j = X_j - X_{N-j} while staged in shared memory.
+// tiles of 32, fields); block (32, 2 G): warp (g, p) owns k = 2 m + p for
+// m = 16 g .. 16 g + 15, accumulated with 8x8x4 FP64 MMA over chunks of JC
+// points j; rows j and N - j are staged by cp.async and folded into
+// X_j +- X_{N-j} as the B fragments are read.
 // ---------------------------------------------------------------------------
 constexpr int kAnaJC = 16;
+constexpr int kAnaStages = 3;
 
-template <int MR>
 __global__ void __launch_bounds__(32 * 2 * kMaxGroups)
 k_yanalysis(Dims d, const double *__restrict__ cana, int kh, const double2 *__restrict__ F,
             double2 *__restrict__ S) {
     extern __shared__ double2 sm[];
     constexpr int JC = kAnaJC;
-    double2 *xab = sm;                                           // [2][2 (j, N-j)][JC][32]
-    double *as = reinterpret_cast<double *>(sm + 2 * 2 * JC * 32);   // [2][JC][2][kh]
+    const int AS = ana_as(kh);
+    constexpr int NS = kAnaStages;
+    double2 *xab = sm;                                                 // [NS][2 side][JC][kXS]
+    double *as = reinterpret_cast<double *>(sm + NS * 2 * JC * kXS);  // [NS][JC][2 par][AS]
     const int lane = threadIdx.x, wy = threadIdx.y;
     const int tid = wy * 32 + lane, nthr = 32 * blockDim.y;
-    const int g = wy >> 1, par = wy & 1;
+    const int kt = blockIdx.z * kMaxGroups + (wy >> 1), par = wy & 1;
+    const int g = lane >> 2, t = lane & 3;
     const int f = blockIdx.y, col0 = blockIdx.x * 32;
     const int ncol = d.ncol, N = d.NY2;
     const double2 *X = F + (long long)f * d.ny2 * ncol;
     const int nchunk = (d.nyh + JC - 1) / JC;
-    // staging of one chunk: rows j and N - j (zero for the middle point and
-    // beyond N/2) and the cosine double2 units
-    const int nxu = JC * 32, nau = JC * kh;
+    const int nxu = 2 * JC * 32, nau = JC * kh;   // X units (both sides), cosine double2 units
     auto fetch = [&](int chunk, int buf) {
-        for (int u = tid; u < 2 * nxu + nau; u += nthr) {
-            if (u < 2 * nxu) {
-                const int side = u >= nxu, v = u - side * nxu;
+        for (int u = tid; u < nxu + nau; u += nthr) {
+            if (u < nxu) {
+                const int side = u >= JC * 32, v = u - side * JC * 32;
                 const int r = v >> 5, l = v & 31;
                 const int j = chunk * JC + r, col = col0 + l;
                 const int jj = side ? N - j : j;
                 const bool ok = j < d.nyh && col < ncol && !(side && jj == j);
-                cp_async16(xab + (buf * 2 + side) * JC * 32 + v, X + (long long)(ok ? jj : 0) * ncol + (ok ? col : 0),
-                           ok ? 16 : 0);
+                cp_async16(xab + ((buf * 2 + side) * JC + r) * kXS + l,
+                           X + (long long)(ok ? jj : 0) * ncol + (ok ? col : 0), ok ? 16 : 0);
             } else {
-                const int c = u - 2 * nxu;
-                const int r = c / kh, h = c - r * kh;
+                const int c = u - nxu;
+                const int r = c / kh, rem = c - r * kh;
+                const int p = rem / (kh / 2), h = rem - p * (kh / 2);
                 const int j = chunk * JC + r;
-                cp_async16(reinterpret_cast<double2 *>(as + buf * JC * 2 * kh) + c,
-                           reinterpret_cast<const double2 *>(cana + (long long)(j < d.nyh ? j : 0) * 2 * kh) + h,
-                           j < d.nyh ? 16 : 0);
+                cp_async16(as + ((buf * JC + r) * 2 + p) * AS + 2 * h,
+                           cana + (long long)(j < d.nyh ? j : 0) * 2 * kh + p * kh + 2 * h, j < d.nyh ? 16 : 0);
             }
         }
         cp_async_commit();
     };
-    double2 acc[MR];
+    double acc[2][8][2];
 #pragma unroll
-    for (int i = 0; i < MR; ++i) acc[i] = mk(0.0, 0.0);
-    const int m0 = g * MR;
-    fetch(0, 0);
+    for (int mr = 0; mr < 2; ++mr)
+#pragma unroll
+        for (int q = 0; q < 8; ++q) acc[mr][q][0] = acc[mr][q][1] = 0.0;
+    const int m0 = kt * 16;
+    const bool kok = m0 < kh;   // warps past the last row tile only stage data
+#pragma unroll
+    for (int c = 0; c < NS - 1; ++c) {
+        if (c < nchunk) fetch(c, c);
+        else cp_async_commit();
+    }
     for (int chunk = 0; chunk < nchunk; ++chunk) {
-        const int buf = chunk & 1;
-        if (chunk + 1 < nchunk) {
-            fetch(chunk + 1, buf ^ 1);
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
-        }
+        const int buf = chunk % NS;
+        cp_async_wait<NS - 2>();
         __syncthreads();
-        const int rmax = min(JC, d.nyh - chunk * JC);
-        for (int r = 0; r < rmax; ++r) {
-            const double2 xa = xab[(buf * 2 * JC + r) * 32 + lane];
-            const double2 xb = xab[((buf * 2 + 1) * JC + r) * 32 + lane];
-            const double2 x = par ? csub(xa, xb) : cadd(xa, xb);
-            const double2 *a2 = reinterpret_cast<const double2 *>(as + ((buf * JC + r) * 2 + par) * kh + m0);
+        if (chunk + NS - 1 < nchunk) fetch(chunk + NS - 1, (chunk + NS - 1) % NS);
+        else cp_async_commit();
 #pragma unroll
-            for (int i = 0; i < MR / 2; ++i) {
-                const double2 a = a2[i];
-                acc[2 * i].x += a.x * x.x;
-                acc[2 * i].y += a.x * x.y;
-                acc[2 * i + 1].x += a.y * x.x;
-                acc[2 * i + 1].y += a.y * x.y;
+        for (int st = 0; st < (kok ? JC / 4 : 0); ++st) {
+            const int r = 4 * st + t;
+            const double *ar = as + ((buf * JC + r) * 2 + par) * AS + m0 + g;
+            const double a0 = ar[0], a1 = ar[8];
+            const double *xa = reinterpret_cast<const double *>(xab + ((buf * 2) * JC + r) * kXS) + (g & 1);
+            const double *xb = reinterpret_cast<const double *>(xab + ((buf * 2 + 1) * JC + r) * kXS) + (g & 1);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int o = 2 * (4 * q + (g >> 1));
+                const double va = xa[o], vb = xb[o];
+                const double bq = par ? va - vb : va + vb;
+                dmma(acc[0][q][0], acc[0][q][1], a0, bq);
+                dmma(acc[1][q][0], acc[1][q][1], a1, bq);
             }
         }
-        __syncthreads();
     }
-    const int col = col0 + lane;
-    if (col < ncol) {
-        const int kzi = col / d.nkx, kx = col - kzi * d.nkx;
-        double2 *Sf = S + (long long)f * d.Ns + (long long)kzi * d.ncy * d.nkx + kx;
-        const double sn = 1.0 / (double)N, s0 = 1.0 / (2.0 * N);
+    cp_async_wait<0>();
+    double2 *Sf = S + (long long)f * d.Ns;
+    const double sn = 1.0 / (double)N, s0 = 1.0 / (2.0 * N);
 #pragma unroll
-        for (int i = 0; i < MR; ++i) {
-            const int k = 2 * (m0 + i) + par;
-            if (k < d.ncy) Sf[(long long)k * d.nkx] = cscale(k == 0 ? s0 : sn, acc[i]);
+    for (int mr = 0; mr < 2; ++mr) {
+        const int k = 2 * (m0 + 8 * mr + g) + par;
+        if (!kok || k >= d.ncy) continue;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int col = col0 + 4 * q + t;
+            if (col >= ncol) continue;
+            const int kzi = col / d.nkx, kx = col - kzi * d.nkx;
+            Sf[((long long)kzi * d.ncy + k) * d.nkx + kx] = cscale(k == 0 ? s0 : sn, mk(acc[mr][q][0], acc[mr][q][1]));
         }
     }
 }
 
 size_t curl_smem(const Dims &d) { return sizeof(double2) * 3 * (size_t)d.ncy * kColsPerBlock; }
-size_t syn_smem(const Dims &d) {
-    const size_t jp = (size_t)syn_groups(d) * kSynRows;
-    const size_t pipe = sizeof(double2) * 2 * kSynKC * 32 + sizeof(double) * 2 * kSynKC * jp;
-    const size_t ex = sizeof(double2) * jp * 32;
+size_t syn_smem(const Dims &) {
+    const size_t pipe = sizeof(double2) * kSynStages * 2 * (kSynKC / 2) * kXS +
+                        sizeof(double) * kSynStages * 2 * (kSynKC / 2) * syn_cs(kSynTiles * 16);
+    const size_t ex = sizeof(double2) * (size_t)kSynTiles * 16 * 36;
     return pipe > ex ? pipe : ex;
 }
 size_t ana_smem(const Dims &d) {
-    const size_t kh = (size_t)ana_groups(d) * kAnaRows;
-    return sizeof(double2) * 2 * 2 * kAnaJC * 32 + sizeof(double) * 2 * kAnaJC * 2 * kh;
+    const int kh = ana_groups(d) * kAnaRows;
+    return sizeof(double2) * kAnaStages * 2 * kAnaJC * kXS + sizeof(double) * kAnaStages * kAnaJC * 2 * ana_as(kh);
 }
 }  // namespace
 
@@ -373,11 +414,10 @@ void launch_cheb_tables(const Dims &d, const double *cosy, double *csyn, double 
 }
 
 cudaError_t configure_cheb_kernels(const Dims &d) {
-    if (syn_groups(d) > kMaxGroups || ana_groups(d) > kMaxGroups) return cudaErrorInvalidValue;
-    cudaError_t e = cudaFuncSetAttribute(k_ysynth<kSynRows>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(k_ysynth, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)syn_smem(d));
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_yanalysis<kAnaRows>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(k_yanalysis, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)ana_smem(d));
     if (e != cudaSuccess) return e;
     const int sm = (int)curl_smem(d);
@@ -406,16 +446,16 @@ void launch_curl(const Dims &d, const Tables &t, const double2 *u, double2 *om, 
 void launch_ysynth(const Dims &d, const Tables &t, const double2 *src0, const double2 *src1, int nsplit,
                    int nf, double2 *F, cudaStream_t s) {
     const int g = syn_groups(d);
-    dim3 block(32, 2 * g);
-    dim3 grid((d.ncol + 31) / 32, nf);
-    k_ysynth<kSynRows><<<grid, block, syn_smem(d), s>>>(d, t.csyn, g * kSynRows, src0, src1, nsplit, F);
+    dim3 block(32, 2 * std::min(g, kSynTiles));
+    dim3 grid((d.ncol + 31) / 32, nf, (g + kSynTiles - 1) / kSynTiles);
+    k_ysynth<<<grid, block, syn_smem(d), s>>>(d, t.csyn, g * kSynRows, src0, src1, nsplit, F);
 }
 
 void launch_yanalysis(const Dims &d, const Tables &t, const double2 *F, double2 *S, int nf, cudaStream_t s) {
     const int g = ana_groups(d);
-    dim3 block(32, 2 * g);
-    dim3 grid((d.ncol + 31) / 32, nf);
-    k_yanalysis<kAnaRows><<<grid, block, ana_smem(d), s>>>(d, t.cana, g * kAnaRows, F, S);
+    dim3 block(32, 2 * std::min(g, kMaxGroups));
+    dim3 grid((d.ncol + 31) / 32, nf, (g + kMaxGroups - 1) / kMaxGroups);
+    k_yanalysis<<<grid, block, ana_smem(d), s>>>(d, t.cana, g * kAnaRows, F, S);
 }
 
 }  // namespace cdns
