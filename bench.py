@@ -44,7 +44,7 @@ METRIC = ("Reτ180 128×129×128 steps/s: FP64 vs FP32/FP64 (err≤1e-6); "
 PI = math.acos(-1.0)
 WORKLOAD = {"workload": "retau180_fp64_step", "grid": "128x129x128", "product_grid": "196x193x196",
             "domain": "4pi x 2 x 2pi", "Re_tau": 180, "DT": 5e-5, "forcing": "fixed dp/dx",
-            "precision": "fp64", "l2_policy": "inputs larger than L2 (about 1.7 GB of stage traffic per step)"}
+            "precision": "fp64", "l2_policy": "inputs larger than L2 (about 1.9 GB of stage traffic per step)"}
 
 
 def workload_mesh():
@@ -73,6 +73,17 @@ def stage_bytes(mesh):
         # tau pivots ad_p, ad_v (1 complex-equivalent), writes u, p (4)
         "solve": 16 * 29 * Ns,
     }
+
+
+# DRAM bytes (read + write) per launch of each stage's kernel at Re_tau180 from
+# one ncu capture of this build (profiles/ holds the summaries and commands).
+NCU_TRAFFIC = {
+    "curl": 51.15e6 + 9.87e6,
+    "y_synthesis": 102.48e6 + 103.33e6,
+    "x_cross": 236.10e6 + 89.73e6,
+    "y_analysis": 77.81e6 + 13.91e6,
+    "solve": 431.27e6 + 79.19e6,
+}
 
 
 def step_bytes_model(mesh):
@@ -336,7 +347,9 @@ def main():
                            step_model_bytes=step_model,
                            step_roofline_frac=(step_model / (ms_per_step * 1e-3) / 1e9) / peak),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "kernel": top,
+                         "frac": achieved / peak,
+                         "traffic": NCU_TRAFFIC.get(top) if WORKLOAD["workload"] == "retau180_fp64_step" else None,
+                         "kernel": top,
                          "algorithmic_bytes": sb[top], "launch_ms": per_launch[top],
                          "peak_source": peak_kind,
                          "stage_ms": {k: round(v, 5) for k, v in per_launch.items()}},
@@ -345,7 +358,7 @@ def main():
                     "d2h_bytes_per_step": d2h, "steps": KE, "finite": finite,
                     "protocol": "upload + steps 1..K one call each with dpdx readback + download"},
             "clocks": clk,
-            "gpu_launches": 6 * K,
+            "gpu_launches": len(per_launch) * K,   # one kernel per stage per step
         }
         print(json.dumps(line), flush=True)
     ctx.close()
