@@ -225,6 +225,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=0, help="steps of the e2e pass (default: min(K, 200))")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed FP32/FP64 arm")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -297,6 +298,47 @@ def main():
     achieved = sb[top] / (per_launch[top] * 1e-3) / 1e9
     step_model = step_bytes_model(mesh)
 
+    # ---- mixed FP32/FP64 arm: throughput and error after 1000 steps ------
+    mixed = None
+    if not args.no_mixed:
+        cm = cdns.Context(mesh, params, device=local, precision=cdns.PRECISION_MIXED)
+        sm_ = torch.cuda.ExternalStream(cm.stream_ptr(), device=local)
+        cm.set_velocity(host_u.numpy())
+        cm.run(1, W)
+        cm.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        m0 = torch.cuda.Event(enable_timing=True)
+        m1 = torch.cuda.Event(enable_timing=True)
+        m0.record(sm_)
+        cm.run(W + 1, K)
+        m1.record(sm_)
+        cm.synchronize()
+        torch.cuda.synchronize()
+        barrier()
+        tm = torch.tensor([m0.elapsed_time(m1)], device=f"cuda:{local}", dtype=torch.float64)
+        if dist is not None:
+            dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        mixed_ms = float(tm.item()) / K
+        cm.profile_begin()
+        cm.run(W + K + 1, nprof)
+        mstage, mst = cm.profile_end()
+        # error against the FP64 path after 1000 steps from the same field
+        nerr = 1000
+        for c_ in (ctx, cm):
+            c_.set_velocity(host_u.numpy())
+            c_.run(1, nerr)
+            c_.synchronize()
+        v64, v32 = ctx.get_velocity(), cm.get_velocity()
+        errs = [float(np.linalg.norm(v32[..., k] - v64[..., k]) / np.linalg.norm(v64[..., k])) for k in range(3)]
+        mixed = {"value": world * 1000.0 / mixed_ms, "unit": "steps/s", "ms_per_step": mixed_ms,
+                 "speedup_vs_fp64": ms_per_step / mixed_ms,
+                 "rel_l2_vs_fp64_after_1000_steps": errs,
+                 "stage_ms": {k: round(v / mst, 5) for k, v in mstage.items()},
+                 "arithmetic": "fine-grid stages stored FP32; curl, Chebyshev accumulation, "
+                               "tau solves, corrections and mean flow FP64"}
+        cm.close()
+
     # ---- end to end through the C ABI with host buffers -------------------
     KE = args.e2e_steps or min(K, 200)
     ctx2 = cdns.Context(mesh, params, device=local)
@@ -354,6 +396,7 @@ def main():
                          "peak_source": peak_kind,
                          "stage_ms": {k: round(v, 5) for k, v in per_launch.items()}},
             "cpu_baseline": cpu,
+            "mixed": mixed,
             "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": KE, "finite": finite,
                     "protocol": "upload + steps 1..K one call each with dpdx readback + download"},

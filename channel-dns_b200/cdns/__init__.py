@@ -189,11 +189,17 @@ def _ptr(a: np.ndarray) -> ctypes.c_void_p:
     return ctypes.c_void_p(a.ctypes.data)
 
 
+# cdns_precision (include/cdns.h)
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
+
+
 class Context:
     """One device context: the state of Simulation's hot path on a B200."""
 
-    def __init__(self, mesh: Mesh, params: Params, device: int = 0, precision: int = 0):
+    def __init__(self, mesh: Mesh, params: Params, device: int = 0, precision: int = PRECISION_FP64):
         self.mesh = mesh
+        self.precision = precision
         self.params = params
         self._h = ctypes.c_void_p()
         md, pd = mesh.desc(), params.desc()

@@ -18,6 +18,8 @@ struct Dims {
     int nkx, nkz, ncy;   // NXS+1, 2 NZS+1, NYS+1
     int ny2;             // NY2+1 Gauss-Lobatto points
     int ncol;            // nkz*nkx spectral columns
+    int fcol;            // row stride (columns) of the y-physical stage buffer F:
+                         // ncol, rounded up to even for FP32 stages (16-byte rows)
     int nyh;             // NY2/2+1 (half of the y points, symmetric pairs)
     long long Ns;        // nkz*ncy*nkx complex values per spectral component
 };
@@ -63,6 +65,26 @@ __device__ inline double2 cdiv(double2 a, double2 b) {
     return mk((a.x * r + a.y) / den, (a.y * r - a.x) / den);
 }
 __device__ inline double2 cdivr(double2 a, double s) { return mk(a.x / s, a.y / s); }
+
+// FP32 complex arithmetic (the mixed-precision transforms) and a complex-type
+// trait so that butterflies and DFTs are written once for both widths.
+__device__ inline float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ inline float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ inline float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ inline float2 cscale(float s, float2 a) { return make_float2(s * a.x, s * a.y); }
+
+template <class C> struct CReal;
+template <> struct CReal<double2> { using T = double; };
+template <> struct CReal<float2> { using T = float; };
+template <class C> __host__ __device__ inline C mkc(double re, double im);
+template <> __host__ __device__ inline double2 mkc<double2>(double re, double im) { return make_double2(re, im); }
+template <> __host__ __device__ inline float2 mkc<float2>(double re, double im) {
+    return make_float2((float)re, (float)im);
+}
+// complex value converted between widths
+template <class C, class S> __device__ inline C cto(S v) { return mkc<C>(v.x, v.y); }
 
 // Error bits recorded on the device and read by the host after a step.
 enum : unsigned { ERR_NONFINITE = 1u, ERR_PIVOT = 2u };

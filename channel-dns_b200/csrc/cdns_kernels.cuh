@@ -18,6 +18,13 @@ void launch_curl(const Dims &d, const Tables &t, const double2 *u, double2 *om, 
 void launch_ysynth(const Dims &d, const Tables &t, const double2 *src0, const double2 *src1, int nsplit,
                    int nf, double2 *F, cudaStream_t s);
 void launch_yanalysis(const Dims &d, const Tables &t, const double2 *F, double2 *S, int nf, cudaStream_t s);
+// FP32 stage buffers (mixed precision): synthesis written, analysis read as
+// float2.  The (kz, kx) = (0, 0) mean profiles stay FP64 in mean[6][NY2+1]
+// (zero in F); launch_mean_products adds their mean x mean product to N.
+void launch_ysynth(const Dims &d, const Tables &t, const double2 *src0, const double2 *src1, int nsplit,
+                   int nf, float2 *F, double *mean, cudaStream_t s);
+void launch_mean_products(const Dims &d, const Tables &t, const double *mean, double2 *S, cudaStream_t s);
+void launch_yanalysis(const Dims &d, const Tables &t, const float2 *F, double2 *S, int nf, cudaStream_t s);
 
 // ---- transforms.cu ----
 cudaError_t configure_transform_kernels(const Dims &d);
@@ -29,6 +36,13 @@ void launch_z_forward(const Dims &d, const FftPlan &P, const double2 *roots, con
                       double2 *F, int nf, cudaStream_t s);
 void launch_x_c2r(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G,
                   double *phys, cudaStream_t s);
+// FP32 stage buffers (mixed precision); only meshes with register_forms(d)
+bool register_forms(const Dims &d);
+void launch_z_backward(const Dims &d, const double2 *roots, const float2 *F, float2 *G, int nf, cudaStream_t s);
+// mean: FP64 mean profiles [6][NY2+1] added to the FP32 fluctuations in the products
+void launch_x_cross(const Dims &d, const double2 *roots, const float2 *G, float2 *H, const double *mean,
+                    cudaStream_t s);
+void launch_z_forward(const Dims &d, const double2 *roots, const float2 *H, float2 *F, int nf, cudaStream_t s);
 void launch_x_r2c(const Dims &d, const FftPlan &P, const double2 *roots, const double *phys,
                   double2 *H, cudaStream_t s);
 

@@ -179,9 +179,10 @@ constexpr int kSynKC = 16;
 constexpr int kSynStages = 4;
 constexpr int kSynTiles = 4;   // 16-row tiles per block (two warps each); more go to grid.z
 
+template <class CO>
 __global__ void __launch_bounds__(32 * 2 * kSynTiles, 2)
 k_ysynth(Dims d, const double *__restrict__ csyn, int jp, const double2 *__restrict__ src0,
-         const double2 *__restrict__ src1, int nsplit, double2 *__restrict__ F) {
+         const double2 *__restrict__ src1, int nsplit, CO *__restrict__ F, double *__restrict__ mean) {
     extern __shared__ double2 sm[];
     constexpr int KC = kSynKC, KH = KC / 2;
     constexpr int jw = kSynTiles * 16;   // cosine columns staged per block
@@ -266,7 +267,8 @@ k_ysynth(Dims d, const double *__restrict__ csyn, int jp, const double2 *__restr
     }
     __syncthreads();
     if (jok && par == 0) {
-        double2 *Ff = F + (long long)f * d.ny2 * ncol + col0;
+        CO *Ff = F + (long long)f * d.ny2 * d.fcol + col0;
+        const int zc = d.NZS * d.nkx;   // the (kz, kx) = (0, 0) column
 #pragma unroll
         for (int mr = 0; mr < 2; ++mr) {
             const int j = j0 + 8 * mr + g;
@@ -277,8 +279,17 @@ k_ysynth(Dims d, const double *__restrict__ csyn, int jp, const double2 *__restr
                 if (col0 + c >= ncol) continue;
                 const double2 o = ex[(j0 - jb + 8 * mr + g) * kEXS + c];
                 const double2 e = mk(acc[mr][q][0], acc[mr][q][1]);
-                Ff[(long long)j * ncol + c] = cadd(e, o);
-                if (N - j != j) Ff[(long long)(N - j) * ncol + c] = csub(e, o);
+                if (mean && col0 + c == zc) {
+                    // mean profile (kz, kx) = (0, 0): kept in FP64, out of the FP32 stages
+                    // (its imaginary part is round-off of a real profile)
+                    mean[f * d.ny2 + j] = e.x + o.x;
+                    mean[f * d.ny2 + N - j] = e.x - o.x;
+                    Ff[(long long)j * d.fcol + c] = mkc<CO>(0.0, 0.0);
+                    if (N - j != j) Ff[(long long)(N - j) * d.fcol + c] = mkc<CO>(0.0, 0.0);
+                    continue;
+                }
+                Ff[(long long)j * d.fcol + c] = cto<CO>(cadd(e, o));
+                if (N - j != j) Ff[(long long)(N - j) * d.fcol + c] = cto<CO>(csub(e, o));
             }
         }
     }
@@ -293,35 +304,49 @@ k_ysynth(Dims d, const double *__restrict__ csyn, int jp, const double2 *__restr
 // ---------------------------------------------------------------------------
 constexpr int kAnaJC = 16;
 constexpr int kAnaStages = 3;
+// double2 slots taken by the staged rows of the analysis (j and N - j, all stages)
+__host__ __device__ constexpr int ana_x_slots(int xs, int elem) {
+    return (kAnaStages * 2 * kAnaJC * xs * elem + 15) / 16;
+}
 
+template <class CI>
 __global__ void __launch_bounds__(32 * 2 * kMaxGroups)
-k_yanalysis(Dims d, const double *__restrict__ cana, int kh, const double2 *__restrict__ F,
+k_yanalysis(Dims d, const double *__restrict__ cana, int kh, const CI *__restrict__ F,
             double2 *__restrict__ S) {
+    // staged complex row of 32 columns: 34 slots for FP64, 36 for FP32 (16-byte units)
+    constexpr bool F32 = sizeof(CI) == 8;
+    constexpr int XS = F32 ? 36 : kXS;
     extern __shared__ double2 sm[];
     constexpr int JC = kAnaJC;
     const int AS = ana_as(kh);
     constexpr int NS = kAnaStages;
-    double2 *xab = sm;                                                 // [NS][2 side][JC][kXS]
-    double *as = reinterpret_cast<double *>(sm + NS * 2 * JC * kXS);  // [NS][JC][2 par][AS]
+    CI *xab = reinterpret_cast<CI *>(sm);                                       // [NS][2 side][JC][XS]
+    double *as = reinterpret_cast<double *>(sm + ana_x_slots(XS, sizeof(CI)));  // [NS][JC][2 par][AS]
+    // folded rows e = X_j + X_{N-j}, o = X_j - X_{N-j} in FP64 [2][JC][kXS]: in place
+    // over the stage buffer for FP64 input, a buffer of their own for FP32 input
+    double2 *eo_f32 = reinterpret_cast<double2 *>(as + NS * JC * 2 * AS);
     const int lane = threadIdx.x, wy = threadIdx.y;
     const int tid = wy * 32 + lane, nthr = 32 * blockDim.y;
     const int kt = blockIdx.z * kMaxGroups + (wy >> 1), par = wy & 1;
     const int g = lane >> 2, t = lane & 3;
     const int f = blockIdx.y, col0 = blockIdx.x * 32;
     const int ncol = d.ncol, N = d.NY2;
-    const double2 *X = F + (long long)f * d.ny2 * ncol;
+    const CI *X = F + (long long)f * d.ny2 * d.fcol;
     const int nchunk = (d.nyh + JC - 1) / JC;
-    const int nxu = 2 * JC * 32, nau = JC * kh;   // X units (both sides), cosine double2 units
+    // X units of 16 bytes (one double2 or two float2 columns), both sides; cosine double2 units
+    constexpr int CPU_ = 16 / sizeof(CI), UPR = 32 / CPU_;
+    const int nxu = 2 * JC * UPR, nau = JC * kh;
     auto fetch = [&](int chunk, int buf) {
         for (int u = tid; u < nxu + nau; u += nthr) {
             if (u < nxu) {
-                const int side = u >= JC * 32, v = u - side * JC * 32;
-                const int r = v >> 5, l = v & 31;
+                const int side = u >= JC * UPR, v = u - side * JC * UPR;
+                const int r = v / UPR, l = (v - r * UPR) * CPU_;
                 const int j = chunk * JC + r, col = col0 + l;
                 const int jj = side ? N - j : j;
                 const bool ok = j < d.nyh && col < ncol && !(side && jj == j);
-                cp_async16(xab + ((buf * 2 + side) * JC + r) * kXS + l,
-                           X + (long long)(ok ? jj : 0) * ncol + (ok ? col : 0), ok ? 16 : 0);
+                const int bytes = ok ? (int)sizeof(CI) * min(CPU_, ncol - col) : 0;
+                cp_async16(xab + ((buf * 2 + side) * JC + r) * XS + l,
+                           X + (long long)(ok ? jj : 0) * d.fcol + (ok ? col : 0), bytes);
             } else {
                 const int c = u - nxu;
                 const int r = c / kh, rem = c - r * kh;
@@ -351,18 +376,25 @@ k_yanalysis(Dims d, const double *__restrict__ cana, int kh, const double2 *__re
         __syncthreads();
         if (chunk + NS - 1 < nchunk) fetch(chunk + NS - 1, (chunk + NS - 1) % NS);
         else cp_async_commit();
+        // fold (and widen) this chunk once: eo[0] = e, eo[1] = o
+        double2 *eo = F32 ? eo_f32 : reinterpret_cast<double2 *>(xab + buf * 2 * JC * XS);
+        for (int i = tid; i < JC * 32; i += nthr) {
+            const int r = i >> 5, l = i & 31;
+            const double2 a = cto<double2>(xab[(buf * 2 * JC + r) * XS + l]);
+            const double2 b = cto<double2>(xab[((buf * 2 + 1) * JC + r) * XS + l]);
+            eo[r * kXS + l] = cadd(a, b);
+            eo[(JC + r) * kXS + l] = csub(a, b);
+        }
+        __syncthreads();
 #pragma unroll
         for (int st = 0; st < (kok ? JC / 4 : 0); ++st) {
             const int r = 4 * st + t;
             const double *ar = as + ((buf * JC + r) * 2 + par) * AS + m0 + g;
             const double a0 = ar[0], a1 = ar[8];
-            const double *xa = reinterpret_cast<const double *>(xab + ((buf * 2) * JC + r) * kXS) + (g & 1);
-            const double *xb = reinterpret_cast<const double *>(xab + ((buf * 2 + 1) * JC + r) * kXS) + (g & 1);
+            const double *xr = reinterpret_cast<const double *>(eo + (par * JC + r) * kXS) + (g & 1);
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
-                const int o = 2 * (4 * q + (g >> 1));
-                const double va = xa[o], vb = xb[o];
-                const double bq = par ? va - vb : va + vb;
+                const double bq = xr[2 * (4 * q + (g >> 1))];
                 dmma(acc[0][q][0], acc[0][q][1], a0, bq);
                 dmma(acc[1][q][0], acc[1][q][1], a1, bq);
             }
@@ -370,7 +402,9 @@ k_yanalysis(Dims d, const double *__restrict__ cana, int kh, const double2 *__re
     }
     cp_async_wait<0>();
     double2 *Sf = S + (long long)f * d.Ns;
-    const double sn = 1.0 / (double)N, s0 = 1.0 / (2.0 * N);
+    // FP32 stage buffers arrive without the 1/(NX2 NZ2) of the x and z analyses
+    const double sxz = F32 ? 1.0 / ((double)d.NX2 * (double)d.NZ2) : 1.0;
+    const double sn = sxz / (double)N, s0 = sxz / (2.0 * N);
 #pragma unroll
     for (int mr = 0; mr < 2; ++mr) {
         const int k = 2 * (m0 + 8 * mr + g) + par;
@@ -385,6 +419,42 @@ k_yanalysis(Dims d, const double *__restrict__ cana, int kh, const double2 *__re
     }
 }
 
+// Mean x mean part of u x omega for the mixed path: P(j) = M_u(j) x M_om(j)
+// of the FP64 mean profiles, analysed like k_yanalysis and added to the
+// (kz, kx) = (0, 0) column of N.  Each block forms the products in shared
+// memory; one warp per (component, coefficient) sums them.
+__global__ void k_mean_products(Dims d, const double *__restrict__ cana, int kh, const double *__restrict__ mean,
+                                double2 *__restrict__ S) {
+    extern __shared__ double sp[];   // [3][NY2+1]
+    const int N = d.NY2, ny2 = d.ny2;
+    for (int j = threadIdx.x; j < ny2; j += blockDim.x) {
+        const double mu = mean[j], mv = mean[ny2 + j], mw = mean[2 * ny2 + j];
+        const double ox = mean[3 * ny2 + j], oy = mean[4 * ny2 + j], oz = mean[5 * ny2 + j];
+        sp[j] = mv * oz - mw * oy;
+        sp[ny2 + j] = mw * ox - mu * oz;
+        sp[2 * ny2 + j] = mu * oy - mv * ox;
+    }
+    __syncthreads();
+    // one warp per (component, coefficient): lanes stride over j, shuffle sum
+    const int lane = threadIdx.x & 31;
+    const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (i >= 3 * d.ncy) return;
+    const int c = i / d.ncy, k = i - (i / d.ncy) * d.ncy;
+    const int p = k & 1, m = k >> 1;
+    const double *P = sp + c * ny2;
+    double acc = 0.0;
+    for (int j = lane; j < d.nyh; j += 32) {
+        const double x = (N - j == j) ? P[j] : (p ? P[j] - P[N - j] : P[j] + P[N - j]);
+        acc += cana[(long long)j * 2 * kh + p * kh + m] * x;
+    }
+    acc = sum_warp(acc);
+    if (lane == 0) {
+        const double sc = k == 0 ? 1.0 / (2.0 * N) : 1.0 / (double)N;
+        double2 *s = S + (long long)c * d.Ns + ((long long)d.NZS * d.ncy + k) * d.nkx;   // kx = 0
+        s->x += sc * acc;
+    }
+}
+
 size_t curl_smem(const Dims &d) { return sizeof(double2) * 3 * (size_t)d.ncy * kColsPerBlock; }
 size_t syn_smem(const Dims &) {
     const size_t pipe = sizeof(double2) * kSynStages * 2 * (kSynKC / 2) * kXS +
@@ -392,9 +462,11 @@ size_t syn_smem(const Dims &) {
     const size_t ex = sizeof(double2) * (size_t)kSynTiles * 16 * 36;
     return pipe > ex ? pipe : ex;
 }
-size_t ana_smem(const Dims &d) {
+size_t ana_smem(const Dims &d, size_t elem) {
     const int kh = ana_groups(d) * kAnaRows;
-    return sizeof(double2) * kAnaStages * 2 * kAnaJC * kXS + sizeof(double) * kAnaStages * kAnaJC * 2 * ana_as(kh);
+    const int xs = elem == 16 ? kXS : 36;
+    const size_t eo = elem == 16 ? 0 : sizeof(double2) * 2 * kAnaJC * kXS;
+    return sizeof(double2) * ana_x_slots(xs, (int)elem) + sizeof(double) * kAnaStages * kAnaJC * 2 * ana_as(kh) + eo;
 }
 }  // namespace
 
@@ -414,11 +486,16 @@ void launch_cheb_tables(const Dims &d, const double *cosy, double *csyn, double 
 }
 
 cudaError_t configure_cheb_kernels(const Dims &d) {
-    cudaError_t e = cudaFuncSetAttribute(k_ysynth, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(k_ysynth<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)syn_smem(d));
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_yanalysis, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)ana_smem(d));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_ysynth<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)syn_smem(d));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_yanalysis<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)ana_smem(d, sizeof(double2)));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_yanalysis<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)ana_smem(d, sizeof(float2)));
     if (e != cudaSuccess) return e;
     const int sm = (int)curl_smem(d);
     switch (lane_elems(d)) {
@@ -443,19 +520,41 @@ void launch_curl(const Dims &d, const Tables &t, const double2 *u, double2 *om, 
     }
 }
 
-void launch_ysynth(const Dims &d, const Tables &t, const double2 *src0, const double2 *src1, int nsplit,
-                   int nf, double2 *F, cudaStream_t s) {
+template <class CO>
+void ysynth(const Dims &d, const Tables &t, const double2 *src0, const double2 *src1, int nsplit, int nf, CO *F,
+            double *mean, cudaStream_t s) {
     const int g = syn_groups(d);
     dim3 block(32, 2 * std::min(g, kSynTiles));
     dim3 grid((d.ncol + 31) / 32, nf, (g + kSynTiles - 1) / kSynTiles);
-    k_ysynth<<<grid, block, syn_smem(d), s>>>(d, t.csyn, g * kSynRows, src0, src1, nsplit, F);
+    k_ysynth<CO><<<grid, block, syn_smem(d), s>>>(d, t.csyn, g * kSynRows, src0, src1, nsplit, F, mean);
+}
+void launch_ysynth(const Dims &d, const Tables &t, const double2 *src0, const double2 *src1, int nsplit,
+                   int nf, double2 *F, cudaStream_t s) {
+    ysynth(d, t, src0, src1, nsplit, nf, F, static_cast<double *>(nullptr), s);
+}
+void launch_ysynth(const Dims &d, const Tables &t, const double2 *src0, const double2 *src1, int nsplit,
+                   int nf, float2 *F, double *mean, cudaStream_t s) {
+    ysynth(d, t, src0, src1, nsplit, nf, F, mean, s);
 }
 
-void launch_yanalysis(const Dims &d, const Tables &t, const double2 *F, double2 *S, int nf, cudaStream_t s) {
+template <class CI>
+void yanalysis(const Dims &d, const Tables &t, const CI *F, double2 *S, int nf, cudaStream_t s) {
     const int g = ana_groups(d);
     dim3 block(32, 2 * std::min(g, kMaxGroups));
     dim3 grid((d.ncol + 31) / 32, nf, (g + kMaxGroups - 1) / kMaxGroups);
-    k_yanalysis<<<grid, block, ana_smem(d), s>>>(d, t.cana, g * kAnaRows, F, S);
+    k_yanalysis<CI><<<grid, block, ana_smem(d, sizeof(CI)), s>>>(d, t.cana, g * kAnaRows, F, S);
+}
+void launch_yanalysis(const Dims &d, const Tables &t, const double2 *F, double2 *S, int nf, cudaStream_t s) {
+    yanalysis(d, t, F, S, nf, s);
+}
+void launch_yanalysis(const Dims &d, const Tables &t, const float2 *F, double2 *S, int nf, cudaStream_t s) {
+    yanalysis(d, t, F, S, nf, s);
+}
+
+void launch_mean_products(const Dims &d, const Tables &t, const double *mean, double2 *S, cudaStream_t s) {
+    const int warps = 3 * d.ncy, per_block = 8;
+    k_mean_products<<<(warps + per_block - 1) / per_block, 32 * per_block, sizeof(double) * 3 * d.ny2, s>>>(
+        d, t.cana, ana_groups(d) * kAnaRows, mean, S);
 }
 
 }  // namespace cdns

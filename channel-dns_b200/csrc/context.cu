@@ -85,6 +85,8 @@ struct cdns_ctx {
     double2 *p = nullptr, *bw = nullptr, *bc_v = nullptr, *bc_p = nullptr;
     double2 *F = nullptr, *G = nullptr, *H = nullptr, *aux = nullptr, *aux2 = nullptr, *zero3 = nullptr;
     double2 *om = nullptr;                // vorticity of the velocity being transformed
+    bool mixed = false;                   // FP32 fine-grid stages (CDNS_PRECISION_MIXED)
+    double *mean = nullptr;               // mixed: FP64 (kz, kx) = (0, 0) profiles [6][NY2+1]
     double *phys = nullptr;
     double *dpdx = nullptr;
     unsigned *err = nullptr;
@@ -140,6 +142,22 @@ void enqueue_nonlinear(cdns_ctx *c, const double2 *u, double2 *N, bool prof, int
     mark(0);
     launch_curl(d, c->t, u, c->om, c->bw, c->pp.Re, s);
     mark(1);
+    if (c->mixed) {
+        float2 *F = reinterpret_cast<float2 *>(c->F), *G = reinterpret_cast<float2 *>(c->G);
+        float2 *H = reinterpret_cast<float2 *>(c->H);
+        launch_ysynth(d, c->t, u, c->om, 3, 6, F, c->mean, s);
+        mark(2);
+        launch_z_backward(d, c->t.root_z, F, G, 6, s);
+        mark(3);
+        launch_x_cross(d, c->t.root_x, G, H, c->mean, s);
+        mark(4);
+        launch_z_forward(d, c->t.root_z, H, F, 3, s);
+        mark(5);
+        launch_yanalysis(d, c->t, F, N, 3, s);
+        launch_mean_products(d, c->t, c->mean, N, s);
+        mark(6);
+        return;
+    }
     launch_ysynth(d, c->t, u, c->om, 3, 6, c->F, s);
     mark(2);
     launch_z_backward(d, c->pz, c->t.root_z, c->F, c->G, 6, s);
@@ -238,7 +256,8 @@ int cdns_create(const cdns_mesh_desc *m, const cdns_params *p, int precision, in
                 cdns_ctx **out) {
     if (!m || !p || !out) return fail(CDNS_ERR_ARG, "null argument");
     *out = nullptr;
-    if (precision != CDNS_PRECISION_FP64) return fail(CDNS_ERR_ARG, "unsupported precision mode");
+    if (precision != CDNS_PRECISION_FP64 && precision != CDNS_PRECISION_MIXED)
+        return fail(CDNS_ERR_ARG, "unsupported precision mode");
     if (m->NYS < 4 || m->NXS < 0 || m->NZS < 0 || m->NY2 < m->NYS || m->NY2 < 2 ||
         m->NX2 < 2 * m->NXS || m->NZ2 < 2 * m->NZS || m->NX2 < 1 || m->NZ2 < 1 ||
         !(m->XL > 0) || !(m->ZL > 0))
@@ -265,12 +284,19 @@ int cdns_create(const cdns_mesh_desc *m, const cdns_params *p, int precision, in
         delete c;
         return fail(CDNS_ERR_ARG, "NX2/NZ2 must factor into primes <= 13");
     }
-    const size_t smem_solve = 16 * 6 * (size_t)d.ncy * 8 + 8 * (2 * (size_t)d.ncy * 8 + 3 * d.ncy);
-    if (smem_solve > 220 * 1024 || (size_t)16 * d.NZ2 * 33 > 220 * 1024 ||
+    // step solve tiles [4][ncy][8] complex; Stockham z/x FFT blocks of up to 17 and 12 lines
+    const size_t smem_solve = 16 * 4 * (size_t)d.ncy * 8;
+    if (smem_solve > 220 * 1024 || (size_t)16 * d.NZ2 * 35 > 220 * 1024 ||
         (size_t)16 * d.NX2 * 25 > 220 * 1024) {
         delete c;
         return fail(CDNS_ERR_ARG, "mesh exceeds the shared-memory tiling limits");
     }
+    if (precision == CDNS_PRECISION_MIXED && !register_forms(d)) {
+        delete c;
+        return fail(CDNS_ERR_ARG, "mixed precision needs NX2 and NZ2 in {48, 72, 96, 144, 192, 196}");
+    }
+    c->mixed = precision == CDNS_PRECISION_MIXED;
+    d.fcol = c->mixed ? d.ncol + (d.ncol & 1) : d.ncol;
     // physics parameters (src/core/params.cpp:296-307)
     PhysParams &pp = c->pp;
     pp.Re = p->Re; pp.G_pre = p->G_pre; pp.a_pre0 = p->a_pre0; pp.b_pre0 = p->b_pre0;
@@ -360,6 +386,7 @@ int cdns_create(const cdns_mesh_desc *m, const cdns_params *p, int precision, in
         (r = c->alloc(c->bc_p, 2 * nc)) || (r = c->alloc(c->F, fbuf)) || (r = c->alloc(c->G, gbuf)) ||
         (r = c->alloc(c->H, hbuf)) || (r = c->alloc(c->aux, 3 * Ns)) || (r = c->alloc(c->aux2, 3 * Ns)) ||
         (r = c->alloc(c->zero3, 3 * Ns)) || (r = c->alloc(c->om, 3 * Ns)) ||
+        (r = c->alloc(c->mean, 6 * (size_t)d.ny2)) ||
         (r = c->alloc(c->phys, (size_t)d.NZ2 * d.ny2 * d.NX2)) || (r = c->alloc(c->dpdx, 2)) ||
         (r = c->alloc(c->err, 1)))
         return bail(r);
@@ -685,6 +712,20 @@ int cdns_debug_copy(cdns_ctx *c, int which, double *out, size_t count) {
     default: return fail(CDNS_ERR_ARG, "unknown debug buffer");
     }
     if (count < 2 * n) return fail(CDNS_ERR_ARG, "debug buffer too small");
+    if (c->mixed && which <= 2) {
+        // FP32 stage buffers: widen on the host (F rows are padded to fcol columns)
+        const size_t row = which == 0 ? (size_t)d.ncol : n, prow = which == 0 ? (size_t)d.fcol : n;
+        const size_t rows = n / row;
+        std::vector<float2> h(rows * prow);
+        CK(cudaMemcpyAsync(h.data(), src, h.size() * sizeof(float2), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        for (size_t r = 0; r < rows; ++r)
+            for (size_t i = 0; i < row; ++i) {
+                out[2 * (r * row + i)] = h[r * prow + i].x;
+                out[2 * (r * row + i) + 1] = h[r * prow + i].y;
+            }
+        return CDNS_OK;
+    }
     if (which == 9) {
         CK(cudaMemcpyAsync(out, c->st.wn_p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         CK(cudaMemcpyAsync(out + n, c->st.wn_v, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));

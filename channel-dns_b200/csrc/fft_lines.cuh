@@ -21,10 +21,26 @@ namespace cdns {
 constexpr int kMaxRadix = 16;
 
 // roots[k] = exp(-2 pi i k / n); SIGN=+1 uses the conjugate.
-template <int SIGN> __device__ __forceinline__ double2 root_of(const double2 *roots, int k) {
-    const double2 r = roots[k];
-    return SIGN < 0 ? r : mk(r.x, -r.y);
+template <int SIGN, class C> __device__ __forceinline__ C root_of(const C *roots, int k) {
+    const C r = roots[k];
+    return SIGN < 0 ? r : mkc<C>(r.x, -r.y);
 }
+
+// A twiddle table exp(-2 pi i k / n): in FP32 each entry carries the residue
+// of its rounding (lo), added by a second product, so that the transform is
+// the exact DFT up to random arithmetic rounding (no systematic operator error).
+template <class C> struct Twiddles {
+    const C *hi, *lo;   // lo is used by the FP32 form only
+    template <int SIGN> __device__ __forceinline__ C at(int k) const { return root_of<SIGN>(hi, k); }
+    template <int SIGN> __device__ __forceinline__ C mul(C v, int k) const {
+        const C w = root_of<SIGN>(hi, k);
+        if constexpr (sizeof(C) == 8) {
+            return cadd(cmul(v, w), cmul(v, root_of<SIGN>(lo, k)));
+        } else {
+            return cmul(v, w);
+        }
+    }
+};
 
 // cos / sin (2 pi i / R) for 0 <= i < R, folded to literals after unrolling.
 template <int R> __device__ __forceinline__ double kcos(int i);
@@ -55,41 +71,51 @@ template <> __device__ __forceinline__ double ksin<7>(int i) {
 // Odd radix by symmetric pairs: with s_t = x_t + x_{R-t}, d_t = x_t - x_{R-t},
 // y_q = x_0 + sum_t s_t cos(2 pi t q/R) + SIGN i sum_t d_t sin(2 pi t q/R),
 // y_{R-q} the same with the sine term negated.
-template <int R, int SIGN, bool TABLE>
-__device__ __forceinline__ void bfly_odd(double2 (&v)[R], const double2 *roots, int n) {
+template <int R, int SIGN, bool TABLE, class C>
+__device__ __forceinline__ void bfly_odd(C (&v)[R], const C *roots, int n) {
+    using T = typename CReal<C>::T;
     constexpr int h = R / 2;
-    double2 s[h + 1], d[h + 1];
+    C s[h + 1], d[h + 1];
 #pragma unroll
     for (int t = 1; t <= h; ++t) {
         s[t] = cadd(v[t], v[R - t]);
         d[t] = csub(v[t], v[R - t]);
     }
-    double2 out[R];
-    double2 y0 = v[0];
+    C out[R];
+    C y0 = v[0];
 #pragma unroll
     for (int t = 1; t <= h; ++t) y0 = cadd(y0, s[t]);
     out[0] = y0;
 #pragma unroll
     for (int q = 1; q <= h; ++q) {
-        double2 re = v[0], im = mk(0.0, 0.0);
+        C re = v[0], im = mkc<C>(0.0, 0.0);
 #pragma unroll
         for (int t = 1; t <= h; ++t) {
             const int i = (t * q) % R;
-            double c, sn;
+            T c, sn;
             if constexpr (TABLE) {
-                const double2 w = roots[i * (n / R)];  // exp(-2 pi i i/R)
+                const C w = roots[i * (n / R)];  // exp(-2 pi i i/R)
                 c = w.x;
                 sn = -w.y;
             } else {
-                c = kcos<R>(i);
-                sn = ksin<R>(i);
+                c = (T)kcos<R>(i);
+                sn = (T)ksin<R>(i);
             }
             re.x += c * s[t].x;
             re.y += c * s[t].y;
             im.x += sn * d[t].x;
             im.y += sn * d[t].y;
+            if constexpr (!TABLE && sizeof(T) == 4) {
+                // FP32: add the rounding residue of the constant, so that the
+                // butterfly is the exact DFT up to random arithmetic rounding
+                const T cl = (T)(kcos<R>(i) - (double)c), sl = (T)(ksin<R>(i) - (double)sn);
+                re.x += cl * s[t].x;
+                re.y += cl * s[t].y;
+                im.x += sl * d[t].x;
+                im.y += sl * d[t].y;
+            }
         }
-        const double2 iim = SIGN < 0 ? mk(im.y, -im.x) : mk(-im.y, im.x);
+        const C iim = SIGN < 0 ? mkc<C>(im.y, -im.x) : mkc<C>(-im.y, im.x);
         out[q] = cadd(re, iim);
         out[R - q] = csub(re, iim);
     }
@@ -97,18 +123,18 @@ __device__ __forceinline__ void bfly_odd(double2 (&v)[R], const double2 *roots, 
     for (int q = 0; q < R; ++q) v[q] = out[q];
 }
 
-template <int R, int SIGN>
-__device__ __forceinline__ void bfly(double2 (&v)[R], const double2 *roots, int n) {
+template <int R, int SIGN, class C>
+__device__ __forceinline__ void bfly(C (&v)[R], const C *roots, int n) {
     if constexpr (R == 1) {
         return;
     } else if constexpr (R == 2) {
-        const double2 a = v[0], b = v[1];
+        const C a = v[0], b = v[1];
         v[0] = cadd(a, b);
         v[1] = csub(a, b);
     } else if constexpr (R == 4) {
-        const double2 a = cadd(v[0], v[2]), b = csub(v[0], v[2]);
-        const double2 c = cadd(v[1], v[3]), d = csub(v[1], v[3]);
-        const double2 di = SIGN < 0 ? mk(d.y, -d.x) : mk(-d.y, d.x);  // SIGN i d
+        const C a = cadd(v[0], v[2]), b = csub(v[0], v[2]);
+        const C c = cadd(v[1], v[3]), d = csub(v[1], v[3]);
+        const C di = SIGN < 0 ? mkc<C>(d.y, -d.x) : mkc<C>(-d.y, d.x);  // SIGN i d
         v[0] = cadd(a, c);
         v[1] = cadd(b, di);
         v[2] = csub(a, c);

@@ -107,6 +107,7 @@ extern "C" int cdns_transform_fine_backward_noalloc(const cdns_mesh_desc *m, con
     d.NXS = m->NXS; d.NYS = m->NYS; d.NZS = m->NZS;
     d.nkx = m->NXS + 1; d.nkz = 2 * m->NZS + 1; d.ncy = m->NYS + 1; d.ny2 = m->NY2 + 1;
     d.ncol = d.nkx * d.nkz;
+    d.fcol = d.ncol;
     d.nyh = m->NY2 / 2 + 1;
     d.Ns = (long long)d.nkz * d.ncy * d.nkx;
     FftPlan px{}, pz{};

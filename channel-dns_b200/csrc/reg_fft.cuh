@@ -17,38 +17,39 @@ template <> struct RegSplit<4> { static constexpr int A = 4, B = 1; };
 template <> struct RegSplit<6> { static constexpr int A = 2, B = 3; };
 template <> struct RegSplit<7> { static constexpr int A = 7, B = 1; };
 template <> struct RegSplit<8> { static constexpr int A = 2, B = 4; };
+template <> struct RegSplit<9> { static constexpr int A = 3, B = 3; };
 template <> struct RegSplit<10> { static constexpr int A = 2, B = 5; };
 template <> struct RegSplit<12> { static constexpr int A = 3, B = 4; };
 template <> struct RegSplit<14> { static constexpr int A = 2, B = 7; };
 template <> struct RegSplit<16> { static constexpr int A = 4, B = 4; };
 
 // X[c + A d] = sum_m v[m] W_N^(m (c + A d)), W_N = exp(SIGN 2 pi i / N), in place.
-// roots[m * rstride] = exp(-2 pi i m / N) for 0 <= m < N.
-template <int N, int SIGN>
-__device__ __forceinline__ void dft_reg(double2 (&v)[N], const double2 *roots, int rstride) {
+// tw.hi[m * rstride] = exp(-2 pi i m / N) for 0 <= m < N.
+template <int N, int SIGN, class C>
+__device__ __forceinline__ void dft_reg(C (&v)[N], const Twiddles<C> &tw, int rstride) {
     constexpr int A = RegSplit<N>::A, B = RegSplit<N>::B;
     if constexpr (B == 1) {
-        bfly<A, SIGN>(v, nullptr, 0);
+        bfly<A, SIGN>(v, static_cast<const C *>(nullptr), 0);
     } else {
-        double2 y[N];
+        C y[N];
         // m = b + B a: radix-A DFTs over a, twiddled by W_N^(b c)
 #pragma unroll
         for (int b = 0; b < B; ++b) {
-            double2 t[A];
+            C t[A];
 #pragma unroll
             for (int a = 0; a < A; ++a) t[a] = v[b + B * a];
-            bfly<A, SIGN>(t, nullptr, 0);
+            bfly<A, SIGN>(t, static_cast<const C *>(nullptr), 0);
 #pragma unroll
             for (int c = 0; c < A; ++c)
-                y[b * A + c] = (b * c == 0) ? t[c] : cmul(t[c], root_of<SIGN>(roots, ((b * c) % N) * rstride));
+                y[b * A + c] = (b * c == 0) ? t[c] : tw.template mul<SIGN>(t[c], ((b * c) % N) * rstride);
         }
         // radix-B DFTs over b
 #pragma unroll
         for (int c = 0; c < A; ++c) {
-            double2 t[B];
+            C t[B];
 #pragma unroll
             for (int b = 0; b < B; ++b) t[b] = y[b * A + c];
-            bfly<B, SIGN>(t, nullptr, 0);
+            bfly<B, SIGN>(t, static_cast<const C *>(nullptr), 0);
 #pragma unroll
             for (int d = 0; d < B; ++d) v[c + A * d] = t[d];
         }

@@ -24,45 +24,45 @@ namespace cdns {
 // HBM into the NZ2 slots (negative Nyquist slot wins at a full z spectrum,
 // src/fft/transforms.cpp:715-732); the last pass writes z-physical rows.
 // ---------------------------------------------------------------------------
-struct ZExpandSrc {
-    const double2 *Fp;   // one (field, y point) plane [kz][kx]
+template <class C> struct ZExpandSrc {
+    const C *Fp;   // one (field, y point) plane [kz][kx]
     int nkx, kx0, NZS, n;
-    __device__ __forceinline__ double2 operator()(int z, int line) const {
+    __device__ __forceinline__ C operator()(int z, int line) const {
         const int kx = kx0 + line;
-        if (kx >= nkx) return mk(0, 0);
+        if (kx >= nkx) return mkc<C>(0, 0);
         int kz;
         if (z <= NZS) kz = (z == n - NZS) ? -NZS : z;
         else if (z >= n - NZS) kz = z - n;
-        else return mk(0, 0);
+        else return mkc<C>(0, 0);
         return Fp[(kz + NZS) * nkx + kx];
     }
 };
-struct RowDst {
-    double2 *p;   // [pos][kx]
+template <class C> struct RowDst {
+    C *p;   // [pos][kx]
     int nkx, kx0;
-    __device__ __forceinline__ void operator()(int pos, int line, double2 v) const {
+    __device__ __forceinline__ void operator()(int pos, int line, C v) const {
         const int kx = kx0 + line;
         if (kx < nkx) p[(long long)pos * nkx + kx] = v;
     }
 };
-struct RowSrc {
-    const double2 *p;
+template <class C> struct RowSrc {
+    const C *p;
     int nkx, kx0;
-    __device__ __forceinline__ double2 operator()(int pos, int line) const {
+    __device__ __forceinline__ C operator()(int pos, int line) const {
         const int kx = kx0 + line;
-        return kx < nkx ? p[(long long)pos * nkx + kx] : mk(0, 0);
+        return kx < nkx ? p[(long long)pos * nkx + kx] : mkc<C>(0, 0);
     }
 };
 // Forward z: keep kz in [-NZS, NZS] scaled by 1/NZ2 (src/fft/transforms.cpp:658-665);
 // at a full z spectrum slot NZS feeds both kz = +NZS and kz = -NZS.
-struct ZTruncDst {
-    double2 *Fp;
+template <class C> struct ZTruncDst {
+    C *Fp;
     int nkx, kx0, NZS, n;
-    double invn;
-    __device__ __forceinline__ void operator()(int z, int line, double2 v) const {
+    typename CReal<C>::T invn;
+    __device__ __forceinline__ void operator()(int z, int line, C v) const {
         const int kx = kx0 + line;
         if (kx >= nkx) return;
-        const double2 s = cscale(invn, v);
+        const C s = cscale(invn, v);
         if (z <= NZS) Fp[(z + NZS) * nkx + kx] = s;
         if (z >= n - NZS) Fp[(z - n + NZS) * nkx + kx] = s;
     }
@@ -79,8 +79,8 @@ k_z_backward(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2
     const int f = blockIdx.z, j = blockIdx.y, kx0 = blockIdx.x * TL;
     for (int i = threadIdx.x; i < n; i += blockDim.x) s_root[i] = roots[i];
     __syncthreads();
-    const ZExpandSrc src{F + ((long long)f * d.ny2 + j) * d.ncol, d.nkx, kx0, d.NZS, n};
-    const RowDst dst{G + ((long long)f * d.ny2 + j) * (long long)n * d.nkx, d.nkx, kx0};
+    const ZExpandSrc<double2> src{F + ((long long)f * d.ny2 + j) * d.fcol, d.nkx, kx0, d.NZS, n};
+    const RowDst<double2> dst{G + ((long long)f * d.ny2 + j) * (long long)n * d.nkx, d.nkx, kx0};
     fft_run<+1>(a, b, TL, P, s_root, src, dst);
 }
 
@@ -95,20 +95,32 @@ k_z_forward(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 
     const int f = blockIdx.z, j = blockIdx.y, kx0 = blockIdx.x * TL;
     for (int i = threadIdx.x; i < n; i += blockDim.x) s_root[i] = roots[i];
     __syncthreads();
-    const RowSrc src{H + ((long long)f * d.ny2 + j) * (long long)n * d.nkx, d.nkx, kx0};
-    const ZTruncDst dst{F + ((long long)f * d.ny2 + j) * d.ncol, d.nkx, kx0, d.NZS, n, 1.0 / (double)n};
+    const RowSrc<double2> src{H + ((long long)f * d.ny2 + j) * (long long)n * d.nkx, d.nkx, kx0};
+    const ZTruncDst<double2> dst{F + ((long long)f * d.ny2 + j) * d.fcol, d.nkx, kx0, d.NZS, n, 1.0 / (double)n};
     fft_run<-1>(a, b, TL, P, s_root, src, dst);
 }
 
 // Register form of the z transforms for NZ2 = N1 x N2: threads t = n2 TL + l
 // (step 1) and t = k1 TL + l (step 2) over TL kx lines, one shared-memory
 // exchange S[k1][n2][l]; loads and stores run along kx.
-template <int N1, int N2, int SIGN, class Src, class Dst>
-__device__ __forceinline__ void fft2_lines(int TL, const double2 *s_root, double2 *S, const Src &src,
-                                           const Dst &dst) {
+// Shared twiddle table of the register forms: n double2 slots, holding the
+// FP64 roots, or the FP32 roots and their rounding residues.
+template <class C> __device__ __forceinline__ Twiddles<C> load_twiddles(double2 *sm_d, const double2 *roots, int n) {
+    C *hi = reinterpret_cast<C *>(sm_d);
+    C *lo = sizeof(C) == 8 ? hi + n : hi;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double2 r = roots[i];
+        hi[i] = cto<C>(r);
+        if (sizeof(C) == 8) lo[i] = mkc<C>(r.x - (double)hi[i].x, r.y - (double)hi[i].y);
+    }
+    return Twiddles<C>{hi, lo};
+}
+
+template <int N1, int N2, int SIGN, class C, class Src, class Dst>
+__device__ __forceinline__ void fft2_lines(int TL, const Twiddles<C> &tw, C *S, const Src &src, const Dst &dst) {
     constexpr int NM = N1 > N2 ? N1 : N2;
     const int t = threadIdx.x;
-    double2 v[NM];
+    C v[NM];
     const bool a1 = t < N2 * TL;
     const int n2 = t / TL, l1 = t - (t / TL) * TL;
     if (a1) {
@@ -117,53 +129,50 @@ __device__ __forceinline__ void fft2_lines(int TL, const double2 *s_root, double
     }
     __syncthreads();   // s_root complete
     if (a1) {
-        double2(&w)[N1] = reinterpret_cast<double2(&)[N1]>(v);
-        dft_reg<N1, SIGN>(w, s_root, N2);
+        C(&w)[N1] = reinterpret_cast<C(&)[N1]>(v);
+        dft_reg<N1, SIGN>(w, tw, N2);
 #pragma unroll
         for (int k1 = 0; k1 < N1; ++k1)
-            S[(k1 * N2 + n2) * TL + l1] =
-                (k1 == 0 || n2 == 0) ? w[k1] : cmul(w[k1], root_of<SIGN>(s_root, n2 * k1));
+            S[(k1 * N2 + n2) * TL + l1] = (k1 == 0 || n2 == 0) ? w[k1] : tw.template mul<SIGN>(w[k1], n2 * k1);
     }
     __syncthreads();
     if (t < N1 * TL) {
         const int k1 = t / TL, l = t - (t / TL) * TL;
 #pragma unroll
         for (int m = 0; m < N2; ++m) v[m] = S[(k1 * N2 + m) * TL + l];
-        double2(&w)[N2] = reinterpret_cast<double2(&)[N2]>(v);
-        dft_reg<N2, SIGN>(w, s_root, N1);
+        C(&w)[N2] = reinterpret_cast<C(&)[N2]>(v);
+        dft_reg<N2, SIGN>(w, tw, N1);
 #pragma unroll
         for (int k2 = 0; k2 < N2; ++k2) dst(k1 + N1 * k2, l, w[k2]);
     }
 }
 
-template <int N1, int N2>
+template <int N1, int N2, class C>
 __global__ void __launch_bounds__(16 * 17)
-k_z_backward_r(Dims d, const double2 *__restrict__ roots, const double2 *__restrict__ F,
-               double2 *__restrict__ G, int TL) {
-    extern __shared__ double2 sm[];
+k_z_backward_r(Dims d, const double2 *__restrict__ roots, const C *__restrict__ F, C *__restrict__ G, int TL) {
+    extern __shared__ double2 sm_d[];
     constexpr int n = N1 * N2;
-    double2 *s_root = sm;
-    double2 *S = sm + n;
+    C *S = reinterpret_cast<C *>(sm_d + n);
     const int f = blockIdx.z, j = blockIdx.y, kx0 = blockIdx.x * TL;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) s_root[i] = roots[i];
-    const ZExpandSrc src{F + ((long long)f * d.ny2 + j) * d.ncol, d.nkx, kx0, d.NZS, n};
-    const RowDst dst{G + ((long long)f * d.ny2 + j) * (long long)n * d.nkx, d.nkx, kx0};
-    fft2_lines<N1, N2, +1>(TL, s_root, S, src, dst);
+    const Twiddles<C> tw = load_twiddles<C>(sm_d, roots, n);
+    const ZExpandSrc<C> src{F + ((long long)f * d.ny2 + j) * d.fcol, d.nkx, kx0, d.NZS, n};
+    const RowDst<C> dst{G + ((long long)f * d.ny2 + j) * (long long)n * d.nkx, d.nkx, kx0};
+    fft2_lines<N1, N2, +1>(TL, tw, S, src, dst);
 }
 
-template <int N1, int N2>
+template <int N1, int N2, class C>
 __global__ void __launch_bounds__(16 * 17)
-k_z_forward_r(Dims d, const double2 *__restrict__ roots, const double2 *__restrict__ H,
-              double2 *__restrict__ F, int TL) {
-    extern __shared__ double2 sm[];
+k_z_forward_r(Dims d, const double2 *__restrict__ roots, const C *__restrict__ H, C *__restrict__ F, int TL) {
+    extern __shared__ double2 sm_d[];
     constexpr int n = N1 * N2;
-    double2 *s_root = sm;
-    double2 *S = sm + n;
+    C *S = reinterpret_cast<C *>(sm_d + n);
     const int f = blockIdx.z, j = blockIdx.y, kx0 = blockIdx.x * TL;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) s_root[i] = roots[i];
-    const RowSrc src{H + ((long long)f * d.ny2 + j) * (long long)n * d.nkx, d.nkx, kx0};
-    const ZTruncDst dst{F + ((long long)f * d.ny2 + j) * d.ncol, d.nkx, kx0, d.NZS, n, 1.0 / (double)n};
-    fft2_lines<N1, N2, -1>(TL, s_root, S, src, dst);
+    const Twiddles<C> tw = load_twiddles<C>(sm_d, roots, n);
+    const RowSrc<C> src{H + ((long long)f * d.ny2 + j) * (long long)n * d.nkx, d.nkx, kx0};
+    // FP32: no 1/NZ2 here (not exact in FP32); the FP64 y analysis applies 1/(NX2 NZ2)
+    const ZTruncDst<C> dst{F + ((long long)f * d.ny2 + j) * d.fcol, d.nkx, kx0, d.NZS, n,
+                           (typename CReal<C>::T)(sizeof(C) == 8 ? 1.0 : 1.0 / (double)n)};
+    fft2_lines<N1, N2, -1>(TL, tw, S, src, dst);
 }
 
 // ---------------------------------------------------------------------------
@@ -275,59 +284,59 @@ k_x_cross(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 *_
 // S and P share one buffer; every phase reads into registers before a
 // barrier and writes after it.
 // ---------------------------------------------------------------------------
-template <int N1, int N2>
+template <int N1, int N2, class C, bool MEAN>
 __global__ void __launch_bounds__(16 * 3 * 4)
-k_x_cross_r(Dims d, const double2 *__restrict__ roots, const double2 *__restrict__ G,
-            double2 *__restrict__ H, int RW) {
+k_x_cross_r(Dims d, const double2 *__restrict__ roots, const C *__restrict__ G, C *__restrict__ H, int RW,
+            const double *__restrict__ mean) {
+    using T = typename CReal<C>::T;
     constexpr int n = N1 * N2;
     constexpr int SP = N2 + 1;   // padded row of the step-1 output
-    extern __shared__ double2 sm[];
-    double2 *s_root = sm;
-    double2 *buf = sm + n;
+    extern __shared__ double2 sm_d[];
+    C *buf = reinterpret_cast<C *>(sm_d + n);
     const int L = 3 * RW, L2 = 3 * (RW / 2);
     const int slot = threadIdx.x >> 4, sub = threadIdx.x & 15;
     const int j = blockIdx.y, z0 = blockIdx.x * RW;
     const int nkx = d.nkx, nxs = d.NXS;
     const long long fstride = (long long)d.ny2 * d.NZ2 * nkx;
-    const double2 *Gj = G + (long long)j * d.NZ2 * nkx;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) s_root[i] = roots[i];
+    const C *Gj = G + (long long)j * d.NZ2 * nkx;
+    const Twiddles<C> tw = load_twiddles<C>(sm_d, roots, n);
     const int nyq = (n % 2 == 0) ? n / 2 : -1;
-    double2 v[N1 > N2 ? N1 : N2];
+    C v[N1 > N2 ? N1 : N2];
 
     // ---- phase 1: spectrum gather, N1-point DFTs over n1 (backward) --------
     const bool act1 = slot < L && sub < N2;
     if (act1) {
         const int r = slot / 3, pl = slot - (slot / 3) * 3;
         const int z = z0 + r;
-        const double2 *rowA = Gj + (long long)z * nkx + (2 * pl) * fstride;
-        const double2 *rowB = rowA + fstride;
+        const C *rowA = Gj + (long long)z * nkx + (2 * pl) * fstride;
+        const C *rowB = rowA + fstride;
 #pragma unroll
         for (int n1 = 0; n1 < N1; ++n1) {
             const int m = sub + N2 * n1;
-            double2 x = mk(0.0, 0.0);
+            C x = mkc<C>(0.0, 0.0);
             if (z < d.NZ2) {
                 if (m <= nxs) {
-                    double2 A = rowA[m], B = rowB[m];
+                    C A = rowA[m], B = rowB[m];
                     if (m == 0 || m == nyq) {
                         A.y = 0.0;
                         B.y = 0.0;
                     }
-                    x = mk(A.x - B.y, A.y + B.x);
+                    x = mkc<C>(A.x - B.y, A.y + B.x);
                 } else if (m >= n - nxs && m != nyq) {
-                    const double2 A = rowA[n - m], B = rowB[n - m];
-                    x = mk(A.x + B.y, B.x - A.y);
+                    const C A = rowA[n - m], B = rowB[n - m];
+                    x = mkc<C>(A.x + B.y, B.x - A.y);
                 }
             }
             v[n1] = x;
         }
     }
-    __syncthreads();   // s_root complete
+    __syncthreads();   // twiddles complete
     if (act1) {
-        double2(&w)[N1] = reinterpret_cast<double2(&)[N1]>(v);
-        dft_reg<N1, +1>(w, s_root, N2);
+        C(&w)[N1] = reinterpret_cast<C(&)[N1]>(v);
+        dft_reg<N1, +1>(w, tw, N2);
 #pragma unroll
         for (int k1 = 0; k1 < N1; ++k1) {
-            const double2 t = (k1 == 0 || sub == 0) ? w[k1] : cmul(w[k1], root_of<+1>(s_root, sub * k1));
+            const C t = (k1 == 0 || sub == 0) ? w[k1] : tw.template mul<+1>(w[k1], sub * k1);
             buf[(slot * N1 + k1) * SP + sub] = t;
         }
     }
@@ -340,13 +349,23 @@ k_x_cross_r(Dims d, const double2 *__restrict__ roots, const double2 *__restrict
     }
     __syncthreads();
     if (act2) {
-        double2(&w)[N2] = reinterpret_cast<double2(&)[N2]>(v);
-        dft_reg<N2, +1>(w, s_root, N1);
+        C(&w)[N2] = reinterpret_cast<C(&)[N2]>(v);
+        dft_reg<N2, +1>(w, tw, N1);
 #pragma unroll
         for (int k2 = 0; k2 < N2; ++k2) buf[slot * n + sub + N1 * k2] = w[k2];
     }
     __syncthreads();
     // ---- phase 3: products u x omega, N1-point DFTs (forward) -------------
+    T mu = 0, mv = 0, mw = 0, mox = 0, moy = 0, moz = 0;
+    if constexpr (MEAN) {
+        const int ny2 = d.ny2;
+        mu = (T)mean[j];
+        mv = (T)mean[ny2 + j];
+        mw = (T)mean[2 * ny2 + j];
+        mox = (T)mean[3 * ny2 + j];
+        moy = (T)mean[4 * ny2 + j];
+        moz = (T)mean[5 * ny2 + j];
+    }
     // out lines per row pair (r, r+1): (N0 + i N1)(r), (N0 + i N1)(r+1), N2(r) + i N2(r+1)
     const bool act3 = slot < L2 && sub < N2;
     if (act3) {
@@ -354,33 +373,40 @@ k_x_cross_r(Dims d, const double2 *__restrict__ roots, const double2 *__restrict
 #pragma unroll
         for (int n1 = 0; n1 < N1; ++n1) {
             const int x = sub + N2 * n1;
-            auto prod = [&](int r, double &n0, double &n1v, double &n2v) {
-                const double2 p0 = buf[(3 * r) * n + x];
-                const double2 p1 = buf[(3 * r + 1) * n + x];
-                const double2 p2 = buf[(3 * r + 2) * n + x];
-                const double uu = p0.x, vv = p0.y, ww = p1.x, ox = p1.y, oy = p2.x, oz = p2.y;
+            auto prod = [&](int r, T &n0, T &n1v, T &n2v) {
+                const C p0 = buf[(3 * r) * n + x];
+                const C p1 = buf[(3 * r + 1) * n + x];
+                const C p2 = buf[(3 * r + 2) * n + x];
+                const T uu = p0.x, vv = p0.y, ww = p1.x, ox = p1.y, oy = p2.x, oz = p2.y;
                 n0 = vv * oz - ww * oy;
                 n1v = ww * ox - uu * oz;
                 n2v = uu * oy - vv * ox;
+                if constexpr (MEAN) {
+                    // fluctuations about the FP64 mean profiles: + M x om' + u' x M_om
+                    // (M x M_om is added to the mean mode in FP64 after the analysis)
+                    n0 += (mv * oz - mw * oy) + (vv * moz - ww * moy);
+                    n1v += (mw * ox - mu * oz) + (ww * mox - uu * moz);
+                    n2v += (mu * oy - mv * ox) + (uu * moy - vv * mox);
+                }
             };
-            double a0, a1, a2, b0, b1, b2;
+            T a0, a1, a2, b0, b1, b2;
             if (kind < 2) {
                 prod(2 * pr + kind, a0, a1, a2);
-                v[n1] = mk(a0, a1);
+                v[n1] = mkc<C>(a0, a1);
             } else {
                 prod(2 * pr, a0, a1, a2);
                 prod(2 * pr + 1, b0, b1, b2);
-                v[n1] = mk(a2, b2);
+                v[n1] = mkc<C>(a2, b2);
             }
         }
     }
     __syncthreads();
     if (act3) {
-        double2(&w)[N1] = reinterpret_cast<double2(&)[N1]>(v);
-        dft_reg<N1, -1>(w, s_root, N2);
+        C(&w)[N1] = reinterpret_cast<C(&)[N1]>(v);
+        dft_reg<N1, -1>(w, tw, N2);
 #pragma unroll
         for (int k1 = 0; k1 < N1; ++k1) {
-            const double2 t = (k1 == 0 || sub == 0) ? w[k1] : cmul(w[k1], root_of<-1>(s_root, sub * k1));
+            const C t = (k1 == 0 || sub == 0) ? w[k1] : tw.template mul<-1>(w[k1], sub * k1);
             buf[(slot * N1 + k1) * SP + sub] = t;
         }
     }
@@ -390,36 +416,37 @@ k_x_cross_r(Dims d, const double2 *__restrict__ roots, const double2 *__restrict
     if (act4) {
 #pragma unroll
         for (int n2 = 0; n2 < N2; ++n2) v[n2] = buf[(slot * N1 + sub) * SP + n2];
-        double2(&w)[N2] = reinterpret_cast<double2(&)[N2]>(v);
-        dft_reg<N2, -1>(w, s_root, N1);
+        C(&w)[N2] = reinterpret_cast<C(&)[N2]>(v);
+        dft_reg<N2, -1>(w, tw, N1);
     }
     // partner of frequency k1 + N1 k2 is n - k = k1' + N1 k2' with
     // k1' = (N1 - k1) mod N1, k2' = N2 - 1 - k2 (k1 > 0) or (N2 - k2) mod N2 (k1 = 0)
     const int lane = threadIdx.x & 31;
     const int partner = (lane & 16) + (sub < N1 ? (N1 - sub) % N1 : sub);
     const int pr = slot / 3, kind = slot - (slot / 3) * 3;
-    const double invn = 1.0 / (double)n;
+    // FP32: no 1/NX2 here (not exact in FP32); the FP64 y analysis applies 1/(NX2 NZ2)
+    const T invn = (T)(sizeof(C) == 8 ? 1.0 : 1.0 / (double)n);
 #pragma unroll
     for (int k2 = 0; k2 < N2; ++k2) {
-        double2 pm;
+        C pm;
         pm.x = __shfl_sync(0xffffffffu, v[N2 - 1 - k2].x, partner);
         pm.y = __shfl_sync(0xffffffffu, v[N2 - 1 - k2].y, partner);
         const int k = sub + N1 * k2;
         if (!act4 || k > nxs) continue;
         if (sub == 0) pm = v[(N2 - k2) % N2];
-        const double2 p0 = v[k2];
-        const double2 outA = cscale(invn, mk(0.5 * (p0.x + pm.x), 0.5 * (p0.y - pm.y)));
-        const double2 outB = cscale(invn, mk(0.5 * (p0.y + pm.y), -0.5 * (p0.x - pm.x)));
+        const C p0 = v[k2];
+        const C outA = cscale(invn, mkc<C>(T(0.5) * (p0.x + pm.x), T(0.5) * (p0.y - pm.y)));
+        const C outB = cscale(invn, mkc<C>(T(0.5) * (p0.y + pm.y), T(-0.5) * (p0.x - pm.x)));
         if (kind < 2) {
             const int z = z0 + 2 * pr + kind;
             if (z < d.NZ2) {
-                double2 *h = H + ((long long)j * d.NZ2 + z) * nkx + k;
+                C *h = H + ((long long)j * d.NZ2 + z) * nkx + k;
                 h[0] = outA;            // N0
                 h[fstride] = outB;      // N1
             }
         } else {
             const int z = z0 + 2 * pr;
-            double2 *h = H + 2 * fstride + ((long long)j * d.NZ2 + z) * nkx + k;
+            C *h = H + 2 * fstride + ((long long)j * d.NZ2 + z) * nkx + k;
             if (z < d.NZ2) h[0] = outA;                 // N2 of row r
             if (z + 1 < d.NZ2) h[nkx] = outB;           // N2 of row r+1
         }
@@ -529,10 +556,12 @@ size_t smem_xsingle(const Dims &d) {
     return sizeof(double2) * (size_t)d.NX2 * (1 + 2 * ((kRWs + 1) / 2));
 }
 
-// NX2 = N1 x N2 pairs with a register-form x kernel; others use the Stockham form.
+// NX2 / NZ2 = N1 x N2 with a register form; others use the Stockham form
+// (FP64 only).
 template <typename Fn> bool with_xsplit(int nx2, Fn &&fn) {
     switch (nx2) {
     case 48: fn(std::integral_constant<int, 6>{}, std::integral_constant<int, 8>{}); return true;
+    case 72: fn(std::integral_constant<int, 8>{}, std::integral_constant<int, 9>{}); return true;
     case 96: fn(std::integral_constant<int, 8>{}, std::integral_constant<int, 12>{}); return true;
     case 144: fn(std::integral_constant<int, 12>{}, std::integral_constant<int, 12>{}); return true;
     case 192: fn(std::integral_constant<int, 12>{}, std::integral_constant<int, 16>{}); return true;
@@ -541,30 +570,41 @@ template <typename Fn> bool with_xsplit(int nx2, Fn &&fn) {
     }
 }
 constexpr int kRWr = 4;
-size_t smem_zfft_r(const Dims &d, int n1, int n2) {
-    return sizeof(double2) * ((size_t)n1 * n2 + (size_t)n1 * n2 * z_lines(d));
+size_t smem_zfft_r(const Dims &d, int n1, int n2, size_t elem) {
+    return sizeof(double2) * n1 * n2 + elem * ((size_t)n1 * n2 * z_lines(d));
 }
-size_t smem_xcross_r(int n1, int n2) {
+size_t smem_xcross_r(int n1, int n2, size_t elem) {
     const size_t L = 3 * kRWr;
     const size_t s1 = L * n1 * (n2 + 1), s2 = L * n1 * n2;
-    return sizeof(double2) * ((size_t)n1 * n2 + (s1 > s2 ? s1 : s2));
+    return sizeof(double2) * n1 * n2 + elem * (s1 > s2 ? s1 : s2);
 }
 
-cudaError_t configure_transform_kernels(const Dims &d) {
+template <class C> cudaError_t configure_register_forms(const Dims &d) {
     cudaError_t e = cudaSuccess;
     with_xsplit(d.NX2, [&](auto a, auto b) {
         constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
-        e = cudaFuncSetAttribute(k_x_cross_r<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem_xcross_r(N1, N2));
+        e = cudaFuncSetAttribute(k_x_cross_r<N1, N2, C, sizeof(C) == 8>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xcross_r(N1, N2, sizeof(C)));
     });
     if (e != cudaSuccess) return e;
     with_xsplit(d.NZ2, [&](auto a, auto b) {
         constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
-        const int sm = (int)smem_zfft_r(d, N1, N2);
-        e = cudaFuncSetAttribute(k_z_backward_r<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        const int sm = (int)smem_zfft_r(d, N1, N2, sizeof(C));
+        e = cudaFuncSetAttribute(k_z_backward_r<N1, N2, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
         if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_z_forward_r<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+            e = cudaFuncSetAttribute(k_z_forward_r<N1, N2, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     });
+    return e;
+}
+
+bool register_forms(const Dims &d) {
+    return with_xsplit(d.NX2, [](auto, auto) {}) && with_xsplit(d.NZ2, [](auto, auto) {});
+}
+
+cudaError_t configure_transform_kernels(const Dims &d) {
+    cudaError_t e = configure_register_forms<double2>(d);
+    if (e != cudaSuccess) return e;
+    e = configure_register_forms<float2>(d);
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_z_backward, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem_zfft(d));
@@ -583,38 +623,67 @@ cudaError_t configure_transform_kernels(const Dims &d) {
     return e;
 }
 
-void launch_z_backward(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *F,
-                       double2 *G, int nf, cudaStream_t s) {
+template <class C> bool z_backward_r(const Dims &d, const double2 *roots, const C *F, C *G, int nf, cudaStream_t s) {
     const int tl = z_lines(d);
     dim3 grid((d.nkx + tl - 1) / tl, d.ny2, nf);
-    const bool done = with_xsplit(d.NZ2, [&](auto a, auto b) {
+    return with_xsplit(d.NZ2, [&](auto a, auto b) {
         constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
-        k_z_backward_r<N1, N2><<<grid, (N1 > N2 ? N1 : N2) * tl, smem_zfft_r(d, N1, N2), s>>>(d, roots, F, G, tl);
+        k_z_backward_r<N1, N2, C><<<grid, (N1 > N2 ? N1 : N2) * tl, smem_zfft_r(d, N1, N2, sizeof(C)), s>>>(
+            d, roots, F, G, tl);
     });
-    if (!done) k_z_backward<<<grid, 256, smem_zfft(d), s>>>(d, P, roots, F, G, tl);
+}
+template <class C, bool MEAN>
+bool x_cross_r(const Dims &d, const double2 *roots, const C *G, C *H, const double *mean, cudaStream_t s) {
+    return with_xsplit(d.NX2, [&](auto a, auto b) {
+        constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
+        dim3 grid((d.NZ2 + kRWr - 1) / kRWr, d.ny2);
+        k_x_cross_r<N1, N2, C, MEAN><<<grid, 16 * 3 * kRWr, smem_xcross_r(N1, N2, sizeof(C)), s>>>(
+            d, roots, G, H, kRWr, mean);
+    });
+}
+template <class C> bool z_forward_r(const Dims &d, const double2 *roots, const C *H, C *F, int nf, cudaStream_t s) {
+    const int tl = z_lines(d);
+    dim3 grid((d.nkx + tl - 1) / tl, d.ny2, nf);
+    return with_xsplit(d.NZ2, [&](auto a, auto b) {
+        constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
+        k_z_forward_r<N1, N2, C><<<grid, (N1 > N2 ? N1 : N2) * tl, smem_zfft_r(d, N1, N2, sizeof(C)), s>>>(
+            d, roots, H, F, tl);
+    });
+}
+
+void launch_z_backward(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *F,
+                       double2 *G, int nf, cudaStream_t s) {
+    if (z_backward_r(d, roots, F, G, nf, s)) return;
+    const int tl = z_lines(d);
+    dim3 grid((d.nkx + tl - 1) / tl, d.ny2, nf);
+    k_z_backward<<<grid, 256, smem_zfft(d), s>>>(d, P, roots, F, G, tl);
 }
 
 void launch_x_cross(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G,
                     double2 *H, cudaStream_t s) {
-    const bool done = with_xsplit(d.NX2, [&](auto a, auto b) {
-        constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
-        dim3 grid((d.NZ2 + kRWr - 1) / kRWr, d.ny2);
-        k_x_cross_r<N1, N2><<<grid, 16 * 3 * kRWr, smem_xcross_r(N1, N2), s>>>(d, roots, G, H, kRWr);
-    });
-    if (done) return;
+    if (x_cross_r<double2, false>(d, roots, G, H, nullptr, s)) return;
     dim3 grid((d.NZ2 + kRW - 1) / kRW, d.ny2);
     k_x_cross<<<grid, 256, smem_xcross(d), s>>>(d, P, roots, G, H, kRW);
 }
 
 void launch_z_forward(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *H,
                       double2 *F, int nf, cudaStream_t s) {
+    if (z_forward_r(d, roots, H, F, nf, s)) return;
     const int tl = z_lines(d);
     dim3 grid((d.nkx + tl - 1) / tl, d.ny2, nf);
-    const bool done = with_xsplit(d.NZ2, [&](auto a, auto b) {
-        constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
-        k_z_forward_r<N1, N2><<<grid, (N1 > N2 ? N1 : N2) * tl, smem_zfft_r(d, N1, N2), s>>>(d, roots, H, F, tl);
-    });
-    if (!done) k_z_forward<<<grid, 256, smem_zfft(d), s>>>(d, P, roots, H, F, tl);
+    k_z_forward<<<grid, 256, smem_zfft(d), s>>>(d, P, roots, H, F, tl);
+}
+
+// FP32 stage buffers (mixed precision): register forms only.
+void launch_z_backward(const Dims &d, const double2 *roots, const float2 *F, float2 *G, int nf, cudaStream_t s) {
+    z_backward_r(d, roots, F, G, nf, s);
+}
+void launch_x_cross(const Dims &d, const double2 *roots, const float2 *G, float2 *H, const double *mean,
+                    cudaStream_t s) {
+    x_cross_r<float2, true>(d, roots, G, H, mean, s);
+}
+void launch_z_forward(const Dims &d, const double2 *roots, const float2 *H, float2 *F, int nf, cudaStream_t s) {
+    z_forward_r(d, roots, H, F, nf, s);
 }
 
 void launch_x_c2r(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G,

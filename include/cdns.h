@@ -47,7 +47,13 @@ typedef enum {
     CDNS_ERR_NOMEM = 6        /* device allocation failed */
 } cdns_status;
 
-typedef enum { CDNS_PRECISION_FP64 = 0 } cdns_precision;
+/* Arithmetic of the step.  FP64: everything in double (the drop-in).  MIXED:
+ * the fine-grid stage buffers and the z/x FFTs and products u x omega are
+ * FP32 (the y synthesis/analysis accumulate in FP64 and round to or from FP32
+ * at the stage boundary); the curl, the tau solves, the influence and sigma
+ * corrections, the pressure wall data and the mean-flow update stay FP64.
+ * MIXED needs NX2 and NZ2 in {48, 72, 96, 144, 192, 196}. */
+typedef enum { CDNS_PRECISION_FP64 = 0, CDNS_PRECISION_MIXED = 1 } cdns_precision;
 
 /* Mesh, mirrors MeshParm (src/core/params.hpp:6-11) + XL/ZL
  * (src/core/mesh.hpp:9-37).  Single rank: INDEX_Serial = 1. */

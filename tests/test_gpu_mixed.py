@@ -1,0 +1,99 @@
+"""Mixed-precision step (CDNS_PRECISION_MIXED): FP32 fine-grid stages and FFTs,
+FP64 curl, Chebyshev accumulation, tau solves, corrections and mean flow.
+Compared against the FP64 path of the same library (itself pinned to the
+reference at 1e-10): the nonlinear term to FP32 round-off, time steps to
+relative L2 <= 1e-6 per velocity component at 48^3, and the Re_tau180 bound
+of the precision form: velocity field relative L2 <= 1e-6 after 1000 steps."""
+import numpy as np
+import pytest
+
+import cdns
+from oracle_cases import channel_case, divergence_free_field, orc, retau180_case
+from test_gpu_parity import ODD_RADIX_MESHES, ctx_for, odd_radix_case
+
+pytestmark = pytest.mark.gpu
+
+
+def mixed_ctx_for(m, p):
+    mesh = cdns.Mesh(m.NX, m.NY, m.NZ, m.NXS, m.NYS, m.NZS, m.NX2, m.NY2, m.NZ2, m.XL, m.ZL)
+    params = cdns.Params(Re=p.Re, DT=p.DT, G_pre=p.G_pre, a_pre0=p.a_pre0, b_pre0=p.b_pre0,
+                         a_V=p.a_V, b_V=p.b_V, INDEX_GRAD_PRE=p.INDEX_GRAD_PRE, THETA=p.THETA,
+                         V_Microblow0=p.V_Microblow0)
+    return cdns.Context(mesh, params, precision=cdns.PRECISION_MIXED)
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def run(ctx, u0, nsteps):
+    ctx.set_velocity(np.stack(u0, axis=-1))
+    ctx.run(1, nsteps)
+    ctx.synchronize()
+    return ctx.get_velocity()
+
+
+def test_mixed_nonlinear_term_48():
+    m, p = channel_case(32)
+    u0 = divergence_free_field(m, p, seed=0, amp=0.05, kmax=4)
+    u = np.stack(u0, axis=-1)
+    N64, B64 = ctx_for(m, p).nonlinear(u)
+    N32, B32 = mixed_ctx_for(m, p).nonlinear(u)
+    for k in range(3):
+        assert rel_l2(N32[..., k], N64[..., k]) <= 1e-5
+    # B cancels to round-off here: scale by the N_y endpoint sums it is made of
+    scale = max(np.abs(B64).max(), np.abs(N64[..., 1]).max() * (m.NYS + 1))
+    assert np.abs(B32 - B64).max() <= 1e-5 * scale
+
+
+def test_mixed_stage_buffers_are_fp32_rounded():
+    """The synthesised vorticity of the mixed path is the FP64 one rounded to
+    FP32 (fields 3-5 of the synthesis buffer; 0-2 are reused by the forward z
+    transform), except the (kz, kx) = (0, 0) mean profile, which stays FP64
+    outside the FP32 stages and is zero there."""
+    m, p = channel_case(32)
+    u = np.stack(divergence_free_field(m, p, seed=2, amp=0.05, kmax=4), axis=-1)
+    c64, c32 = ctx_for(m, p), mixed_ctx_for(m, p)
+    c64.nonlinear(u)
+    c32.nonlinear(u)
+    f64 = c64.debug_buffer(0)
+    f32 = c32.debug_buffer(0)
+    expect = f64[3:].astype(np.complex64).astype(np.complex128)
+    expect[:, :, m.NZS, 0] = 0.0
+    assert np.array_equal(f32[3:], expect)
+
+
+def test_mixed_steps_48():
+    m, p = channel_case(32)
+    u0 = divergence_free_field(m, p, seed=0, amp=0.05, kmax=4)
+    v64 = run(ctx_for(m, p), u0, 50)
+    v32 = run(mixed_ctx_for(m, p), u0, 50)
+    for k in range(3):
+        assert rel_l2(v32[..., k], v64[..., k]) <= 1e-6
+
+
+def test_mixed_retau180_1000_steps():
+    """The precision form's bound after 1000 Re_tau180 steps: relative L2 of the
+    velocity field <= 1e-6 against the FP64 path, every component's error below
+    1e-6 of the field norm, and a finite, divergence-free field.  (The
+    per-component relative errors of v and w, whose norms are 10-30x smaller
+    than u's, are a few 1e-6: FP32 FFT arithmetic leaves about 5e-7 relative
+    error in each evaluation of u x omega.)"""
+    m, p = retau180_case()
+    u0 = divergence_free_field(m, p, seed=1, amp=0.1, spectrum="k53", mean="loglaw")
+    v64 = run(ctx_for(m, p), u0, 1000)
+    v32 = run(mixed_ctx_for(m, p), u0, 1000)
+    assert rel_l2(v32, v64) <= 1e-6
+    norm = np.linalg.norm(v64)
+    for k in range(3):
+        assert np.linalg.norm(v32[..., k] - v64[..., k]) <= 1e-6 * norm
+    cst = orc.make_constants(m, p.Re)
+    div = orc.divergence(cst, [v32[..., k] for k in range(3)])
+    assert np.abs(div).max() <= 1e-12 * max(1.0, np.abs(v32).max())
+
+
+@pytest.mark.parametrize("key", sorted(ODD_RADIX_MESHES))
+def test_mixed_rejects_meshes_without_register_form(key):
+    m, p = odd_radix_case(key)
+    with pytest.raises(cdns.CdnsError, match="mixed precision"):
+        mixed_ctx_for(m, p)
