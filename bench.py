@@ -217,6 +217,54 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def ensemble_case(n: int, re: float):
+    """Channel member: N x (N+1) x N base grid, NXS=NZS=N/2, NYS=N-2, 3/2 product
+    grid, 4pi x 2 x 2pi, fixed pressure gradient."""
+    import cdns
+    n2 = 3 * n // 2
+    mesh = cdns.Mesh(n, n, n, n // 2, n - 2, n // 2, n2, n2, n2, 4.0 * math.pi, 2.0 * math.pi)
+    params = cdns.Params(Re=re, DT=5e-5, G_pre=0.0, a_pre0=0.0, b_pre0=1.0, a_V=(1.0, 1.0, 1.0),
+                         b_V=(0.0, 0.0, 0.0), INDEX_GRAD_PRE=1, THETA=0.0, V_Microblow0=0.0)
+    return mesh, params
+
+
+def run_ensemble(members: int, K: int, W: int, precision: int, device: int, seed: int) -> dict:
+    """Ensemble form: `members` channels with N drawn from {32, 48, 64, 96} and
+    Re_tau from U[100, 180] (seeded), laminar profile + 5 % divergence-free
+    perturbation on |k| <= 4; K graph-replayed steady steps after W warm-up
+    steps, timed with CUDA events on the batch stream."""
+    import numpy as np
+    import torch
+    import cdns
+    from cdns.fields import divergence_free_field
+    rng = np.random.default_rng(3)
+    sizes = rng.choice([32, 48, 64, 96], size=members)
+    res = rng.uniform(100.0, 180.0, size=members)
+    cases = [ensemble_case(int(n), float(r)) for n, r in zip(sizes, res)]
+    batch = cdns.Batch([c[0] for c in cases], [c[1] for c in cases], device=device, precision=precision)
+    for i, (ctx, (mesh, params)) in enumerate(zip(batch.members, cases)):
+        u = divergence_free_field(mesh, params, seed=seed + i, amp=0.05, kmax=4)
+        ctx.set_velocity(np.stack(u, axis=-1))
+    batch.run(1, W)
+    batch.synchronize()
+    stream = torch.cuda.ExternalStream(batch.stream_ptr(), device=device)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    batch.run(W + 1, K)
+    e1.record(stream)
+    batch.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    points = int(sum(int(n) * (int(n) + 1) * int(n) for n in sizes))
+    batch.close()
+    return {"members": members, "steps": K, "ms_per_batch_step": ms / K,
+            "grid_points_steps_per_s": points * K / (ms / 1000.0), "grid_points": points,
+            "sizes": {str(n): int((sizes == n).sum()) for n in (32, 48, 64, 96)},
+            "re_tau_range": [float(res.min()), float(res.max())]}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -226,6 +274,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=0, help="steps of the e2e pass (default: min(K, 200))")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed FP32/FP64 arm")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the ensemble-batch arm")
+    ap.add_argument("--ensemble-members", type=int, default=64)
+    ap.add_argument("--ensemble-steps", type=int, default=200)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -339,6 +390,14 @@ def main():
                                "tau solves, corrections and mean flow FP64"}
         cm.close()
 
+    # ---- ensemble arm: independent channels of seeded sizes in one batch ---
+    ensemble = None
+    if not args.no_ensemble:
+        ensemble = {}
+        for label, prec in (("fp64", cdns.PRECISION_FP64), ("mixed", cdns.PRECISION_MIXED)):
+            ensemble[label] = run_ensemble(args.ensemble_members, args.ensemble_steps, W, prec, local,
+                                           1000 + rank)
+
     # ---- end to end through the C ABI with host buffers -------------------
     KE = args.e2e_steps or min(K, 200)
     ctx2 = cdns.Context(mesh, params, device=local)
@@ -397,6 +456,7 @@ def main():
                          "stage_ms": {k: round(v, 5) for k, v in per_launch.items()}},
             "cpu_baseline": cpu,
             "mixed": mixed,
+            "ensemble": ensemble,
             "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": KE, "finite": finite,
                     "protocol": "upload + steps 1..K one call each with dpdx readback + download"},

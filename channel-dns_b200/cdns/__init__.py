@@ -77,6 +77,14 @@ _SIGNATURES = {
                                              ctypes.c_void_p],
     "cdns_last_error": [ctypes.c_char_p, ctypes.c_size_t],
     "cdns_version": [],
+    "cdns_batch_create": [ctypes.c_int, ctypes.POINTER(MeshDesc), ctypes.POINTER(ParamsDesc), ctypes.c_int,
+                          ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)],
+    "cdns_batch_destroy": [ctypes.c_void_p],
+    "cdns_batch_size": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)],
+    "cdns_batch_member": [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)],
+    "cdns_batch_run": [ctypes.c_void_p, ctypes.c_int, ctypes.c_int],
+    "cdns_batch_synchronize": [ctypes.c_void_p],
+    "cdns_batch_stream": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)],
 }
 
 
@@ -206,10 +214,19 @@ class Context:
         _check(lib().cdns_create(ctypes.byref(md), ctypes.byref(pd), precision, device,
                                  ctypes.byref(self._h)))
 
+    _owned = True
+
+    @classmethod
+    def _member(cls, handle: ctypes.c_void_p, mesh: Mesh, params: Params, precision: int) -> "Context":
+        """A view of a batch member (owned and destroyed by its batch)."""
+        c = cls.__new__(cls)
+        c.mesh, c.params, c.precision, c._h, c._owned = mesh, params, precision, handle, False
+        return c
+
     def close(self) -> None:
-        if self._h:
+        if self._h and self._owned:
             lib().cdns_destroy(self._h)
-            self._h = ctypes.c_void_p()
+        self._h = ctypes.c_void_p()
 
     def __del__(self):
         try:
@@ -349,6 +366,53 @@ def fine_backward_noalloc(mesh: Mesh, spectral_ptr: int, physical_ptr: int, stre
     _check(lib().cdns_transform_fine_backward_noalloc(ctypes.byref(md), ctypes.c_void_p(spectral_ptr),
                                                       ctypes.c_void_p(physical_ptr),
                                                       ctypes.c_void_p(stream)))
+
+
+class Batch:
+    """An ensemble of independent channels advanced together (cdns_batch_*):
+    members are full contexts; steady steps replay one graph with every
+    member's step as a parallel branch."""
+
+    def __init__(self, meshes, params, device: int = 0, precision: int = PRECISION_FP64):
+        if len(meshes) != len(params) or not meshes:
+            raise ValueError("one Params per Mesh, at least one member")
+        n = len(meshes)
+        md = (MeshDesc * n)(*[m.desc() for m in meshes])
+        pd = (ParamsDesc * n)(*[p.desc() for p in params])
+        self._h = ctypes.c_void_p()
+        _check(lib().cdns_batch_create(n, md, pd, precision, device, ctypes.byref(self._h)))
+        self.members = []
+        for i in range(n):
+            h = ctypes.c_void_p()
+            _check(lib().cdns_batch_member(self._h, i, ctypes.byref(h)))
+            self.members.append(Context._member(h, meshes[i], params[i], precision))
+
+    def __len__(self) -> int:
+        return len(self.members)
+
+    def run(self, first_iteration: int, nsteps: int) -> None:
+        _check(lib().cdns_batch_run(self._h, first_iteration, nsteps))
+
+    def synchronize(self) -> None:
+        _check(lib().cdns_batch_synchronize(self._h))
+
+    def stream_ptr(self) -> int:
+        s = ctypes.c_void_p()
+        _check(lib().cdns_batch_stream(self._h, ctypes.byref(s)))
+        return s.value
+
+    def close(self) -> None:
+        if self._h:
+            for m in self.members:
+                m._h = ctypes.c_void_p()
+            lib().cdns_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def version() -> str:

@@ -86,6 +86,16 @@ template <> __host__ __device__ inline float2 mkc<float2>(double re, double im) 
 // complex value converted between widths
 template <class C, class S> __device__ inline C cto(S v) { return mkc<C>(v.x, v.y); }
 
+// Raise a kernel's dynamic shared-memory limit to at least `bytes` (never
+// lower it: contexts of different meshes share the kernel attribute).
+template <class K> inline cudaError_t raise_smem(K *kernel, size_t bytes) {
+    cudaFuncAttributes a{};
+    cudaError_t e = cudaFuncGetAttributes(&a, kernel);
+    if (e != cudaSuccess) return e;
+    if ((size_t)a.maxDynamicSharedSizeBytes >= bytes) return cudaSuccess;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
 // Error bits recorded on the device and read by the host after a step.
 enum : unsigned { ERR_NONFINITE = 1u, ERR_PIVOT = 2u };
 

@@ -486,23 +486,20 @@ void launch_cheb_tables(const Dims &d, const double *cosy, double *csyn, double 
 }
 
 cudaError_t configure_cheb_kernels(const Dims &d) {
-    cudaError_t e = cudaFuncSetAttribute(k_ysynth<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)syn_smem(d));
+    cudaError_t e = raise_smem(k_ysynth<double2>, (int)syn_smem(d));
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_ysynth<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)syn_smem(d));
+        e = raise_smem(k_ysynth<float2>, (int)syn_smem(d));
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_yanalysis<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)ana_smem(d, sizeof(double2)));
+        e = raise_smem(k_yanalysis<double2>, (int)ana_smem(d, sizeof(double2)));
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_yanalysis<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)ana_smem(d, sizeof(float2)));
+        e = raise_smem(k_yanalysis<float2>, (int)ana_smem(d, sizeof(float2)));
     if (e != cudaSuccess) return e;
     const int sm = (int)curl_smem(d);
     switch (lane_elems(d)) {
-    case 1: return cudaFuncSetAttribute(k_curl<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    case 2: return cudaFuncSetAttribute(k_curl<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    case 4: return cudaFuncSetAttribute(k_curl<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    case 8: return cudaFuncSetAttribute(k_curl<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    case 1: return raise_smem(k_curl<1>, sm);
+    case 2: return raise_smem(k_curl<2>, sm);
+    case 4: return raise_smem(k_curl<4>, sm);
+    case 8: return raise_smem(k_curl<8>, sm);
     default: return cudaErrorInvalidValue;
     }
 }

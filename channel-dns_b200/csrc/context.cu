@@ -755,6 +755,174 @@ int cdns_last_error(char *buf, size_t len) {
     return CDNS_OK;
 }
 
-const char *cdns_version(void) { return "cdns-b200 0.1 (sm_100a, fp64)"; }
+const char *cdns_version(void) { return "cdns-b200 0.2 (sm_100a, fp64 + mixed fp32/fp64, batch)"; }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Ensemble batch: independent channels (each a full context with its own
+// stream, state and graphs) whose steady steps (it >= 3) are captured into
+// one CUDA graph: a fork event on the batch stream, every member's step body
+// on its own stream as a parallel branch, and a join back to the batch
+// stream.  Steps 1 and 2 (setup) run member by member on the member streams.
+// ---------------------------------------------------------------------------
+struct cdns_batch {
+    int device = 0;
+    std::vector<cdns_ctx *> members;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t fork = nullptr, done = nullptr;
+    std::vector<cudaEvent_t> join;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+};
+
+namespace {
+// batch stream waits for the members' pending work; members wait for the batch
+int batch_order_members_before(cdns_batch *b) {
+    for (size_t i = 0; i < b->members.size(); ++i) {
+        CK(cudaEventRecord(b->join[i], b->members[i]->stream));
+        CK(cudaStreamWaitEvent(b->stream, b->join[i], 0));
+    }
+    return CDNS_OK;
+}
+int batch_order_members_after(cdns_batch *b) {
+    CK(cudaEventRecord(b->done, b->stream));
+    for (cdns_ctx *m : b->members) CK(cudaStreamWaitEvent(m->stream, b->done, 0));
+    return CDNS_OK;
+}
+
+int batch_step(cdns_batch *b, int it) {
+    bool direct = it < 3;
+    for (cdns_ctx *m : b->members) {
+        if (!m->have_velocity) return fail(CDNS_ERR_STATE, "batch step before every member has a velocity");
+        direct = direct || m->prof || m->cur != b->members[0]->cur;
+    }
+    if (direct) {
+        for (cdns_ctx *m : b->members) {
+            int r = one_step(m, it);
+            if (r) return r;
+        }
+        return CDNS_OK;
+    }
+    cudaGraphExec_t &ge = b->graph[b->members[0]->cur];
+    if (!ge) {
+        cudaGraph_t graph;
+        CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        CK(cudaEventRecord(b->fork, b->stream));
+        for (size_t i = 0; i < b->members.size(); ++i) {
+            cdns_ctx *m = b->members[i];
+            double a0, a1, b0, b1, g;
+            step_coefficients(it, m->DT, m->pp.Re, a0, a1, b0, b1, g);
+            CK(cudaStreamWaitEvent(m->stream, b->fork, 0));
+            enqueue_step_body(m, a0, a1, b0, b1, g, false, 0);
+            CK(cudaEventRecord(b->join[i], m->stream));
+            CK(cudaStreamWaitEvent(b->stream, b->join[i], 0));
+        }
+        CK(cudaStreamEndCapture(b->stream, &graph));
+        CK(cudaGraphInstantiate(&ge, graph, 0));
+        CK(cudaGraphDestroy(graph));
+    }
+    int r = batch_order_members_before(b);
+    if (r) return r;
+    CK(cudaGraphLaunch(ge, b->stream));
+    r = batch_order_members_after(b);
+    if (r) return r;
+    for (cdns_ctx *m : b->members) m->cur = 1 - m->cur;
+    return CDNS_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int cdns_batch_create(int n, const cdns_mesh_desc *meshes, const cdns_params *params, int precision, int device,
+                      cdns_batch **out) {
+    if (!out || n <= 0 || !meshes || !params) return fail(CDNS_ERR_ARG, "bad batch arguments");
+    *out = nullptr;
+    cdns_batch *b = new (std::nothrow) cdns_batch();
+    if (!b) return fail(CDNS_ERR_NOMEM, "host allocation failed");
+    b->device = device;
+    auto bail = [&](int code) { cdns_batch_destroy(b); return code; };
+    for (int i = 0; i < n; ++i) {
+        cdns_ctx *m = nullptr;
+        int r = cdns_create(&meshes[i], &params[i], precision, device, &m);
+        if (r) return bail(r);
+        b->members.push_back(m);
+    }
+    DeviceGuard guard(device);
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) != cudaSuccess)
+        return bail(fail(CDNS_ERR_CUDA, "batch stream/event creation failed"));
+    b->join.resize(n, nullptr);
+    for (auto &e : b->join)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+            return bail(fail(CDNS_ERR_CUDA, "batch event creation failed"));
+    *out = b;
+    return CDNS_OK;
+}
+
+int cdns_batch_destroy(cdns_batch *b) {
+    if (!b) return CDNS_OK;
+    {
+        DeviceGuard guard(b->device);
+        if (b->stream) cudaStreamSynchronize(b->stream);
+        for (auto &g : b->graph)
+            if (g) cudaGraphExecDestroy(g);
+        for (auto e : b->join)
+            if (e) cudaEventDestroy(e);
+        if (b->fork) cudaEventDestroy(b->fork);
+        if (b->done) cudaEventDestroy(b->done);
+        if (b->stream) cudaStreamDestroy(b->stream);
+    }
+    for (cdns_ctx *m : b->members) cdns_destroy(m);
+    delete b;
+    return CDNS_OK;
+}
+
+int cdns_batch_size(cdns_batch *b, int *n) {
+    if (!b || !n) return fail(CDNS_ERR_ARG, "null argument");
+    *n = (int)b->members.size();
+    return CDNS_OK;
+}
+
+int cdns_batch_member(cdns_batch *b, int i, cdns_ctx **ctx) {
+    if (!b || !ctx) return fail(CDNS_ERR_ARG, "null argument");
+    if (i < 0 || i >= (int)b->members.size()) return fail(CDNS_ERR_ARG, "member index out of range");
+    *ctx = b->members[i];
+    return CDNS_OK;
+}
+
+int cdns_batch_run(cdns_batch *b, int first, int nsteps) {
+    if (!b) return fail(CDNS_ERR_ARG, "null batch");
+    if (nsteps < 0 || first < 1) return fail(CDNS_ERR_ARG, "bad iteration range");
+    DeviceGuard guard(b->device);
+    for (int i = 0; i < nsteps; ++i) {
+        int r = batch_step(b, first + i);
+        if (r) return r;
+    }
+    return CDNS_OK;
+}
+
+int cdns_batch_synchronize(cdns_batch *b) {
+    if (!b) return fail(CDNS_ERR_ARG, "null batch");
+    DeviceGuard guard(b->device);
+    CK(cudaStreamSynchronize(b->stream));
+    int first_error = CDNS_OK;
+    std::string msg;
+    for (size_t i = 0; i < b->members.size(); ++i) {
+        int r = cdns_synchronize(b->members[i]);
+        if (r && !first_error) {
+            first_error = r;
+            msg = "member " + std::to_string(i) + ": " + g_error;
+        }
+    }
+    if (first_error) return fail(first_error, msg);
+    return CDNS_OK;
+}
+
+int cdns_batch_stream(cdns_batch *b, void **stream) {
+    if (!b || !stream) return fail(CDNS_ERR_ARG, "null argument");
+    *stream = (void *)b->stream;
+    return CDNS_OK;
+}
 
 }  // extern "C"

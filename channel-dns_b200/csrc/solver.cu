@@ -437,7 +437,7 @@ __global__ void k_pressure_bc(Dims d, const double2 *N, const double2 *bw, doubl
 
 template <int E>
 cudaError_t configure_e(const Dims &d) {
-    return cudaFuncSetAttribute(k_solve<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem(d));
+    return raise_smem(k_solve<E>, (int)solve_smem(d));
 }
 
 template <int E>

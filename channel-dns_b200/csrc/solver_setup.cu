@@ -329,9 +329,9 @@ __global__ void k_unit_response(Dims d, Tables t, PhysParams pp, double g_v, con
 
 cudaError_t configure_setup_kernels(const Dims &d) {
     const int sm = (int)setup_smem(d);
-    cudaError_t e = cudaFuncSetAttribute(k_setup_solve<MODE_BASE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaError_t e = raise_smem(k_setup_solve<MODE_BASE>, sm);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_setup_solve<MODE_COUPLED>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    return raise_smem(k_setup_solve<MODE_COUPLED>, sm);
 }
 
 void setup_solver(const Dims &d, const Tables &t, const PhysParams &pp, double g_v, SolverState &st,

@@ -583,16 +583,15 @@ template <class C> cudaError_t configure_register_forms(const Dims &d) {
     cudaError_t e = cudaSuccess;
     with_xsplit(d.NX2, [&](auto a, auto b) {
         constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
-        e = cudaFuncSetAttribute(k_x_cross_r<N1, N2, C, sizeof(C) == 8>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_xcross_r(N1, N2, sizeof(C)));
+        e = raise_smem(k_x_cross_r<N1, N2, C, sizeof(C) == 8>, smem_xcross_r(N1, N2, sizeof(C)));
     });
     if (e != cudaSuccess) return e;
     with_xsplit(d.NZ2, [&](auto a, auto b) {
         constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
         const int sm = (int)smem_zfft_r(d, N1, N2, sizeof(C));
-        e = cudaFuncSetAttribute(k_z_backward_r<N1, N2, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        e = raise_smem(k_z_backward_r<N1, N2, C>, sm);
         if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_z_forward_r<N1, N2, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+            e = raise_smem(k_z_forward_r<N1, N2, C>, sm);
     });
     return e;
 }
@@ -606,20 +605,15 @@ cudaError_t configure_transform_kernels(const Dims &d) {
     if (e != cudaSuccess) return e;
     e = configure_register_forms<float2>(d);
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_z_backward, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem_zfft(d));
+    e = raise_smem(k_z_backward, (int)smem_zfft(d));
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_z_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem_zfft(d));
+    e = raise_smem(k_z_forward, (int)smem_zfft(d));
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_x_cross, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem_xcross(d));
+    e = raise_smem(k_x_cross, (int)smem_xcross(d));
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_x_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem_xsingle(d));
+    e = raise_smem(k_x_c2r, (int)smem_xsingle(d));
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_x_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem_xsingle(d));
+    e = raise_smem(k_x_r2c, (int)smem_xsingle(d));
     return e;
 }
 

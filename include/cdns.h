@@ -189,6 +189,26 @@ int cdns_last_error(char *buf, size_t len);
 /* Library version string. */
 const char *cdns_version(void);
 
+/* Ensemble batch: n independent channels (meshes and params may differ, one
+ * precision mode) on one device.  No reference counterpart (the reference
+ * runs one channel per process); each member is a full context whose state
+ * is set and read with the single-channel calls on cdns_batch_member.
+ * cdns_batch_run advances every member from `first_iteration`: steps 1-2 run
+ * member by member, steady steps replay one CUDA graph holding every
+ * member's step as a parallel branch.  All members must be at the same
+ * iteration (set their velocities before the first run). */
+typedef struct cdns_batch cdns_batch;
+int cdns_batch_create(int n, const cdns_mesh_desc *meshes, const cdns_params *params, int precision,
+                      int device, cdns_batch **out);
+int cdns_batch_destroy(cdns_batch *batch);
+int cdns_batch_size(cdns_batch *batch, int *n);
+int cdns_batch_member(cdns_batch *batch, int i, cdns_ctx **ctx);
+int cdns_batch_run(cdns_batch *batch, int first_iteration, int nsteps);
+/* Waits for every member and reports the first member error (with its index). */
+int cdns_batch_synchronize(cdns_batch *batch);
+/* The batch's CUDA stream (a cudaStream_t): steady steps are launched on it. */
+int cdns_batch_stream(cdns_batch *batch, void **stream);
+
 #ifdef __cplusplus
 }
 #endif
