@@ -77,6 +77,12 @@ _SIGNATURES = {
                                              ctypes.c_void_p],
     "cdns_last_error": [ctypes.c_char_p, ctypes.c_size_t],
     "cdns_version": [],
+    "cdns_adjoint_run": [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+    "cdns_solve_adjoint": [ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                           ctypes.c_void_p, ctypes.c_void_p],
+    "cdns_nonlinear_adjoint": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                               ctypes.c_void_p],
     "cdns_batch_create": [ctypes.c_int, ctypes.POINTER(MeshDesc), ctypes.POINTER(ParamsDesc), ctypes.c_int,
                           ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)],
     "cdns_batch_destroy": [ctypes.c_void_p],
@@ -200,6 +206,8 @@ def _ptr(a: np.ndarray) -> ctypes.c_void_p:
 # cdns_precision (include/cdns.h)
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
+OBJECTIVE_WALL_SHEAR = 0
+OBJECTIVE_PROJECTION = 1
 
 
 class Context:
@@ -315,6 +323,53 @@ class Context:
         _check(lib().cdns_solve(self._h, g, _ptr(rhs), _ptr(pbc), _ptr(vbc), _ptr(p), _ptr(v),
                                 _ptr(units)))
         return p, v, units[:ncy].copy(), units[ncy:].copy()
+
+    # ---- discrete adjoint ----
+    def adjoint_run(self, nsteps: int, checkpoint_interval: int, control: Optional[np.ndarray] = None,
+                    gradient: bool = True, weights: Optional[np.ndarray] = None):
+        """Objective over iterations 1..nsteps from the current velocity and,
+        with gradient=True, its gradients with respect to the initial velocity
+        [nkz][ncy][nkx][3] and the velocity wall data [nkz][2][nkx][3]
+        (d/dRe + i d/dIm of every stored coefficient).  The objective is the
+        time-averaged wall shear stress, or Re <weights, u^nsteps> when
+        weights (velocity layout) are given.  Returns (J, gu, gbc)."""
+        nkz, ncy, nkx = self.mesh.spectral_shape
+        ctl = None if control is None else np.ascontiguousarray(control, dtype=np.complex128)
+        wts = None if weights is None else np.ascontiguousarray(weights, dtype=np.complex128)
+        objective = OBJECTIVE_WALL_SHEAR if wts is None else OBJECTIVE_PROJECTION
+        J = np.zeros(1)
+        gu = np.empty((nkz, ncy, nkx, 3), dtype=np.complex128) if gradient else None
+        gb = np.empty((nkz, 2, nkx, 3), dtype=np.complex128) if gradient else None
+        _check(lib().cdns_adjoint_run(self._h, nsteps, checkpoint_interval, objective,
+                                      None if wts is None else _ptr(wts), None if ctl is None else _ptr(ctl),
+                                      _ptr(J), None if gu is None else _ptr(gu),
+                                      None if gb is None else _ptr(gb)))
+        return float(J[0]), gu, gb
+
+    def solve_adjoint(self, g: float, pressure_adj: Optional[np.ndarray], velocity_adj: np.ndarray):
+        """Transpose of solve(): adjoints of (pressure, velocity) -> adjoints
+        of (rhs, pressure_bc, velocity_bc)."""
+        nkz, ncy, nkx = self.mesh.spectral_shape
+        lp = None if pressure_adj is None else np.ascontiguousarray(pressure_adj, dtype=np.complex128)
+        lv = np.ascontiguousarray(velocity_adj, dtype=np.complex128)
+        lr = np.empty((nkz, ncy, nkx, 3), dtype=np.complex128)
+        lpb = np.empty((nkz, 2, nkx), dtype=np.complex128)
+        lvb = np.empty((nkz, 2, nkx, 3), dtype=np.complex128)
+        _check(lib().cdns_solve_adjoint(self._h, g, None if lp is None else _ptr(lp), _ptr(lv), _ptr(lr),
+                                        _ptr(lpb), _ptr(lvb)))
+        return lr, lpb, lvb
+
+    def nonlinear_adjoint(self, u: np.ndarray, nonlinear_adj: np.ndarray,
+                          pressure_bc_adj: Optional[np.ndarray] = None) -> np.ndarray:
+        """Transpose of the linearisation of nonlinear() about u."""
+        nkz, ncy, nkx = self.mesh.spectral_shape
+        u = np.ascontiguousarray(u, dtype=np.complex128)
+        ln = np.ascontiguousarray(nonlinear_adj, dtype=np.complex128)
+        lb = None if pressure_bc_adj is None else np.ascontiguousarray(pressure_bc_adj, dtype=np.complex128)
+        lu = np.empty((nkz, ncy, nkx, 3), dtype=np.complex128)
+        _check(lib().cdns_nonlinear_adjoint(self._h, _ptr(u), _ptr(ln), None if lb is None else _ptr(lb),
+                                            _ptr(lu)))
+        return lu
 
     # ---- per-stage timing ----
     def profile_begin(self) -> None:

@@ -25,6 +25,13 @@ void launch_ysynth(const Dims &d, const Tables &t, const double2 *src0, const do
                    int nf, float2 *F, double *mean, cudaStream_t s);
 void launch_mean_products(const Dims &d, const Tables &t, const double *mean, double2 *S, cudaStream_t s);
 void launch_yanalysis(const Dims &d, const Tables &t, const float2 *F, double2 *S, int nf, cudaStream_t s);
+// Discrete adjoint: tables of the transposed analysis (synthesis layout) and
+// transposed synthesis (analysis layout); analysis with a custom table and
+// one output scale for every coefficient.
+void launch_cheb_tables_adjoint(const Dims &d, const double *cosy, double *csyn_t, double *cana_t,
+                                cudaStream_t s);
+void launch_yanalysis_scaled(const Dims &d, const double *cana, const double2 *F, double2 *S, int nf,
+                             double scale, cudaStream_t s);
 
 // ---- transforms.cu ----
 cudaError_t configure_transform_kernels(const Dims &d);
@@ -45,6 +52,9 @@ void launch_x_cross(const Dims &d, const double2 *roots, const float2 *G, float2
 void launch_z_forward(const Dims &d, const double2 *roots, const float2 *H, float2 *F, int nf, cudaStream_t s);
 void launch_x_r2c(const Dims &d, const FftPlan &P, const double2 *roots, const double *phys,
                   double2 *H, cudaStream_t s);
+// Transpose of x_cross about the forward fields G[6]: L[0..2] = lH in, L[0..5] = lG out.
+void launch_x_adjoint(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G, double2 *L,
+                      cudaStream_t s);
 
 // ---- solver.cu ----
 // Precomputed solver state (EqSolvePV members, src/solver/eqsolve_pv.hpp:60-76).
@@ -95,6 +105,24 @@ cudaError_t configure_solver_kernels(const Dims &d);
 // Pressure wall data of a standalone nonlinear evaluation: B = bw + endpoint sums of N_y.
 void launch_pressure_bc(const Dims &d, const double2 *N, const double2 *bw, double2 *B,
                         cudaStream_t s);
+
+// ---- adjoint.cu ----
+cudaError_t configure_adjoint_kernels(const Dims &d);
+// Transpose of the column solve: lp (may be null) and lv[3][Ns] of the
+// solution -> lR[3][Ns], lBc[2][ncol] (pressure wall data), lbcv[3][2][ncol]
+// += (velocity wall data).  solve_only = 0 adds the zero-mode overwrite and
+// the wall-shear seed.
+void launch_solve_adjoint(const Dims &d, const Tables &t, const PhysParams &pp, double g_v, const SolverState &st,
+                          const double2 *lp, const double2 *lv, double2 *lR, double2 *lBc, double2 *lbcv,
+                          int solve_only, double seed, cudaStream_t s);
+// lu[3][Ns] += lS[0..2] + curl^T(lS[3..5], lbw[2][ncol]) (lbw may be null)
+void launch_curl_adjoint(const Dims &d, const Tables &t, const double2 *lS, const double2 *lbw, double2 *lu,
+                         double re, cudaStream_t s);
+void launch_adjoint_accumulate(const Dims &d, const double2 *lR, const double2 *lBc, double a0, double a1,
+                               double b0, double b1, double2 *lu1, double2 *lu2, double2 *lN1, double2 *lN2,
+                               const double2 *lB1, double2 *lbw, double2 *lB2, cudaStream_t s);
+void launch_pressure_bc_adjoint(const Dims &d, const double2 *lB, double2 *lN, cudaStream_t s);
+void launch_wall_shear(const Dims &d, const double2 *u, double re, double *out, cudaStream_t s);
 
 // ---- context.cu ----
 int record_error(int code, const char *msg);

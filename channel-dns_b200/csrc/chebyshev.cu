@@ -68,6 +68,35 @@ __global__ void k_cheb_tables(Dims d, const double *__restrict__ cosy, double *c
     }
 }
 
+// Tables of the transposed Chebyshev stages (discrete adjoint), in the
+// layouts of csyn and cana so that the synthesis kernel applies the
+// transposed analysis and the analysis kernel the transposed synthesis:
+//   csyn_t[k][j]    = s_k v_j cos(pi j k / N) * xs    (v_j, s_k of the analysis;
+//                     xs = 1/(NX2 NZ2), the transposed x and z scalings)
+//   cana_t[j][p][m] = cos(pi j k / N), k = 2m + p     (synthesis weights w_k = 1)
+__global__ void k_cheb_tables_adjoint(Dims d, const double *__restrict__ cosy, double *csyn_t, int jp,
+                                      double *cana_t, int kh, double xs) {
+    const int N = d.NY2, twoN = 2 * N;
+    const long long nsyn = (long long)d.ncy * jp;
+    const long long nana = (long long)d.nyh * 2 * kh;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nsyn + nana;
+         i += (long long)gridDim.x * blockDim.x) {
+        if (i < nsyn) {
+            const int k = (int)(i / jp), j = (int)(i - (i / jp) * jp);
+            const double sk = k == 0 ? 1.0 / (2.0 * N) : 1.0 / (double)N;
+            const double vj = j == 0 ? 1.0 : 2.0;
+            csyn_t[i] = (j < d.nyh) ? cosy[((long long)j * k) % twoN] * (sk * vj * xs) : 0.0;
+        } else {
+            const long long q = i - nsyn;
+            const int j = (int)(q / (2 * kh));
+            const int r = (int)(q - (long long)j * 2 * kh);
+            const int p = r / kh, m = r - (r / kh) * kh;
+            const int k = 2 * m + p;
+            cana_t[q] = (k < d.ncy) ? cosy[((long long)j * k) % twoN] : 0.0;
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Spectral curl, warp per column (src/solver/vector_ops.cpp:112-151):
 //   om_x = dw/dy - i kz v,  om_y = i kz u - i kx w,  om_z = i kx v - du/dy,
@@ -312,7 +341,7 @@ __host__ __device__ constexpr int ana_x_slots(int xs, int elem) {
 template <class CI>
 __global__ void __launch_bounds__(32 * 2 * kMaxGroups)
 k_yanalysis(Dims d, const double *__restrict__ cana, int kh, const CI *__restrict__ F,
-            double2 *__restrict__ S) {
+            double2 *__restrict__ S, double s0, double sn) {
     // staged complex row of 32 columns: 34 slots for FP64, 36 for FP32 (16-byte units)
     constexpr bool F32 = sizeof(CI) == 8;
     constexpr int XS = F32 ? 36 : kXS;
@@ -402,9 +431,6 @@ k_yanalysis(Dims d, const double *__restrict__ cana, int kh, const CI *__restric
     }
     cp_async_wait<0>();
     double2 *Sf = S + (long long)f * d.Ns;
-    // FP32 stage buffers arrive without the 1/(NX2 NZ2) of the x and z analyses
-    const double sxz = F32 ? 1.0 / ((double)d.NX2 * (double)d.NZ2) : 1.0;
-    const double sn = sxz / (double)N, s0 = sxz / (2.0 * N);
 #pragma unroll
     for (int mr = 0; mr < 2; ++mr) {
         const int k = 2 * (m0 + 8 * mr + g) + par;
@@ -485,6 +511,17 @@ void launch_cheb_tables(const Dims &d, const double *cosy, double *csyn, double 
                                          ana_groups(d) * kAnaRows);
 }
 
+void launch_cheb_tables_adjoint(const Dims &d, const double *cosy, double *csyn_t, double *cana_t,
+                                cudaStream_t s) {
+    size_t ns, na;
+    cheb_table_sizes(d, &ns, &na);
+    const long long n = (long long)(ns + na);
+    const int blocks = (int)std::min<long long>((n + 255) / 256, 4096);
+    k_cheb_tables_adjoint<<<blocks, 256, 0, s>>>(d, cosy, csyn_t, syn_groups(d) * kSynRows, cana_t,
+                                                 ana_groups(d) * kAnaRows,
+                                                 1.0 / ((double)d.NX2 * (double)d.NZ2));
+}
+
 cudaError_t configure_cheb_kernels(const Dims &d) {
     cudaError_t e = raise_smem(k_ysynth<double2>, (int)syn_smem(d));
     if (e == cudaSuccess)
@@ -535,17 +572,30 @@ void launch_ysynth(const Dims &d, const Tables &t, const double2 *src0, const do
 }
 
 template <class CI>
-void yanalysis(const Dims &d, const Tables &t, const CI *F, double2 *S, int nf, cudaStream_t s) {
+void yanalysis(const Dims &d, const double *cana, const CI *F, double2 *S, int nf, double s0, double sn,
+               cudaStream_t s) {
     const int g = ana_groups(d);
     dim3 block(32, 2 * std::min(g, kMaxGroups));
     dim3 grid((d.ncol + 31) / 32, nf, (g + kMaxGroups - 1) / kMaxGroups);
-    k_yanalysis<CI><<<grid, block, ana_smem(d, sizeof(CI)), s>>>(d, t.cana, g * kAnaRows, F, S);
+    k_yanalysis<CI><<<grid, block, ana_smem(d, sizeof(CI)), s>>>(d, cana, g * kAnaRows, F, S, s0, sn);
+}
+// Output scales of the analysis: s_0 = 1/(2N), s_k = 1/N; FP32 stage buffers
+// arrive without the 1/(NX2 NZ2) of the x and z analyses.
+template <class CI>
+void yanalysis(const Dims &d, const Tables &t, const CI *F, double2 *S, int nf, cudaStream_t s) {
+    const double sxz = sizeof(CI) == 8 ? 1.0 / ((double)d.NX2 * (double)d.NZ2) : 1.0;
+    yanalysis(d, t.cana, F, S, nf, sxz / (2.0 * d.NY2), sxz / (double)d.NY2, s);
 }
 void launch_yanalysis(const Dims &d, const Tables &t, const double2 *F, double2 *S, int nf, cudaStream_t s) {
     yanalysis(d, t, F, S, nf, s);
 }
 void launch_yanalysis(const Dims &d, const Tables &t, const float2 *F, double2 *S, int nf, cudaStream_t s) {
     yanalysis(d, t, F, S, nf, s);
+}
+
+void launch_yanalysis_scaled(const Dims &d, const double *cana, const double2 *F, double2 *S, int nf,
+                             double scale, cudaStream_t s) {
+    yanalysis(d, cana, F, S, nf, scale, scale, s);
 }
 
 void launch_mean_products(const Dims &d, const Tables &t, const double *mean, double2 *S, cudaStream_t s) {

@@ -10,20 +10,20 @@
 #include <vector>
 
 #include "../../include/cdns.h"
-#include "cdns_kernels.cuh"
+#include "context.cuh"
 
 using namespace cdns;
 
 namespace {
 thread_local std::string g_error;
+}  // namespace
 
+namespace cdns {
 int fail(int code, const std::string &msg) {
     g_error = msg;
     return code;
 }
-}  // namespace
 
-namespace cdns {
 // Records the calling thread's last error for cdns_last_error (used by
 // entry points defined in other translation units).
 int record_error(int code, const char *msg) {
@@ -34,17 +34,8 @@ int record_error(int code, const char *msg) {
 
 namespace {
 
-#define CK(call)                                                                          \
-    do {                                                                                  \
-        cudaError_t e_ = (call);                                                          \
-        if (e_ != cudaSuccess)                                                            \
-            return fail(CDNS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
-    } while (0)
-
-constexpr int kStages = 7;
 const char *kStageNames[kStages] = {"curl", "y_synthesis", "z_backward", "x_cross",
                                     "z_forward", "y_analysis", "solve"};
-constexpr int kMaxProfSteps = 256;
 
 bool plan_fft(int n, FftPlan &p) {
     p.n = n;
@@ -67,53 +58,6 @@ bool plan_fft(int n, FftPlan &p) {
 }
 }  // namespace
 
-struct cdns_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    Dims d{};
-    Tables t{};
-    FftPlan px{}, pz{};
-    PhysParams pp{};
-    double DT = 0.0;
-    std::vector<void *> allocs;
-    size_t bytes = 0;
-    // state (component planar)
-    double2 *U[2] = {nullptr, nullptr};   // velocity / previous velocity
-    double2 *Nb[2] = {nullptr, nullptr};  // nonlinear term, current / previous
-    double2 *Bb[2] = {nullptr, nullptr};  // pressure wall data, current / previous
-    int cur = 0;                          // U[cur] = u, Nb[cur] = next N, Bb[cur] = next B
-    double2 *p = nullptr, *bw = nullptr, *bc_v = nullptr, *bc_p = nullptr;
-    double2 *F = nullptr, *G = nullptr, *H = nullptr, *aux = nullptr, *aux2 = nullptr, *zero3 = nullptr;
-    double2 *om = nullptr;                // vorticity of the velocity being transformed
-    bool mixed = false;                   // FP32 fine-grid stages (CDNS_PRECISION_MIXED)
-    double *mean = nullptr;               // mixed: FP64 (kz, kx) = (0, 0) profiles [6][NY2+1]
-    double *phys = nullptr;
-    double *dpdx = nullptr;
-    unsigned *err = nullptr;
-    SolverState st{};
-    double g_setup = NAN;
-    bool have_velocity = false;
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    bool prof = false;
-    int prof_steps = 0;
-    std::vector<cudaEvent_t> ev;
-
-    template <typename T> int alloc(T *&ptr, size_t count) {
-        void *p = nullptr;
-        const size_t b = sizeof(T) * (count ? count : 1);
-        cudaError_t e = cudaMalloc(&p, b);
-        if (e != cudaSuccess) return fail(CDNS_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-        // Zero on the context stream: a cudaMemset on the legacy default stream
-        // is not ordered against this non-blocking stream and could land after
-        // the kernels that fill the buffer.
-        e = cudaMemsetAsync(p, 0, b, stream);
-        if (e != cudaSuccess) return fail(CDNS_ERR_CUDA, cudaGetErrorString(e));
-        allocs.push_back(p);
-        bytes += b;
-        ptr = static_cast<T *>(p);
-        return CDNS_OK;
-    }
-};
 
 namespace {
 int upload(cdns_ctx *c, void *dst, const void *src, size_t b) {
@@ -121,6 +65,9 @@ int upload(cdns_ctx *c, void *dst, const void *src, size_t b) {
     return CDNS_OK;
 }
 
+}  // namespace
+
+namespace cdns {
 void step_coefficients(int it, double dt, double re, double &a0, double &a1, double &b0, double &b1,
                        double &g) {
     // src/sim/simulation.cpp:36-45
@@ -132,8 +79,7 @@ void step_coefficients(int it, double dt, double re, double &a0, double &a1, dou
     g = (a0 + a1) * re;
 }
 
-// Nonlinear stages K1..K5a: u -> N (planar spectral), bw.
-void enqueue_nonlinear(cdns_ctx *c, const double2 *u, double2 *N, bool prof, int step_slot) {
+void enqueue_nonlinear(cdns_ctx *c, const double2 *u, double2 *N, bool prof, int step_slot, double2 *G_fp64) {
     const Dims &d = c->d;
     cudaStream_t s = c->stream;
     auto mark = [&](int stage) {
@@ -158,11 +104,12 @@ void enqueue_nonlinear(cdns_ctx *c, const double2 *u, double2 *N, bool prof, int
         mark(6);
         return;
     }
+    double2 *G = G_fp64 ? G_fp64 : c->G;
     launch_ysynth(d, c->t, u, c->om, 3, 6, c->F, s);
     mark(2);
-    launch_z_backward(d, c->pz, c->t.root_z, c->F, c->G, 6, s);
+    launch_z_backward(d, c->pz, c->t.root_z, c->F, G, 6, s);
     mark(3);
-    launch_x_cross(d, c->px, c->t.root_x, c->G, c->H, s);
+    launch_x_cross(d, c->px, c->t.root_x, G, c->H, s);
     mark(4);
     launch_z_forward(d, c->pz, c->t.root_z, c->H, c->F, 3, s);
     mark(5);
@@ -170,6 +117,9 @@ void enqueue_nonlinear(cdns_ctx *c, const double2 *u, double2 *N, bool prof, int
     mark(6);
 }
 
+}  // namespace cdns
+
+namespace {
 void enqueue_step_body(cdns_ctx *c, double a0, double a1, double b0, double b1, double g_v,
                        bool prof, int slot) {
     const int k = c->cur;
@@ -195,6 +145,9 @@ void enqueue_step_body(cdns_ctx *c, double a0, double a1, double b0, double b1, 
     if (prof) cudaEventRecord(c->ev[(size_t)slot * (kStages + 1) + kStages], c->stream);
 }
 
+}  // namespace
+
+namespace cdns {
 int do_setup(cdns_ctx *c, double g_v) {
     if (c->g_setup == g_v) return CDNS_OK;  // deterministic: same g gives the same state
     setup_solver(c->d, c->t, c->pp, g_v, c->st, nullptr, c->stream);
@@ -203,6 +156,9 @@ int do_setup(cdns_ctx *c, double g_v) {
     return CDNS_OK;
 }
 
+}  // namespace cdns
+
+namespace {
 int one_step(cdns_ctx *c, int it) {
     if (!c->have_velocity) return fail(CDNS_ERR_STATE, "cdns_step before cdns_set_velocity");
     if (it < 1) return fail(CDNS_ERR_ARG, "iteration must be >= 1");
@@ -238,16 +194,6 @@ int one_step(cdns_ctx *c, int it) {
     return CDNS_OK;
 }
 
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int dev) {
-        cudaGetDevice(&prev);
-        if (prev != dev) cudaSetDevice(dev);
-    }
-    ~DeviceGuard() {
-        if (prev >= 0) cudaSetDevice(prev);
-    }
-};
 }  // namespace
 
 extern "C" {
@@ -418,6 +364,7 @@ int cdns_destroy(cdns_ctx *c) {
     for (auto &g : c->graph)
         if (g) cudaGraphExecDestroy(g);
     for (auto ev : c->ev) cudaEventDestroy(ev);
+    adjoint_release(c->adj);
     for (void *p : c->allocs) cudaFree(p);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -745,7 +692,7 @@ int cdns_get_stream(cdns_ctx *c, void **stream) {
 
 int cdns_device_bytes(cdns_ctx *c, size_t *b) {
     if (!c || !b) return fail(CDNS_ERR_ARG, "null argument");
-    *b = c->bytes;
+    *b = c->bytes + adjoint_bytes(c->adj);
     return CDNS_OK;
 }
 
@@ -755,7 +702,7 @@ int cdns_last_error(char *buf, size_t len) {
     return CDNS_OK;
 }
 
-const char *cdns_version(void) { return "cdns-b200 0.2 (sm_100a, fp64 + mixed fp32/fp64, batch)"; }
+const char *cdns_version(void) { return "cdns-b200 0.3 (sm_100a, fp64 + mixed fp32/fp64, batch, discrete adjoint)"; }
 
 }  // extern "C"
 

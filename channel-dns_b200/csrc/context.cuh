@@ -1,0 +1,108 @@
+// Internal view of a cdns context, shared by the translation units that
+// orchestrate the forward step (context.cu) and its discrete adjoint
+// (adjoint_run.cu).  Not part of the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/cdns.h"
+#include "cdns_kernels.cuh"
+
+namespace cdns {
+
+// Records msg as the calling thread's last error (cdns_last_error) and returns code.
+int fail(int code, const std::string &msg);
+
+constexpr int kStages = 7;
+constexpr int kMaxProfSteps = 256;
+
+struct AdjointWork;   // adjoint_run.cu
+void adjoint_release(AdjointWork *w);
+size_t adjoint_bytes(const AdjointWork *w);
+
+}  // namespace cdns
+
+#define CK(call)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            return ::cdns::fail(CDNS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+struct cdns_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cdns::Dims d{};
+    cdns::Tables t{};
+    cdns::FftPlan px{}, pz{};
+    cdns::PhysParams pp{};
+    double DT = 0.0;
+    std::vector<void *> allocs;
+    size_t bytes = 0;
+    // state (component planar)
+    double2 *U[2] = {nullptr, nullptr};   // velocity / previous velocity
+    double2 *Nb[2] = {nullptr, nullptr};  // nonlinear term, current / previous
+    double2 *Bb[2] = {nullptr, nullptr};  // pressure wall data, current / previous
+    int cur = 0;                          // U[cur] = u, Nb[cur] = next N, Bb[cur] = next B
+    double2 *p = nullptr, *bw = nullptr, *bc_v = nullptr, *bc_p = nullptr;
+    double2 *F = nullptr, *G = nullptr, *H = nullptr, *aux = nullptr, *aux2 = nullptr, *zero3 = nullptr;
+    double2 *om = nullptr;                // vorticity of the velocity being transformed
+    bool mixed = false;                   // FP32 fine-grid stages (CDNS_PRECISION_MIXED)
+    double *mean = nullptr;               // mixed: FP64 (kz, kx) = (0, 0) profiles [6][NY2+1]
+    double *phys = nullptr;
+    double *dpdx = nullptr;
+    unsigned *err = nullptr;
+    cdns::SolverState st{};
+    double g_setup = NAN;
+    bool have_velocity = false;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    bool prof = false;
+    int prof_steps = 0;
+    std::vector<cudaEvent_t> ev;
+    cdns::AdjointWork *adj = nullptr;     // discrete-adjoint workspace, made on first use
+
+    template <typename T> int alloc(T *&ptr, size_t count) {
+        void *p = nullptr;
+        const size_t b = sizeof(T) * (count ? count : 1);
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e != cudaSuccess)
+            return cdns::fail(CDNS_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        // Zero on the context stream: a cudaMemset on the legacy default stream
+        // is not ordered against this non-blocking stream and could land after
+        // the kernels that fill the buffer.
+        e = cudaMemsetAsync(p, 0, b, stream);
+        if (e != cudaSuccess) return cdns::fail(CDNS_ERR_CUDA, cudaGetErrorString(e));
+        allocs.push_back(p);
+        bytes += b;
+        ptr = static_cast<T *>(p);
+        return CDNS_OK;
+    }
+};
+
+namespace cdns {
+
+// Multistep coefficients of iteration it (src/sim/simulation.cpp:36-45).
+void step_coefficients(int it, double dt, double re, double &a0, double &a1, double &b0, double &b1,
+                       double &g);
+// Nonlinear stages u -> N (planar spectral) and bw; G_fp64 (FP64 contexts)
+// receives the z-physical fields of u and omega, c->G if null.
+void enqueue_nonlinear(cdns_ctx *c, const double2 *u, double2 *N, bool prof, int step_slot,
+                       double2 *G_fp64 = nullptr);
+// Solver state of c for wall-normal Helmholtz constant g_v (no-op if current).
+int do_setup(cdns_ctx *c, double g_v);
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace cdns

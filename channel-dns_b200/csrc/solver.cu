@@ -37,11 +37,6 @@ struct SolveArgs {
     StepArgs step;
 };
 
-__device__ __forceinline__ double tau_func(double a, double b, int y) {
-    const int q = y & 1;
-    if (a == 0.0 && b == 0.0) return (double)((1 - q) * y * y + q);
-    return a + b * y * y;
-}
 
 // Tau solve of (D^2 - k^2 - g) f = r with a f + b f' = (lower, upper) at
 // y = (+1, -1), both parities at once (src/solver/eqsolve_pv.cpp:64-128).

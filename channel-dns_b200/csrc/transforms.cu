@@ -532,6 +532,94 @@ k_x_r2c(Dims d, FftPlan P, const double2 *__restrict__ roots, const double *__re
 }
 
 // ---------------------------------------------------------------------------
+// Transpose of K3 (discrete adjoint) about the fields G of the forward step:
+// with P = u x omega = c2r(G) products and H = r2c(P) / NX2 (modes k <= NXS),
+//   lP    = c2r(Y),  Y_0 = lH_0, Y_k = lH_k / 2       (the 1/NX2 is applied
+//                                                      by the caller's tables)
+//   lu    = omega x lP,  lomega = lP x u
+//   lG_0  = sum_x l(x) (real),  lG_k = 2 sum_x l(x) e^{-2 pi i k x / NX2}.
+// L holds lH in fields 0..2 on entry and lG in fields 0..5 on return; a block
+// reads and writes only its own rows, so the update is in place.  Block = RW
+// rows (z, j); inverse lines per row: (u, v), (w, om_x), (om_y, om_z),
+// (lP_0, lP_1), (lP_2, 0); forward lines: (lu, lv), (lw, lom_x), (lom_y, lom_z).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256, 2)
+k_x_adjoint(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 *__restrict__ G,
+            double2 *__restrict__ Lb, int RW) {
+    extern __shared__ double2 sm[];
+    const int n = d.NX2;
+    double2 *s_root = sm;
+    const int L5 = 5 * RW, L3 = 3 * RW;
+    double2 *a = sm + n;
+    double2 *b = a + n * L5;
+    const int j = blockIdx.y, z0 = blockIdx.x * RW;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s_root[i] = roots[i];
+    const long long fstride = (long long)d.ny2 * d.NZ2 * d.nkx;
+    const double2 *Gj = G + (long long)j * d.NZ2 * d.nkx;
+    double2 *Lj = Lb + (long long)j * d.NZ2 * d.nkx;
+    const int nyq = (n % 2 == 0) ? n / 2 : -1;
+    const int nkx = d.nkx;
+    const int zlo = d.NXS + 1, zhi = n - d.NXS;   // slots [zlo, zhi) are zero
+    for (int i = threadIdx.x; i < (zhi - zlo) * L5; i += blockDim.x) {
+        const int k = zlo + i / L5, line = i - (i / L5) * L5;
+        a[k * L5 + line] = mk(0, 0);
+    }
+    for (int i = threadIdx.x; i < L5 * nkx; i += blockDim.x) {
+        const int line = i / nkx, m = i - (i / nkx) * nkx;
+        const int r = line / 5, q = line - (line / 5) * 5;
+        const int z = z0 + r;
+        double2 A = mk(0, 0), B = mk(0, 0);
+        if (z < d.NZ2) {
+            const long long o = (long long)z * nkx + m;
+            if (q < 3) {
+                A = Gj[(2 * q) * fstride + o];
+                B = Gj[(2 * q + 1) * fstride + o];
+            } else {
+                const double h = m == 0 ? 1.0 : 0.5;
+                A = cscale(h, Lj[(q == 3 ? 0 : 2) * fstride + o]);
+                if (q == 3) B = cscale(h, Lj[fstride + o]);
+            }
+        }
+        if (m == 0 || m == nyq) {
+            A.y = 0.0;
+            B.y = 0.0;
+        }
+        a[m * L5 + line] = mk(A.x - B.y, A.y + B.x);
+        if (m != 0 && m != nyq) a[(n - m) * L5 + line] = mk(A.x + B.y, B.x - A.y);
+    }
+    __syncthreads();
+    double2 *res = fft_lines<+1>(a, b, L5, P, s_root);
+    double2 *oth = (res == a) ? b : a;
+    for (int i = threadIdx.x; i < n * RW; i += blockDim.x) {
+        const int x = i / RW, r = i - (i / RW) * RW;
+        const double2 p0 = res[x * L5 + 5 * r], p1 = res[x * L5 + 5 * r + 1], p2 = res[x * L5 + 5 * r + 2];
+        const double2 p3 = res[x * L5 + 5 * r + 3], p4 = res[x * L5 + 5 * r + 4];
+        const double uu = p0.x, vv = p0.y, ww = p1.x, ox = p1.y, oy = p2.x, oz = p2.y;
+        const double l0 = p3.x, l1 = p3.y, l2 = p4.x;
+        oth[x * L3 + 3 * r] = mk(oy * l2 - oz * l1, oz * l0 - ox * l2);        // omega x lP
+        oth[x * L3 + 3 * r + 1] = mk(ox * l1 - oy * l0, l1 * ww - l2 * vv);    // ..., (lP x u)_x
+        oth[x * L3 + 3 * r + 2] = mk(l2 * uu - l0 * ww, l0 * vv - l1 * uu);    // (lP x u)_y, _z
+    }
+    __syncthreads();
+    double2 *res2 = fft_lines<-1>(oth, res, L3, P, s_root);
+    for (int i = threadIdx.x; i < RW * 6 * nkx; i += blockDim.x) {
+        const int rf = i / nkx, k = i - (i / nkx) * nkx;
+        const int r = rf / 6, f = rf - (rf / 6) * 6;
+        const int z = z0 + r;
+        if (z >= d.NZ2) continue;
+        const int km = (n - k) % n;
+        const int line = 3 * r + (f >> 1);
+        const double2 P0 = res2[k * L3 + line];
+        const double2 Pm = res2[km * L3 + line];
+        // unpack A = (P + conj Pm)/2, B = (P - conj Pm)/(2i); the c2r transpose doubles k >= 1
+        double2 out = (f & 1) ? mk(0.5 * (P0.y + Pm.y), -0.5 * (P0.x - Pm.x))
+                              : mk(0.5 * (P0.x + Pm.x), 0.5 * (P0.y - Pm.y));
+        out = (k == 0) ? mk(out.x, 0.0) : cscale(2.0, out);
+        Lj[f * fstride + (long long)z * nkx + k] = out;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------
 namespace {
@@ -552,6 +640,8 @@ int z_lines(const Dims &d) {
 
 size_t smem_zfft(const Dims &d) { return sizeof(double2) * (size_t)d.NZ2 * (1 + 2 * z_lines(d)); }
 size_t smem_xcross(const Dims &d) { return sizeof(double2) * (size_t)d.NX2 * (1 + 2 * 3 * kRW); }
+constexpr int kRWa = 2;
+size_t smem_xadjoint(const Dims &d) { return sizeof(double2) * (size_t)d.NX2 * (1 + 2 * 5 * kRWa); }
 size_t smem_xsingle(const Dims &d) {
     return sizeof(double2) * (size_t)d.NX2 * (1 + 2 * ((kRWs + 1) / 2));
 }
@@ -610,6 +700,8 @@ cudaError_t configure_transform_kernels(const Dims &d) {
     e = raise_smem(k_z_forward, (int)smem_zfft(d));
     if (e != cudaSuccess) return e;
     e = raise_smem(k_x_cross, (int)smem_xcross(d));
+    if (e != cudaSuccess) return e;
+    e = raise_smem(k_x_adjoint, (int)smem_xadjoint(d));
     if (e != cudaSuccess) return e;
     e = raise_smem(k_x_c2r, (int)smem_xsingle(d));
     if (e != cudaSuccess) return e;
@@ -678,6 +770,12 @@ void launch_x_cross(const Dims &d, const double2 *roots, const float2 *G, float2
 }
 void launch_z_forward(const Dims &d, const double2 *roots, const float2 *H, float2 *F, int nf, cudaStream_t s) {
     z_forward_r(d, roots, H, F, nf, s);
+}
+
+void launch_x_adjoint(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G, double2 *L,
+                      cudaStream_t s) {
+    dim3 grid((d.NZ2 + kRWa - 1) / kRWa, d.ny2);
+    k_x_adjoint<<<grid, 256, smem_xadjoint(d), s>>>(d, P, roots, G, L, kRWa);
 }
 
 void launch_x_c2r(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G,

@@ -155,6 +155,30 @@ template <int E> __device__ __forceinline__ void suffix_sum(double2 (&S)[E]) {
     for (int e = 0; e < E; ++e) S[e] = cadd(carry, S[e]);
 }
 
+// Diagonal of the tau boundary rows (src/solver/eqsolve_pv.cpp:64-128).
+__device__ __forceinline__ double tau_func(double a, double b, int y) {
+    const int q = y & 1;
+    if (a == 0.0 && b == 0.0) return (double)((1 - q) * y * y + q);
+    return a + b * y * y;
+}
+
+// In-place prefix sums S_y = sum_{j <= y, j = y mod 2} S_j.
+template <int E> __device__ __forceinline__ void prefix_sum(double2 (&S)[E]) {
+    const int L = lane_id();
+#pragma unroll
+    for (int e = 1; e < E; ++e) S[e] = cadd(S[e - 1], S[e]);
+    double2 b = S[E - 1];
+#pragma unroll
+    for (int d = 2; d < 32; d <<= 1) {
+        const double2 t = shfl2_up(b, d);
+        if (L >= d) b = cadd(t, b);
+    }
+    double2 carry = shfl2_up(b, 2);
+    if (L < 2) carry = mk(0.0, 0.0);
+#pragma unroll
+    for (int e = 0; e < E; ++e) S[e] = cadd(carry, S[e]);
+}
+
 // Chebyshev derivative (src/solver/vector_ops.cpp:17-25):
 // d_k = sum_{j > k, j = k+1 mod 2} 2 j f_j, d_0 halved.  f is zero beyond ny.
 template <int E> __device__ __forceinline__ void deriv_warp(int ny, const double2 (&f)[E], double2 (&d)[E]) {

@@ -189,6 +189,46 @@ int cdns_last_error(char *buf, size_t len);
 /* Library version string. */
 const char *cdns_version(void);
 
+/* Discrete adjoint of the FP64 step (no reference counterpart).
+ *
+ * cdns_adjoint_run runs iterations 1..nsteps from the context's velocity
+ * (a first-order start, as after cdns_set_velocity) with the velocity wall
+ * data `control` ([2*NZS+1][2][NXS+1][3] as in cdns_set_velocity_bc; NULL
+ * keeps the current data, a non-NULL array becomes the context's data),
+ * and evaluates `objective`:
+ *   CDNS_OBJECTIVE_WALL_SHEAR  J = (1/nsteps) sum_{n=1..nsteps} tau_w(u^n),
+ *     tau_w = (dU/dy(-1) - dU/dy(+1)) / (2 Re) of the streamwise mean
+ *     profile U (the (kz, kx) = (0, 0) mode of component 0); `weights` unused.
+ *   CDNS_OBJECTIVE_PROJECTION  J = Re sum conj(w) u^nsteps over the stored
+ *     coefficients, w = `weights` in the velocity layout: the gradients are
+ *     then the vector-Jacobian product of the nsteps-step map with w.
+ * If grad_velocity or grad_control is not NULL it also returns the gradient
+ * of J with respect to the real and imaginary parts of every stored
+ * coefficient of the initial velocity ([..spectral..][3], as cdns_set_velocity)
+ * and of the velocity wall data ([..][2][..][3]), by the hand-written
+ * transpose of every stage of the step, run backwards over states restored
+ * from in-memory checkpoints taken every `checkpoint_interval` steps of the
+ * forward sweep (recomputing each interval once).  On return the context
+ * holds the state after `nsteps` steps, as after cdns_run(ctx, 1, nsteps).
+ * Requires CDNS_PRECISION_FP64, INDEX_GRAD_PRE = 1 and dealiased meshes
+ * (NX2 > 2 NXS, NZ2 > 2 NZS, NY2 > NYS). */
+#define CDNS_OBJECTIVE_WALL_SHEAR 0
+#define CDNS_OBJECTIVE_PROJECTION 1
+int cdns_adjoint_run(cdns_ctx *ctx, int nsteps, int checkpoint_interval, int objective,
+                     const double *weights, const double *control, double *objective_value,
+                     double *grad_velocity, double *grad_control);
+
+/* Transposes of single stages, for tests of the adjoint: the solve of
+ * cdns_solve (inputs are the adjoints of its pressure and velocity outputs,
+ * outputs the adjoints of its rhs, pressure and velocity wall data, in the
+ * same layouts) and the nonlinear term of cdns_nonlinear about `velocity`
+ * (adjoints of N and of the pressure wall data in, adjoint of the velocity
+ * out).  Under the real inner product Re sum conj(a) b of the stored arrays. */
+int cdns_solve_adjoint(cdns_ctx *ctx, double g, const double *pressure_adj, const double *velocity_adj,
+                       double *rhs_adj, double *pressure_bc_adj, double *velocity_bc_adj);
+int cdns_nonlinear_adjoint(cdns_ctx *ctx, const double *velocity, const double *nonlinear_adj,
+                           const double *pressure_bc_adj, double *velocity_adj);
+
 /* Ensemble batch: n independent channels (meshes and params may differ, one
  * precision mode) on one device.  No reference counterpart (the reference
  * runs one channel per process); each member is a full context whose state
