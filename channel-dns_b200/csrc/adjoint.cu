@@ -165,6 +165,15 @@ struct AdjArgs {
     double2 *lbcv;            // [3][2][ncol] adjoint of the velocity wall data (accumulated)
     int solve_only;           // 1: no zero-mode overwrite (cdns_solve)
     double seed;              // objective seed on the mean profile (0: none)
+    // Reverse-step bookkeeping in place of the lR output (acc != 0), for
+    // R = a0 u^{s-1} + a1 u^{s-2} + b0 N^{s-1} + b1 N^{s-2} and wall data
+    // b0 B^{s-1} + b1 B^{s-2} (B = bw + wall sums of N_y):
+    //   lu1 += a0 lR, lu2 = a1 lR, lN1 += b0 lR (+ wall sums^T(lbw) in y),
+    //   lN2 = b1 lR, lbw = lB1 + b0 lBc, lB2 = b1 lBc.
+    int acc;
+    double a0, a1, b0, b1;
+    double2 *lu1, *lu2, *lN1, *lN2, *lbw, *lB2;
+    const double2 *lB1;
 };
 
 template <int E>
@@ -173,6 +182,7 @@ k_solve_adj(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, AdjArgs
     extern __shared__ double2 tile[];   // [4][ncy][TC]
     __shared__ double2 red[TC][TC][4];  // [warp][column][lc0, lc1, lsg0, lsg1]
     __shared__ double2 s_zbc;           // zero mode: adjoint of the mean wall v
+    __shared__ double2 s_bw[TC][2];     // per column: complete lbw (top, bottom)
     const int ncy = d.ncy, ny = d.NYS, nkx = d.nkx, ncol = d.ncol;
     const long long Ns = d.Ns;
     const int S = ncy * TC;
@@ -353,6 +363,16 @@ k_solve_adj(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, AdjArgs
         if (L == 0) {
             A.lBc[col] = llo;
             A.lBc[ncol + col] = lup;
+            if (A.acc) {
+                const double2 bt = cadd(A.lB1[col], cscale(A.b0, llo));
+                const double2 bb = cadd(A.lB1[ncol + col], cscale(A.b0, lup));
+                A.lbw[col] = bt;
+                A.lbw[ncol + col] = bb;
+                A.lB2[col] = cscale(A.b1, llo);
+                A.lB2[ncol + col] = cscale(A.b1, lup);
+                s_bw[w][0] = bt;
+                s_bw[w][1] = bb;
+            }
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
                 double2 lo = lblo[c], up = lbup[c];
@@ -373,8 +393,23 @@ k_solve_adj(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, AdjArgs
         const int kzi = c2 / nkx, kx = c2 - (c2 / nkx) * nkx;
         const long long off = ((long long)kzi * ncy + y) * nkx + kx;
         const int sl = tile_slot<E>(y, l);
+        if (!A.acc) {
 #pragma unroll
-        for (int c = 0; c < 3; ++c) A.lR[c * Ns + off] = tile[(1 + c) * S + sl];
+            for (int c = 0; c < 3; ++c) A.lR[c * Ns + off] = tile[(1 + c) * S + sl];
+            continue;
+        }
+        const double2 bt = s_bw[l][0], bb = s_bw[l][1];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const long long o = c * Ns + off;
+            const double2 r = tile[(1 + c) * S + sl];
+            A.lu1[o] = cadd(A.lu1[o], cscale(A.a0, r));
+            A.lu2[o] = cscale(A.a1, r);
+            double2 nn = cadd(A.lN1[o], cscale(A.b0, r));
+            if (c == 1) nn = cadd(nn, (y & 1) ? cadd(bt, bb) : csub(bt, bb));
+            A.lN1[o] = nn;
+            A.lN2[o] = cscale(A.b1, r);
+        }
     }
 }
 
@@ -399,6 +434,44 @@ static cudaError_t configure_solve_adjoint(const Dims &d) {
     }
 }
 
+static void solve_adj_dispatch(const Dims &d, const Tables &t, const PhysParams &pp, double g_v,
+                               const SolverState &st, const AdjArgs &A, cudaStream_t s) {
+    switch (lane_elems(d)) {
+    case 1: solve_adj_e<1>(d, t, pp, g_v, st, A, s); break;
+    case 2: solve_adj_e<2>(d, t, pp, g_v, st, A, s); break;
+    case 4: solve_adj_e<4>(d, t, pp, g_v, st, A, s); break;
+    case 8: solve_adj_e<8>(d, t, pp, g_v, st, A, s); break;
+    default: break;
+    }
+}
+
+void launch_solve_adjoint_step(const Dims &d, const Tables &t, const PhysParams &pp, double g_v,
+                               const SolverState &st, const double2 *lv, double seed, double a0, double a1,
+                               double b0, double b1, double2 *lu1, double2 *lu2, double2 *lN1, double2 *lN2,
+                               const double2 *lB1, double2 *lbw, double2 *lB2, double2 *lBc, double2 *lbcv,
+                               cudaStream_t s) {
+    AdjArgs A{};
+    A.p_a = pp.a_pre0;
+    A.p_b = pp.b_pre0;
+    A.lv = lv;
+    A.lBc = lBc;
+    A.lbcv = lbcv;
+    A.seed = seed;
+    A.acc = 1;
+    A.a0 = a0;
+    A.a1 = a1;
+    A.b0 = b0;
+    A.b1 = b1;
+    A.lu1 = lu1;
+    A.lu2 = lu2;
+    A.lN1 = lN1;
+    A.lN2 = lN2;
+    A.lB1 = lB1;
+    A.lbw = lbw;
+    A.lB2 = lB2;
+    solve_adj_dispatch(d, t, pp, g_v, st, A, s);
+}
+
 void launch_solve_adjoint(const Dims &d, const Tables &t, const PhysParams &pp, double g_v, const SolverState &st,
                           const double2 *lp, const double2 *lv, double2 *lR, double2 *lBc, double2 *lbcv,
                           int solve_only, double seed, cudaStream_t s) {
@@ -412,13 +485,7 @@ void launch_solve_adjoint(const Dims &d, const Tables &t, const PhysParams &pp, 
     A.lBc = lBc;
     A.lbcv = lbcv;
     A.solve_only = solve_only;
-    switch (lane_elems(d)) {
-    case 1: solve_adj_e<1>(d, t, pp, g_v, st, A, s); break;
-    case 2: solve_adj_e<2>(d, t, pp, g_v, st, A, s); break;
-    case 4: solve_adj_e<4>(d, t, pp, g_v, st, A, s); break;
-    case 8: solve_adj_e<8>(d, t, pp, g_v, st, A, s); break;
-    default: break;
-    }
+    solve_adj_dispatch(d, t, pp, g_v, st, A, s);
 }
 
 
@@ -505,49 +572,6 @@ k_curl_adj(Dims d, Tables t, const double2 *__restrict__ lS, const double2 *__re
 
 size_t curl_adj_smem(const Dims &d) { return sizeof(double2) * 3 * (size_t)d.ncy * kColsPerBlock; }
 
-// Multistep bookkeeping of the reverse step s (R = a0 u^{s-1} + a1 u^{s-2} +
-// b0 N^{s-1} + b1 N^{s-2}, wall data b0 B^{s-1} + b1 B^{s-2}):
-//   lu1 += a0 lR, lu2 = a1 lR, lN1 += b0 lR, lN2 = b1 lR,
-//   lbw = lB1 + b0 lBc (complete), lB2 = b1 lBc,
-// and the wall sums B = bw + sum_y (1, s_y) N_y transposed into lN1's y component.
-__global__ void k_adj_accumulate(Dims d, const double2 *__restrict__ lR, const double2 *__restrict__ lBc,
-                                 double a0, double a1, double b0, double b1, double2 *__restrict__ lu1,
-                                 double2 *__restrict__ lu2, double2 *__restrict__ lN1, double2 *__restrict__ lN2,
-                                 const double2 *__restrict__ lB1, double2 *__restrict__ lbw,
-                                 double2 *__restrict__ lB2) {
-    const long long n3 = 3 * d.Ns, ncol = d.ncol;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3 + ncol;
-         i += (long long)gridDim.x * blockDim.x) {
-        if (i < n3) {
-            const int c = (int)(i / d.Ns);
-            const long long off = i - c * d.Ns;
-            const double2 r = lR[i];
-            lu1[i] = cadd(lu1[i], cscale(a0, r));
-            lu2[i] = cscale(a1, r);
-            double2 n = cadd(lN1[i], cscale(b0, r));
-            if (c == 1) {
-                const int kx = (int)(off % d.nkx);
-                const long long q = off / d.nkx;
-                const int y = (int)(q % d.ncy), kzi = (int)(q / d.ncy);
-                const long long col = (long long)kzi * d.nkx + kx;
-                const double2 bt = cadd(lB1[col], cscale(b0, lBc[col]));
-                const double2 bb = cadd(lB1[ncol + col], cscale(b0, lBc[ncol + col]));
-                n = cadd(n, (y & 1) ? cadd(bt, bb) : csub(bt, bb));
-            }
-            lN1[i] = n;
-            lN2[i] = cscale(b1, r);
-        } else {
-            const long long col = i - n3;
-            for (int wall = 0; wall < 2; ++wall) {
-                const long long o = wall * ncol + col;
-                const double2 lc = lBc[o];
-                lbw[o] = cadd(lB1[o], cscale(b0, lc));
-                lB2[o] = cscale(b1, lc);
-            }
-        }
-    }
-}
-
 // lN_y += the transposed wall sums of lB (standalone nonlinear adjoint).
 __global__ void k_pressure_bc_adj(Dims d, const double2 *__restrict__ lB, double2 *__restrict__ lN) {
     const long long ncol = d.ncol;
@@ -603,13 +627,6 @@ void launch_curl_adjoint(const Dims &d, const Tables &t, const double2 *lS, cons
 }
 
 static int grid_for(long long n) { return (int)std::min<long long>((n + 255) / 256, 148LL * 16); }
-
-void launch_adjoint_accumulate(const Dims &d, const double2 *lR, const double2 *lBc, double a0, double a1,
-                               double b0, double b1, double2 *lu1, double2 *lu2, double2 *lN1, double2 *lN2,
-                               const double2 *lB1, double2 *lbw, double2 *lB2, cudaStream_t s) {
-    k_adj_accumulate<<<grid_for(3 * d.Ns + d.ncol), 256, 0, s>>>(d, lR, lBc, a0, a1, b0, b1, lu1, lu2, lN1, lN2,
-                                                                 lB1, lbw, lB2);
-}
 
 void launch_pressure_bc_adjoint(const Dims &d, const double2 *lB, double2 *lN, cudaStream_t s) {
     k_pressure_bc_adj<<<grid_for(d.Ns), 256, 0, s>>>(d, lB, lN);

@@ -16,7 +16,11 @@
 // B^{s-1}) every checkpoint_interval steps; the reverse sweep restores each
 // interval, recomputes it once keeping the z-physical fields of u and omega
 // of every step (the linearisation point of u x omega), and runs its reverse
-// steps.  Iteration 1 (g of the first-order start) has its own solver state.
+// steps.  The last interval keeps those fields from the forward sweep and is
+// not recomputed; the recomputation of interval i-1 (context stream) runs
+// concurrently with the reverse steps of interval i (a second stream), the
+// two alternating between two slot sets.  Iteration 1 (g of the first-order
+// start) has its own solver state.
 #include <algorithm>
 #include <cstring>
 
@@ -34,14 +38,22 @@ struct AdjointWork {
     double2 *lR = nullptr, *lBc = nullptr, *lbw = nullptr, *lbcv = nullptr, *l6 = nullptr;
     double2 *ck = nullptr;    // checkpoints [nck][9 Ns + 2 ncol]
     size_t nck = 0;
-    double2 *gs = nullptr;    // z-physical fields of one interval [ngs][6][NY2+1][NZ2][NXS+1]
+    double2 *gs = nullptr;    // z-physical fields of two intervals [2][k][6][NY2+1][NZ2][NXS+1]
     size_t ngs = 0;
     double *jbuf = nullptr;   // objective per step
     size_t nj = 0;
+    double2 *AF = nullptr, *AG = nullptr;   // stage scratch of the reverse steps
+    cudaStream_t rs = nullptr;              // reverse-step stream (recomputation runs on the context's)
+    cudaEvent_t ev_rec[2] = {nullptr, nullptr}, ev_rev[2] = {nullptr, nullptr}, ev_fwd = nullptr,
+                ev_done = nullptr;
 };
 
 void adjoint_release(AdjointWork *w) {
     if (!w) return;
+    if (w->rs) cudaStreamSynchronize(w->rs);
+    for (cudaEvent_t e : {w->ev_rec[0], w->ev_rec[1], w->ev_rev[0], w->ev_rev[1], w->ev_fwd, w->ev_done})
+        if (e) cudaEventDestroy(e);
+    if (w->rs) cudaStreamDestroy(w->rs);
     for (void *p : w->allocs) cudaFree(p);
     if (w->ck) cudaFree(w->ck);
     if (w->gs) cudaFree(w->gs);
@@ -117,8 +129,12 @@ int ensure_work(cdns_ctx *c, size_t nck, size_t ngs, size_t nj) {
             (r = dalloc(c, w, w->lB[0], 2 * nc)) || (r = dalloc(c, w, w->lB[1], 2 * nc)) ||
             (r = dalloc(c, w, w->lR, 3 * Ns)) || (r = dalloc(c, w, w->lBc, 2 * nc)) ||
             (r = dalloc(c, w, w->lbw, 2 * nc)) || (r = dalloc(c, w, w->lbcv, 6 * nc)) ||
-            (r = dalloc(c, w, w->l6, 6 * Ns)))
+            (r = dalloc(c, w, w->l6, 6 * Ns)) || (r = dalloc(c, w, w->AF, 6 * (size_t)d.ny2 * d.fcol)) ||
+            (r = dalloc(c, w, w->AG, gs_size(d))))
             return r;
+        CK(cudaStreamCreateWithFlags(&w->rs, cudaStreamNonBlocking));
+        for (cudaEvent_t *e : {&w->ev_rec[0], &w->ev_rec[1], &w->ev_rev[0], &w->ev_rev[1], &w->ev_fwd, &w->ev_done})
+            CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
         launch_cheb_tables_adjoint(d, c->t.cosy, w->csyn_t, w->cana_t, c->stream);
         CK(configure_adjoint_kernels(d));
         CK(cudaGetLastError());
@@ -158,13 +174,20 @@ int load_checkpoint(cdns_ctx *c, size_t i) {
 }
 
 // One forward step (the body of cdns_step) with an explicit solver state and
-// z-physical buffer; solve = false stops after the nonlinear term.
+// z-physical buffer; solve = false stops once G holds the z-physical fields
+// of u and omega (the linearisation point the reverse step needs).
 void forward_step(cdns_ctx *c, int it, const SolverState &st, double2 *G, bool solve) {
     double a0, a1, b0, b1, g;
     step_coefficients(it, c->DT, c->pp.Re, a0, a1, b0, b1, g);
     const int k = c->cur;
+    const Dims &d = c->d;
+    if (!solve) {
+        launch_curl(d, c->t, c->U[k], c->om, nullptr, c->pp.Re, c->stream);
+        launch_ysynth(d, c->t, c->U[k], c->om, 3, 6, c->F, c->stream);
+        launch_z_backward(d, c->pz, c->t.root_z, c->F, G, 6, c->stream);
+        return;
+    }
     enqueue_nonlinear(c, c->U[k], c->Nb[k], false, 0, G);
-    if (!solve) return;
     StepArgs a{};
     a.u = c->U[k];
     a.u_prev = c->U[1 - k];
@@ -188,19 +211,20 @@ void forward_step(cdns_ctx *c, int it, const SolverState &st, double2 *G, bool s
 
 // lu += NL'(u)^T (lN, lbw) about the z-physical fields G6 of u and omega:
 // transposed analysis -> transposed z analysis -> transposed x stage ->
-// transposed z synthesis -> transposed synthesis -> transposed curl.
-void nonlinear_adjoint(cdns_ctx *c, const double2 *G6, const double2 *lN, const double2 *lbw, double2 *lu) {
+// transposed z synthesis -> transposed synthesis -> transposed curl, on
+// stream s with the adjoint's own stage scratch.
+void nonlinear_adjoint(cdns_ctx *c, const double2 *G6, const double2 *lN, const double2 *lbw, double2 *lu,
+                       cudaStream_t s) {
     const Dims &d = c->d;
     AdjointWork *w = c->adj;
-    cudaStream_t s = c->stream;
     Tables ta = c->t;
     ta.csyn = w->csyn_t;   // includes 1/(NX2 NZ2): the transposed x and z analysis scalings
-    launch_ysynth(d, ta, lN, nullptr, 3, 3, c->F, s);
-    launch_z_backward(d, c->pz, c->t.root_z, c->F, c->G, 3, s);
-    launch_x_adjoint(d, c->px, c->t.root_x, G6, c->G, s);
+    launch_ysynth(d, ta, lN, nullptr, 3, 3, w->AF, s);
+    launch_z_backward(d, c->pz, c->t.root_z, w->AF, w->AG, 3, s);
+    launch_x_adjoint(d, c->px, c->t.root_x, G6, w->AG, s);
     // transposed z synthesis = NZ2 x the (1/NZ2-scaled) forward z transform
-    launch_z_forward(d, c->pz, c->t.root_z, c->G, c->F, 6, s);
-    launch_yanalysis_scaled(d, w->cana_t, c->F, w->l6, 6, (double)d.NZ2, s);
+    launch_z_forward(d, c->pz, c->t.root_z, w->AG, w->AF, 6, s);
+    launch_yanalysis_scaled(d, w->cana_t, w->AF, w->l6, 6, (double)d.NZ2, s);
     launch_curl_adjoint(d, c->t, w->l6, lbw, lu, c->pp.Re, s);
 }
 
@@ -241,7 +265,7 @@ int cdns_adjoint_run(cdns_ctx *c, int nsteps, int kck, int objective, const doub
     cudaStream_t s = c->stream;
     const bool grad = grad_u || grad_bc;
     const int nseg = (nsteps + kck - 1) / kck;
-    if ((r = ensure_work(c, grad ? nseg + 1 : 0, grad ? kck : 0, nsteps))) return r;
+    if ((r = ensure_work(c, grad ? nseg + 1 : 0, grad ? (size_t)kck * (nseg > 1 ? 2 : 1) : 0, nsteps))) return r;
     AdjointWork *w = c->adj;
     double a0, a1, b0, b1, g1, g2;
     step_coefficients(1, c->DT, c->pp.Re, a0, a1, b0, b1, g1);
@@ -253,10 +277,15 @@ int cdns_adjoint_run(cdns_ctx *c, int nsteps, int kck, int objective, const doub
     }
     if ((r = do_setup(c, g2))) return r;
     auto state_for = [&](int it) -> const SolverState & { return it == 1 ? w->st1 : c->st; };
-    // ---- forward sweep ----
+    // ---- forward sweep (the last interval keeps its z-physical fields) ----
+    const size_t gsz = gs_size(d);
+    const int s_last = (nseg - 1) * kck;
+    // z-physical slot of iteration it in interval seg (two sets, alternating)
+    auto slot = [&](int seg, int it) { return w->gs + ((size_t)(seg & 1) * kck + (it - seg * kck - 1)) * gsz; };
     for (int it = 1; it <= nsteps; ++it) {
         if (grad && (it - 1) % kck == 0 && (r = save_checkpoint(c, (size_t)(it - 1) / kck))) return r;
-        forward_step(c, it, state_for(it), c->G, true);
+        double2 *G = (grad && it > s_last) ? slot(nseg - 1, it) : c->G;
+        forward_step(c, it, state_for(it), G, true);
         if (shear) launch_wall_shear(d, c->U[c->cur], c->pp.Re, w->jbuf + it - 1, s);
     }
     CK(cudaGetLastError());
@@ -285,25 +314,36 @@ int cdns_adjoint_run(cdns_ctx *c, int nsteps, int kck, int objective, const doub
             launch_deinterleave(c->aux2, w->lU[nsteps & 1], d.Ns, 3, s);
         }
         const double seed = shear ? -1.0 / ((double)nsteps * c->pp.Re) : 0.0;
-        const size_t gsz = gs_size(d);
-        // ---- reverse sweep, interval by interval ----
+        // ---- reverse sweep: the reverse steps of interval seg run on the
+        // reverse stream while the context stream recomputes interval seg - 1
+        // from its checkpoint into the other slot set ----
+        cudaStream_t rs = w->rs;
+        CK(cudaEventRecord(w->ev_fwd, s));
+        CK(cudaStreamWaitEvent(rs, w->ev_fwd, 0));
         for (int seg = nseg - 1; seg >= 0; --seg) {
+            if (seg >= 1) {
+                const int ps = seg - 1, p0 = ps * kck, p1 = std::min(p0 + kck, nsteps);
+                if (seg + 1 <= nseg - 1) CK(cudaStreamWaitEvent(s, w->ev_rev[ps & 1], 0));
+                if ((r = load_checkpoint(c, (size_t)ps))) return r;
+                for (int it = p0 + 1; it <= p1; ++it) forward_step(c, it, state_for(it), slot(ps, it), it < p1);
+                CK(cudaEventRecord(w->ev_rec[ps & 1], s));
+            }
             const int s0 = seg * kck, s1 = std::min(s0 + kck, nsteps);
-            if ((r = load_checkpoint(c, (size_t)seg))) return r;
-            for (int it = s0 + 1; it <= s1; ++it)
-                forward_step(c, it, state_for(it), w->gs + (size_t)(it - s0 - 1) * gsz, it < s1);
+            if (seg < nseg - 1) CK(cudaStreamWaitEvent(rs, w->ev_rec[seg & 1], 0));
             for (int it = s1; it > s0; --it) {
                 double g;
                 step_coefficients(it, c->DT, c->pp.Re, a0, a1, b0, b1, g);
                 const int cu = it & 1, pv = (it - 1) & 1;
-                launch_solve_adjoint(d, c->t, c->pp, g, state_for(it), nullptr, w->lU[cu], w->lR, w->lBc, w->lbcv,
-                                     0, seed, s);
-                launch_adjoint_accumulate(d, w->lR, w->lBc, a0, a1, b0, b1, w->lU[pv], w->lU[cu], w->lN[pv],
-                                          w->lN[cu], w->lB[pv], w->lbw, w->lB[cu], s);
-                nonlinear_adjoint(c, w->gs + (size_t)(it - s0 - 1) * gsz, w->lN[pv], w->lbw, w->lU[pv]);
+                launch_solve_adjoint_step(d, c->t, c->pp, g, state_for(it), w->lU[cu], seed, a0, a1, b0, b1,
+                                          w->lU[pv], w->lU[cu], w->lN[pv], w->lN[cu], w->lB[pv], w->lbw,
+                                          w->lB[cu], w->lBc, w->lbcv, rs);
+                nonlinear_adjoint(c, slot(seg, it), w->lN[pv], w->lbw, w->lU[pv], rs);
             }
+            CK(cudaEventRecord(w->ev_rev[seg & 1], rs));
             CK(cudaGetLastError());
         }
+        CK(cudaEventRecord(w->ev_done, rs));
+        CK(cudaStreamWaitEvent(s, w->ev_done, 0));
         if (grad_u) {
             launch_interleave(w->lU[0], c->aux, d.Ns, 3, s);
             CK(cudaGetLastError());
@@ -380,7 +420,7 @@ int cdns_nonlinear_adjoint(cdns_ctx *c, const double *velocity, const double *lN
     CK(cudaMemcpyAsync(w->lbw, hb.data(), hb.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
     launch_pressure_bc_adjoint(d, w->lbw, w->lN[0], s);
     CK(cudaMemsetAsync(w->lU[0], 0, 3 * Ns * sizeof(double2), s));
-    nonlinear_adjoint(c, w->gs, w->lN[0], w->lbw, w->lU[0]);
+    nonlinear_adjoint(c, w->gs, w->lN[0], w->lbw, w->lU[0], s);
     launch_interleave(w->lU[0], c->aux2, d.Ns, 3, s);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(lu, c->aux2, 3 * Ns * sizeof(double2), cudaMemcpyDeviceToHost, s));

@@ -118,9 +118,15 @@ void launch_solve_adjoint(const Dims &d, const Tables &t, const PhysParams &pp, 
 // lu[3][Ns] += lS[0..2] + curl^T(lS[3..5], lbw[2][ncol]) (lbw may be null)
 void launch_curl_adjoint(const Dims &d, const Tables &t, const double2 *lS, const double2 *lbw, double2 *lu,
                          double re, cudaStream_t s);
-void launch_adjoint_accumulate(const Dims &d, const double2 *lR, const double2 *lBc, double a0, double a1,
+// Reverse step s of the time stepping: the solve transpose of lv = lu^s
+// (+ the wall-shear seed) with the multistep bookkeeping fused:
+//   lu1 += a0 lR, lu2 = a1 lR, lN1 += b0 lR + wall sums^T(lbw), lN2 = b1 lR,
+//   lbw = lB1 + b0 lBc, lB2 = b1 lBc, lbcv += the velocity wall data adjoint.
+void launch_solve_adjoint_step(const Dims &d, const Tables &t, const PhysParams &pp, double g_v,
+                               const SolverState &st, const double2 *lv, double seed, double a0, double a1,
                                double b0, double b1, double2 *lu1, double2 *lu2, double2 *lN1, double2 *lN2,
-                               const double2 *lB1, double2 *lbw, double2 *lB2, cudaStream_t s);
+                               const double2 *lB1, double2 *lbw, double2 *lB2, double2 *lBc, double2 *lbcv,
+                               cudaStream_t s);
 void launch_pressure_bc_adjoint(const Dims &d, const double2 *lB, double2 *lN, cudaStream_t s);
 void launch_wall_shear(const Dims &d, const double2 *u, double re, double *out, cudaStream_t s);
 

@@ -454,6 +454,151 @@ k_x_cross_r(Dims d, const double2 *__restrict__ roots, const C *__restrict__ G, 
 }
 
 // ---------------------------------------------------------------------------
+// Transpose of K3 in the register form (NX2 = N1 x N2, FP64): k_x_adjoint's
+// algebra with the layout of k_x_cross_r.  16 lanes per line, RW rows per
+// block; five inverse lines per row, (u, v), (w, om_x), (om_y, om_z),
+// (lP_0, lP_1), (lP_2, 0), and three forward lines per row, (lu, lv),
+// (lw, lom_x), (lom_y, lom_z).  Phase 1 reads lH (fields 0..2 of L) and
+// phase 4 writes lG (fields 0..5 of L) for the block's own rows only.
+// ---------------------------------------------------------------------------
+template <int N1, int N2>
+__global__ void __launch_bounds__(16 * 5 * 2)
+k_x_adjoint_r(Dims d, const double2 *__restrict__ roots, const double2 *__restrict__ G, double2 *__restrict__ Lb,
+              int RW) {
+    using C = double2;
+    constexpr int n = N1 * N2;
+    constexpr int SP = N2 + 1;
+    extern __shared__ double2 sm_d[];
+    C *buf = sm_d + n;
+    const int L = 5 * RW, L3 = 3 * RW;
+    const int slot = threadIdx.x >> 4, sub = threadIdx.x & 15;
+    const int j = blockIdx.y, z0 = blockIdx.x * RW;
+    const int nkx = d.nkx, nxs = d.NXS;
+    const long long fstride = (long long)d.ny2 * d.NZ2 * nkx;
+    const C *Gj = G + (long long)j * d.NZ2 * nkx;
+    C *Lj = Lb + (long long)j * d.NZ2 * nkx;
+    const Twiddles<C> tw = load_twiddles<C>(sm_d, roots, n);
+    const int nyq = (n % 2 == 0) ? n / 2 : -1;
+    C v[N1 > N2 ? N1 : N2];
+
+    // ---- phase 1: spectrum gather, N1-point DFTs (backward) ---------------
+    const bool act1 = slot < L && sub < N2;
+    if (act1) {
+        const int r = slot / 5, q = slot - (slot / 5) * 5;
+        const int z = z0 + r;
+        const bool lam = q >= 3, hasB = q != 4;
+        const C *rowA = q < 3 ? Gj + (long long)z * nkx + (2 * q) * fstride
+                              : Lj + (long long)z * nkx + (q == 3 ? 0 : 2) * fstride;
+        const C *rowB = rowA + fstride;
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) {
+            const int m = sub + N2 * n1;
+            C x = mk(0.0, 0.0);
+            if (z < d.NZ2) {
+                const int mm = m <= nxs ? m : n - m;
+                if (m <= nxs || (m >= n - nxs && m != nyq)) {
+                    C A = rowA[mm], B = hasB ? rowB[mm] : mk(0.0, 0.0);
+                    if (lam && mm > 0) {
+                        A = cscale(0.5, A);
+                        B = cscale(0.5, B);
+                    }
+                    if (mm == 0 || mm == nyq) {
+                        A.y = 0.0;
+                        B.y = 0.0;
+                    }
+                    x = m <= nxs ? mk(A.x - B.y, A.y + B.x) : mk(A.x + B.y, B.x - A.y);
+                }
+            }
+            v[n1] = x;
+        }
+    }
+    __syncthreads();   // twiddles complete
+    if (act1) {
+        C(&w)[N1] = reinterpret_cast<C(&)[N1]>(v);
+        dft_reg<N1, +1>(w, tw, N2);
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1)
+            buf[(slot * N1 + k1) * SP + sub] = (k1 == 0 || sub == 0) ? w[k1] : tw.template mul<+1>(w[k1], sub * k1);
+    }
+    __syncthreads();
+    // ---- phase 2: N2-point DFTs -> physical rows --------------------------
+    const bool act2 = slot < L && sub < N1;
+    if (act2) {
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) v[n2] = buf[(slot * N1 + sub) * SP + n2];
+    }
+    __syncthreads();
+    if (act2) {
+        C(&w)[N2] = reinterpret_cast<C(&)[N2]>(v);
+        dft_reg<N2, +1>(w, tw, N1);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) buf[slot * n + sub + N1 * k2] = w[k2];
+    }
+    __syncthreads();
+    // ---- phase 3: lu = om x lP, lom = lP x u; N1-point DFTs (forward) -----
+    const bool act3 = slot < L3 && sub < N2;
+    if (act3) {
+        const int r = slot / 3, q = slot - (slot / 3) * 3;
+        const C *P = buf + (5 * r) * n;
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) {
+            const int x = sub + N2 * n1;
+            const C p0 = P[x], p1 = P[n + x], p2 = P[2 * n + x], p3 = P[3 * n + x], p4 = P[4 * n + x];
+            const double uu = p0.x, vv = p0.y, ww = p1.x, ox = p1.y, oy = p2.x, oz = p2.y;
+            const double l0 = p3.x, l1 = p3.y, l2 = p4.x;
+            C t;
+            if (q == 0) t = mk(oy * l2 - oz * l1, oz * l0 - ox * l2);
+            else if (q == 1) t = mk(ox * l1 - oy * l0, l1 * ww - l2 * vv);
+            else t = mk(l2 * uu - l0 * ww, l0 * vv - l1 * uu);
+            v[n1] = t;
+        }
+    }
+    __syncthreads();
+    if (act3) {
+        C(&w)[N1] = reinterpret_cast<C(&)[N1]>(v);
+        dft_reg<N1, -1>(w, tw, N2);
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1)
+            buf[(slot * N1 + k1) * SP + sub] = (k1 == 0 || sub == 0) ? w[k1] : tw.template mul<-1>(w[k1], sub * k1);
+    }
+    __syncthreads();
+    // ---- phase 4: N2-point DFTs, unpack, modes k <= NXS (x 2 for k >= 1) --
+    const bool act4 = slot < L3 && sub < N1;
+    if (act4) {
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) v[n2] = buf[(slot * N1 + sub) * SP + n2];
+        C(&w)[N2] = reinterpret_cast<C(&)[N2]>(v);
+        dft_reg<N2, -1>(w, tw, N1);
+    }
+    const int lane = threadIdx.x & 31;
+    const int partner = (lane & 16) + (sub < N1 ? (N1 - sub) % N1 : sub);
+    const int r = slot / 3, q = slot - (slot / 3) * 3;
+    const int z = z0 + r;
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) {
+        C pm;
+        pm.x = __shfl_sync(0xffffffffu, v[N2 - 1 - k2].x, partner);
+        pm.y = __shfl_sync(0xffffffffu, v[N2 - 1 - k2].y, partner);
+        const int k = sub + N1 * k2;
+        if (!act4 || k > nxs || z >= d.NZ2) continue;
+        if (sub == 0) pm = v[(N2 - k2) % N2];
+        const C p0 = v[k2];
+        C outA = mk(0.5 * (p0.x + pm.x), 0.5 * (p0.y - pm.y));
+        C outB = mk(0.5 * (p0.y + pm.y), -0.5 * (p0.x - pm.x));
+        if (k == 0) {
+            outA.y = 0.0;
+            outB.y = 0.0;
+        } else {
+            outA = cscale(2.0, outA);
+            outB = cscale(2.0, outB);
+        }
+        C *h = Lj + (2 * q) * fstride + (long long)z * nkx + k;
+        h[0] = outA;
+        h[fstride] = outB;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Single-field x transforms for the standalone fine transform (tests and
 // to-physical output): c2r / r2c of one real field [z][j][x].
 // ---------------------------------------------------------------------------
@@ -663,6 +808,12 @@ constexpr int kRWr = 4;
 size_t smem_zfft_r(const Dims &d, int n1, int n2, size_t elem) {
     return sizeof(double2) * n1 * n2 + elem * ((size_t)n1 * n2 * z_lines(d));
 }
+constexpr int kRWar = 2;   // rows per block of the register-form x adjoint (16 * 5 * kRWar threads)
+size_t smem_xadjoint_r(int n1, int n2) {
+    const size_t L = 5 * kRWar;
+    const size_t s1 = L * n1 * (n2 + 1), s2 = L * n1 * n2;
+    return sizeof(double2) * (n1 * n2 + (s1 > s2 ? s1 : s2));
+}
 size_t smem_xcross_r(int n1, int n2, size_t elem) {
     const size_t L = 3 * kRWr;
     const size_t s1 = L * n1 * (n2 + 1), s2 = L * n1 * n2;
@@ -674,6 +825,7 @@ template <class C> cudaError_t configure_register_forms(const Dims &d) {
     with_xsplit(d.NX2, [&](auto a, auto b) {
         constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
         e = raise_smem(k_x_cross_r<N1, N2, C, sizeof(C) == 8>, smem_xcross_r(N1, N2, sizeof(C)));
+        if (e == cudaSuccess && sizeof(C) == 16) e = raise_smem(k_x_adjoint_r<N1, N2>, smem_xadjoint_r(N1, N2));
     });
     if (e != cudaSuccess) return e;
     with_xsplit(d.NZ2, [&](auto a, auto b) {
@@ -774,6 +926,12 @@ void launch_z_forward(const Dims &d, const double2 *roots, const float2 *H, floa
 
 void launch_x_adjoint(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G, double2 *L,
                       cudaStream_t s) {
+    const bool reg = with_xsplit(d.NX2, [&](auto a, auto b) {
+        constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
+        dim3 grid((d.NZ2 + kRWar - 1) / kRWar, d.ny2);
+        k_x_adjoint_r<N1, N2><<<grid, 16 * 5 * kRWar, smem_xadjoint_r(N1, N2), s>>>(d, roots, G, L, kRWar);
+    });
+    if (reg) return;
     dim3 grid((d.NZ2 + kRWa - 1) / kRWa, d.ny2);
     k_x_adjoint<<<grid, 256, smem_xadjoint(d), s>>>(d, P, roots, G, L, kRWa);
 }
