@@ -265,6 +265,72 @@ def run_ensemble(members: int, K: int, W: int, precision: int, device: int, seed
             "re_tau_range": [float(res.min()), float(res.max())]}
 
 
+def run_adjoint(device: int, seed: int, reps: int = 3) -> dict:
+    """Adjoint form: a 64 x 65 x 64 channel (96 x 97 x 96 product grid) at
+    Re_tau 180 from a log-law mean plus a k^-5/3 perturbation (10 % rms), the
+    wall shear stress averaged over 50 steps, wall blowing/suction on the
+    |k| <= 8 modes (0.01 per mode), checkpoints every 10 steps.  The forward
+    run (cdns_run, iterations 1..50) and the gradient run (cdns_adjoint_run:
+    forward sweep, recomputation and reverse steps) are timed with CUDA events
+    on the context stream, best of `reps`; a 4th-order central difference
+    along one velocity and one control direction checks the gradient."""
+    import numpy as np
+    import torch
+    import cdns
+    from cdns.fields import blowing_suction, divergence_free_field
+    mesh, params = ensemble_case(64, 180.0)
+    N, KC = 50, 10
+    u0 = np.stack(divergence_free_field(mesh, params, seed=seed, amp=0.1, spectrum="k53", mean="loglaw"), axis=-1)
+    bc0 = blowing_suction(mesh, seed + 1, amp=1e-2)
+    ctx = cdns.Context(mesh, params, device=device)
+    ctx.set_velocity_bc(bc0)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=device)
+
+    def timed(fn):
+        best = float("inf")
+        for _ in range(reps):
+            ctx.set_velocity(u0)
+            ctx.synchronize()
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            out = fn()
+            b.record(stream)
+            torch.cuda.synchronize()
+            best = min(best, a.elapsed_time(b))
+        return best, out
+
+    def forward():
+        ctx.run(1, N)
+        ctx.synchronize()
+
+    ms_fwd, _ = timed(forward)
+    ms_sweep, _ = timed(lambda: ctx.adjoint_run(N, KC, gradient=False))
+    ms_grad, (J0, gu, gb) = timed(lambda: ctx.adjoint_run(N, KC))
+    # central-difference spot check (4th order) along a velocity and a control direction
+    du = np.stack(divergence_free_field(mesh, params, seed=seed + 2, amp=0.05, kmax=8), axis=-1)
+    du[mesh.NZS, :, 0, 0] = np.random.default_rng(seed + 3).standard_normal(mesh.NYS + 1) * 0.3
+    dc = blowing_suction(mesh, seed + 4)
+    errs = []
+    for d_u, d_c, h in ((du, 0.0 * bc0, 1e-2), (0.0 * u0, dc, 1e-4)):
+        def J(t):
+            ctx.set_velocity(u0 + t * d_u)
+            return ctx.adjoint_run(N, KC, control=bc0 + t * d_c, gradient=False)[0]
+        fd = (J(-2 * h) - 8 * J(-h) + 8 * J(h) - J(2 * h)) / (12 * h)
+        ad = float(np.sum(np.real(np.conj(gu) * d_u)) + np.sum(np.real(np.conj(gb) * d_c)))
+        errs.append(abs(fd - ad) / abs(ad))
+    out = {"workload": "adjoint_64x65x64_retau180_wall_shear_50_steps_checkpoint_10",
+           "steps": N, "checkpoint_interval": KC, "objective": J0,
+           "forward_ms": ms_fwd, "gradient_ms": ms_grad, "forward_sweep_ms": ms_sweep,
+           "cost_ratio": ms_grad / ms_fwd, "reverse_ratio": (ms_grad - ms_sweep) / ms_fwd,
+           "fd_rel_err": errs, "device_bytes": ctx.device_bytes(),
+           "note": "cost_ratio = gradient run (forward sweep + recomputation + reverse steps) / forward run; "
+                   "reverse_ratio excludes the forward sweep"}
+    ctx.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -277,6 +343,7 @@ def main():
     ap.add_argument("--no-ensemble", action="store_true", help="skip the ensemble-batch arm")
     ap.add_argument("--ensemble-members", type=int, default=64)
     ap.add_argument("--ensemble-steps", type=int, default=200)
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the discrete-adjoint arm")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -398,6 +465,11 @@ def main():
             ensemble[label] = run_ensemble(args.ensemble_members, args.ensemble_steps, W, prec, local,
                                            1000 + rank)
 
+    # ---- discrete-adjoint arm: gradient cost against the forward run ------
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = run_adjoint(local, 2000 + rank)
+
     # ---- end to end through the C ABI with host buffers -------------------
     KE = args.e2e_steps or min(K, 200)
     ctx2 = cdns.Context(mesh, params, device=local)
@@ -457,6 +529,7 @@ def main():
             "cpu_baseline": cpu,
             "mixed": mixed,
             "ensemble": ensemble,
+            "adjoint": adjoint,
             "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": KE, "finite": finite,
                     "protocol": "upload + steps 1..K one call each with dpdx readback + download"},

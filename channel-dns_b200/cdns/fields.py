@@ -129,3 +129,24 @@ def divergence_free_field(mesh, params, seed: int, amp: float, kmax: int | None 
     a[1] -= 0.5 * (top - bot)
     ux[zk, :, 0] = a
     return [ux, uy, uz]
+
+
+def blowing_suction(mesh, seed: int, kmax: int = 8, amp: float = 1.0) -> np.ndarray:
+    """Seeded wall blowing/suction in the velocity wall-data layout
+    [2 NZS+1][2][NXS+1][3]: wall-normal velocity of the Fourier modes
+    kx <= kmax, |kz| <= kmax (mean mode excluded) at both walls, standard
+    normal real and imaginary parts times ``amp``, Hermitian in kz at kx = 0
+    (a real wall velocity)."""
+    rng = np.random.default_rng(seed)
+    nkz, nkx = 2 * mesh.NZS + 1, mesh.NXS + 1
+    bc = np.zeros((nkz, 2, nkx, 3), dtype=np.complex128)
+    zk = mesh.NZS
+    for w in range(2):
+        for kx in range(0, min(kmax, mesh.NXS) + 1):
+            for kz in range(-min(kmax, mesh.NZS), min(kmax, mesh.NZS) + 1):
+                if kx == 0 and kz <= 0:
+                    continue
+                bc[zk + kz, w, kx, 1] = complex(rng.standard_normal(), rng.standard_normal())
+                if kx == 0:
+                    bc[zk - kz, w, kx, 1] = np.conj(bc[zk + kz, w, kx, 1])
+    return bc * amp

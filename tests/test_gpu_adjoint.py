@@ -33,21 +33,9 @@ def crandom(rng, shape):
 
 
 def wall_control(m, seed, kmax=8, amp=1.0):
-    """Wall-normal blowing/suction at both walls, Fourier modes |kx|, |kz| <= kmax
-    (zero mode excluded), Hermitian in kz at kx = 0: [nkz][2][nkx][3]."""
-    rng = np.random.default_rng(seed)
-    nkz, _, nkx = m.spectral_shape()
-    bc = np.zeros((nkz, 2, nkx, 3), dtype=np.complex128)
-    zk = m.NZS
-    for w in range(2):
-        for kx in range(0, min(kmax, m.NXS) + 1):
-            for kz in range(-min(kmax, m.NZS), min(kmax, m.NZS) + 1):
-                if kx == 0 and kz <= 0:
-                    continue
-                bc[zk + kz, w, kx, 1] = complex(rng.standard_normal(), rng.standard_normal())
-                if kx == 0:
-                    bc[zk - kz, w, kx, 1] = np.conj(bc[zk + kz, w, kx, 1])
-    return bc * amp
+    """Wall-normal blowing/suction of the |k| <= kmax modes at both walls."""
+    from cdns.fields import blowing_suction
+    return blowing_suction(m, seed, kmax=kmax, amp=amp)
 
 
 @pytest.mark.parametrize("n", [32, 64])
