@@ -212,6 +212,140 @@ def fine_forward(m: Mesh, P: np.ndarray) -> np.ndarray:
 
 
 # --------------------------------------------------------------------------
+# Coarse-grid transform (src/fft/transforms.cpp:452-582): physical
+# [NZ][NY+1][NX], full spectra allowed (NXS = NX/2, NZS = NZ/2) with the
+# Nyquist halve/mirror convention.
+# --------------------------------------------------------------------------
+def coarse_backward(m: Mesh, U: np.ndarray) -> np.ndarray:
+    """Spectral [nkz][ncy][nkx] -> coarse physical [NZ][NY+1][NX].
+
+    y: copy NYS+1 coefficients, zero-pad to NY+1, double c_0, DCT-I
+    (:536-552); z: expand into NZ slots scaled by 0.5, at a full z spectrum the
+    Nyquist slot is 0.5 (K(NZH) + K(-NZH)) (:560-572), backward c2c; a full
+    x spectrum doubles the Nyquist bin (:574-576); x: c2r over NX (:580).
+    """
+    nkz, ncy, nkx = m.spectral_shape()
+    assert U.shape == (nkz, ncy, nkx)
+    NX, NY, NZ = m.NX, m.NY, m.NZ
+    NZH, NXH = NZ // 2, NX // 2
+    fullz, fullx = m.NZS == NZH, m.NXS == NXH
+    Y = np.zeros((nkz, NY + 1, nkx), dtype=np.complex128)
+    Y[:, :ncy, :] = U
+    Y[:, 0, :] = Y[:, 0, :] + Y[:, 0, :]
+    Y = sfft.dct(Y.real, type=1, axis=1) + 1j * sfft.dct(Y.imag, type=1, axis=1)
+    X = np.zeros((NZ, NY + 1, NX // 2 + 1), dtype=np.complex128)
+    for iz in range(NZ):
+        if iz <= m.NZS or iz >= NZ - m.NZS:
+            kz = iz if iz <= m.NZS else iz - NZ
+            X[iz, :, :nkx] = Y[kz + m.NZS] * 0.5
+            if fullz and iz == NZH:
+                X[iz, :, :nkx] = Y[NZH + m.NZS] * 0.5 + Y[-NZH + m.NZS] * 0.5
+    X = np.fft.ifft(X, axis=0) * NZ
+    if fullx:
+        X[:, :, NXH] *= 2.0
+    return np.fft.irfft(X, n=NX, axis=2) * NX
+
+
+def coarse_forward(m: Mesh, P: np.ndarray) -> np.ndarray:
+    """Coarse physical [NZ][NY+1][NX] -> spectral [nkz][ncy][nkx].
+
+    x r2c, x1/NX on kx <= NXS and x0.5 on a full-spectrum Nyquist bin
+    (:480-496); z forward c2c, x1/NZ, a full-spectrum Nyquist halved and
+    mirrored to -NZH (:498-512); DCT-I, x1/(2 NY) at j = 0 and 1/NY for
+    j >= 1, keep j <= NYS (:518-529).
+    """
+    NX, NY, NZ = m.NX, m.NY, m.NZ
+    assert P.shape == (NZ, NY + 1, NX)
+    NZH, NXH = NZ // 2, NX // 2
+    fullz, fullx = m.NZS == NZH, m.NXS == NXH
+    nxs1 = m.NXS + 1
+    X = np.fft.rfft(P, axis=2)[:, :, :nxs1] * (1.0 / NX)
+    if fullx:
+        X[:, :, NXH] *= 0.5
+    Z = np.fft.fft(X, axis=0)
+    invnz = 1.0 / NZ
+    K = np.zeros((m.nkz, NY + 1, nxs1), dtype=np.complex128)
+    for kz in range(0, m.NZS + 1):
+        K[kz + m.NZS] = Z[kz] * invnz
+    for kz in range(-m.NZS, 0):
+        K[kz + m.NZS] = Z[NZ + kz] * invnz
+    if fullz:
+        K[NZH + m.NZS] = Z[NZH] * invnz * 0.5
+        K[-NZH + m.NZS] = K[NZH + m.NZS]
+    Y = sfft.dct(K.real, type=1, axis=1) + 1j * sfft.dct(K.imag, type=1, axis=1)
+    out = np.empty((m.nkz, m.ncy, nxs1), dtype=np.complex128)
+    out[:, 0, :] = Y[:, 0, :] * (1.0 / (2.0 * NY))
+    out[:, 1:, :] = Y[:, 1:m.ncy, :] * (1.0 / NY)
+    return out
+
+
+# --------------------------------------------------------------------------
+# Output reduction: FieldIO::to_physical (src/io/field_io.cpp:199-220),
+# Statistics::reduce (src/sim/statistics.cpp:55-110) and
+# Diagnostics::evaluate (src/sim/diagnostics.cpp:14-80).
+# --------------------------------------------------------------------------
+def to_physical(m: Mesh, velocity, pressure):
+    """Four coarse backward transforms: (u, v, w) and p on [NZ][NY+1][NX]."""
+    return [coarse_backward(m, np.asarray(v)) for v in velocity], coarse_backward(m, np.asarray(pressure))
+
+
+def plane_moments(velocity_phys, pressure_phys, higher: bool = True) -> np.ndarray:
+    """Per-plane sums [NY+1][20] in PlaneMoments order (statistics.cpp:58-86):
+    u, v, w, p, uu, vv, ww, uv, vw, wu, pu, pv, pw, pp, uuu, vvv, www, uuuu,
+    vvvv, wwww, with p = raw p - 0.5 (uu + vv + ww).  Sums over (z, x)."""
+    u, v, w = velocity_phys
+    p = pressure_phys - 0.5 * (u * u + v * v + w * w)
+    terms = [u, v, w, p, u * u, v * v, w * w]
+    if higher:
+        terms += [u * v, v * w, w * u, p * u, p * v, p * w, p * p,
+                  u * u * u, v * v * v, w * w * w, u * u * u * u, v * v * v * v, w * w * w * w]
+    out = np.zeros((u.shape[1], 20))
+    for k, t in enumerate(terms):
+        out[:, k] = t.sum(axis=(0, 2))
+    return out
+
+
+def clenshaw_curtis_weights(NY: int) -> np.ndarray:
+    """Clenshaw-Curtis weights on the NY+1 Gauss-Lobatto points, divided by
+    the channel height 2 (diagnostics.cpp:18-36)."""
+    n = NY
+    w = np.zeros(n + 1)
+    for j in range(n + 1):
+        th = PI * j / n
+        if j == 0 or j == n:
+            wt = 1.0 / (n * n - (1.0 if n % 2 == 0 else 0.0))
+        else:
+            val = 1.0
+            for k in range(1, (n - 1) // 2 + 1):
+                val -= 2.0 * math.cos(2 * k * th) / (4.0 * k * k - 1.0)
+            if n % 2 == 0:
+                val -= math.cos(n * th) / (n * n - 1.0)
+            wt = 2.0 * val / n
+        w[j] = wt / 2.0
+    return w
+
+
+def diagnostics(m: Mesh, c: Constants, planes: np.ndarray, velocity) -> Tuple[float, float, float]:
+    """(EKT, TKE, divergence L2) of Diagnostics::evaluate (diagnostics.cpp:38-80):
+    EKT = sum v^2 over the grid nodes, TKE = sum_y 0.5 w_y sum_c var_c, div L2
+    = sqrt(sum_y w_y mean_xz(div^2)) with div from the coarse transform of the
+    spectral divergence."""
+    wts = clenshaw_curtis_weights(m.NY)
+    inv_plane = 1.0 / (m.NX * m.NZ)
+    div = coarse_backward(m, divergence(c, velocity))
+    ekt = float(planes[:, 5].sum())
+    tke = 0.0
+    for iy in range(m.NY + 1):
+        var = 0.0
+        for k in range(3):
+            mean = planes[iy, k] * inv_plane
+            var += max(0.0, planes[iy, 4 + k] * inv_plane - mean * mean)
+        tke += 0.5 * wts[iy] * var
+    div_sq = float(np.sum(wts[None, :, None] * inv_plane * div * div))
+    return ekt, tke, math.sqrt(div_sq)
+
+
+# --------------------------------------------------------------------------
 # Spectral operators (src/solver/vector_ops.cpp)
 # Vector fields are tuples/lists of 3 arrays [nkz][ncy][nkx].
 # --------------------------------------------------------------------------

@@ -154,6 +154,44 @@ def fine(m, p, spectral):
     return phys, back
 
 
+def coarse(m, p, spectral):
+    """Reference coarse transform 'B' then 'F' (physical [NZ][NY+1][NX], spectral)."""
+    d = tempfile.mkdtemp(prefix="cdns_ref_")
+    write_config(d, m, p, 1)
+    inp = os.path.join(d, "s.bin")
+    np.asarray(spectral, dtype="<c16").tofile(inp)
+    out = os.path.join(d, "c.bin")
+    subprocess.run([RUNNER, "coarse", d, inp, out], check=True, capture_output=True)
+    raw = open(out, "rb").read()
+    nphys = m.NZ * (m.NY + 1) * m.NX
+    phys = np.frombuffer(raw[: 8 * nphys], dtype="<f8").reshape(m.NZ, m.NY + 1, m.NX).copy()
+    back = np.frombuffer(raw[8 * nphys:], dtype="<c16").reshape(m.spectral_shape()).copy()
+    _rmtree(d)
+    return phys, back
+
+
+def reduce(m, p, velocity, pressure):
+    """Reference output branch on a state: physical (u, v, w, p), plane sums
+    [NY+1][20], plane finite flags, (EKT, TKE, div_L2, finite)."""
+    d = tempfile.mkdtemp(prefix="cdns_ref_")
+    write_config(d, m, p, 1)
+    inp = os.path.join(d, "st.bin")
+    with open(inp, "wb") as fh:
+        fh.write(np.stack(velocity, axis=-1).astype("<c16").tobytes())
+        fh.write(np.asarray(pressure).astype("<c16").tobytes())
+    out = os.path.join(d, "r.bin")
+    subprocess.run([RUNNER, "reduce", d, inp, out], check=True, capture_output=True)
+    raw = np.frombuffer(open(out, "rb").read(), dtype="<f8")
+    nphys = m.NZ * (m.NY + 1) * m.NX
+    ny1 = m.NY + 1
+    phys = raw[: 4 * nphys].reshape(4, m.NZ, ny1, m.NX).copy()
+    planes = raw[4 * nphys: 4 * nphys + 20 * ny1].reshape(ny1, 20).copy()
+    flags = raw[4 * nphys + 20 * ny1: 4 * nphys + 21 * ny1].copy()
+    values = raw[4 * nphys + 21 * ny1:].copy()
+    _rmtree(d)
+    return phys, planes, flags, values
+
+
 def solve(m, p, g, rhs_v, bc_p, bc_v):
     d = tempfile.mkdtemp(prefix="cdns_ref_")
     write_config(d, m, p, 1)

@@ -13,6 +13,15 @@
 //   ref_runner fine <run-dir> <spectral.bin> <out.bin>
 //       Transforms::channel_xyzfft2 'B' then 'F' of one scalar field
 //       (src/fft/transforms.cpp:615-741): writes physical then spectral.
+//   ref_runner coarse <run-dir> <spectral.bin> <out.bin>
+//       Transforms::channel_xyzfft 'B' then 'F' of one scalar field
+//       (src/fft/transforms.cpp:452-582): writes physical then spectral.
+//   ref_runner reduce <run-dir> <state.bin> <out.bin>
+//       The output branch of Simulation::run (src/sim/simulation.cpp:226-235)
+//       on a given velocity [kz][y][kx][3] and pressure [kz][y][kx]:
+//       FieldIO::to_physical, Statistics::reduce(higher, validate) and
+//       Diagnostics::evaluate; writes the physical u, v, w, p, the plane sums
+//       [NY+1][20], the plane finite flags and (EKT, TKE, div_L2, finite).
 //   ref_runner solve <run-dir> <g> <rhs.bin> <out.bin>
 //       EqSolvePV::setup(g) then the fused solve_modes with fused RHS and
 //       sigma correction (src/solver/eqsolve_pv.cpp:311-450); input is the
@@ -32,7 +41,10 @@
 #include "core/mpi_context.hpp"
 #include "core/params.hpp"
 #include "fft/transforms.hpp"
+#include "io/field_io.hpp"
+#include "sim/diagnostics.hpp"
 #include "sim/simulation.hpp"
+#include "sim/statistics.hpp"
 #include "solver/eqsolve_pv.hpp"
 #include "solver/fields.hpp"
 #include "solver/timestepper.hpp"
@@ -69,7 +81,7 @@ void fill(Array4D<std::complex<double>> &f, const std::complex<double> *src) {
 
 int main(int argc, char **argv) {
     if (argc < 4) {
-        std::cerr << "usage: ref_runner run|nonlinear|fine|solve <run-dir> ...\n";
+        std::cerr << "usage: ref_runner run|nonlinear|fine|coarse|reduce|solve <run-dir> ...\n";
         return 2;
     }
     const std::string mode = argv[1];
@@ -126,6 +138,45 @@ int main(int argc, char **argv) {
             std::ofstream out(argv[4], std::ios::binary);
             write(out, phys.data(), phys.size());
             write(out, back.data(), back.size());
+            return out ? 0 : 1;
+        }
+        if (mode == "coarse" && argc >= 5) {
+            ScalarField spec = make_scalar_field(mesh), back = make_scalar_field(mesh);
+            std::vector<std::complex<double>> buf(spec.size());
+            read_all(argv[3], buf);
+            fill(spec, buf.data());
+            std::vector<double> phys(static_cast<std::size_t>(mesh.NZ) * (mesh.NYP + 1) * mesh.NX);
+            fft.channel_xyzfft('B', phys.data(), spec.data());
+            fft.channel_xyzfft('F', phys.data(), back.data());
+            std::ofstream out(argv[4], std::ios::binary);
+            write(out, phys.data(), phys.size());
+            write(out, back.data(), back.size());
+            return out ? 0 : 1;
+        }
+        if (mode == "reduce" && argc >= 5) {
+            VectorField velocity = make_vector_field(mesh);
+            ScalarField pressure = make_scalar_field(mesh);
+            std::vector<std::complex<double>> buf(velocity.size() + pressure.size());
+            read_all(argv[3], buf);
+            fill(velocity, buf.data());
+            fill(pressure, buf.data() + velocity.size());
+            FieldIO io(mesh, fft, dir, &mpi);
+            bool finite = true;
+            const auto &snapshot = io.to_physical(velocity, pressure, &finite);
+            Statistics stats(mesh);
+            const auto &planes = stats.reduce(snapshot.velocity, snapshot.pressure, true, true);
+            Diagnostics diag(mesh, fft, &mpi);
+            const auto values = diag.evaluate(planes, velocity, finite);
+            std::ofstream out(argv[4], std::ios::binary);
+            for (int c = 0; c < 3; ++c) write(out, snapshot.velocity[c].data(), snapshot.velocity[c].size());
+            write(out, snapshot.pressure.data(), snapshot.pressure.size());
+            for (const auto &pl : planes) write(out, pl.sum.data(), pl.sum.size());
+            for (const auto &pl : planes) {
+                const double f = pl.finite ? 1.0 : 0.0;
+                write(out, &f, 1);
+            }
+            const double v[4] = {values.ekt, values.tke, values.divergence_l2, values.finite ? 1.0 : 0.0};
+            write(out, v, 4);
             return out ? 0 : 1;
         }
         if (mode == "solve" && argc >= 6) {

@@ -16,8 +16,15 @@ on small seeded inputs and stores inputs and outputs as compressed npz files:
                         random wall data (NXS=5: a ragged x extent).
   golden_fine.npz       fine-grid backward/forward transforms of a band
                         spectrum on a 3/2 product grid.
+  golden_coarse.npz     coarse-grid backward/forward transforms on a full
+                        spectrum (Nyquist halve/mirror branches, 16x17x16)
+                        and a ragged one (NXS=5, NZS=6): a realisable and an
+                        arbitrary spectrum each.
+  golden_reduce.npz     the output branch on a 16x17x16 state: physical
+                        u, v, w, p, plane sums, finite flags, EKT/TKE/div_L2.
 
-Usage: python tests/golden/make_golden.py   (needs oracle/_ref built)
+Usage: python tests/golden/make_golden.py [name ...]   (needs oracle/_ref built;
+names: step example nonlinear solve fine coarse reduce, default all)
 """
 import os
 import sys
@@ -39,9 +46,39 @@ def mesh_dict(m, p):
                                p.INDEX_GRAD_PRE, p.THETA, p.DT, p.V_Microblow0]))
 
 
-def main():
+def coarse_and_reduce(which):
+    if "coarse" in which:
+        out = {}
+        for tag, (m, p) in (("full", channel_case(16)),
+                            ("ragged", example_case(NXS=5, NYS=14, NZS=6, N2=16, N=16))):
+            rng = np.random.default_rng(51)
+            realisable = orc.coarse_forward(m, rng.standard_normal((m.NZ, m.NY + 1, m.NX)))
+            sh = m.spectral_shape()
+            arbitrary = rng.standard_normal(sh) + 1j * rng.standard_normal(sh)
+            for kind, U in (("real", realisable), ("arb", arbitrary)):
+                phys, back = ref_io.coarse(m, p, U)
+                out[f"{tag}_{kind}_U"], out[f"{tag}_{kind}_phys"], out[f"{tag}_{kind}_back"] = U, phys, back
+            out[f"{tag}_mesh"] = mesh_dict(m, p)["mesh"]
+            out[f"{tag}_dom"] = mesh_dict(m, p)["dom"]
+            out[f"{tag}_parm"] = mesh_dict(m, p)["parm"]
+        np.savez_compressed(os.path.join(HERE, "golden_coarse.npz"), **out)
+    if "reduce" in which:
+        m, p = channel_case(16)
+        u = divergence_free_field(m, p, seed=61, amp=0.1, spectrum="k53", mean="loglaw")
+        rng = np.random.default_rng(62)
+        pres = orc.coarse_forward(m, rng.standard_normal((m.NZ, m.NY + 1, m.NX)))
+        phys, planes, flags, values = ref_io.reduce(m, p, u, pres)
+        np.savez_compressed(os.path.join(HERE, "golden_reduce.npz"), **mesh_dict(m, p), u=np.stack(u),
+                            p=pres, phys=phys, planes=planes, flags=flags, values=values)
+
+
+def main(which):
     if not ref_io.available():
         raise SystemExit("oracle/_ref is not built: run make -C oracle")
+    coarse_and_reduce(which)
+    if "step" not in which:
+        print("golden fixtures written to", HERE)
+        return
     # 1. small channel, 4 steps
     m, p = channel_case(16)
     u0 = divergence_free_field(m, p, seed=11, amp=0.05, kmax=4)
@@ -92,4 +129,4 @@ def _cheb_1my2(ncy):
 
 
 if __name__ == "__main__":
-    main()
+    main(set(sys.argv[1:]) or {"step", "example", "nonlinear", "solve", "fine", "coarse", "reduce"})

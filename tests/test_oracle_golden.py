@@ -1,9 +1,11 @@
 """The oracle against golden vectors produced by the reference's own sources
 (tests/golden/make_golden.py).  CPU only."""
+import os
+
 import numpy as np
 import pytest
 
-from golden_io import load
+from golden_io import GOLDEN, load
 from oracle_cases import orc
 
 
@@ -51,3 +53,50 @@ def test_oracle_fine_transforms_match_reference():
     phys = orc.fine_backward(m, d["U"])
     assert np.abs(phys - d["phys"]).max() <= 1e-13 * np.abs(d["phys"]).max()
     assert np.abs(orc.fine_forward(m, d["phys"]) - d["back"]).max() <= 1e-13
+
+
+def plane_sum_scale(vp, pp):
+    """Per-plane sums of the absolute values of the 20 moment terms (the
+    round-off scale of sums that cancel, e.g. the plane mean of v)."""
+    a = [np.abs(x) for x in vp]
+    ap = np.abs(pp) + 0.5 * (a[0] ** 2 + a[1] ** 2 + a[2] ** 2)
+    return orc.plane_moments(a, ap + 0.5 * (a[0] ** 2 + a[1] ** 2 + a[2] ** 2)) + 1e-300
+
+
+def _coarse_case(d, tag):
+    mm = [int(v) for v in d[f"{tag}_mesh"]]
+    m = orc.Mesh(*mm, float(d[f"{tag}_dom"][0]), float(d[f"{tag}_dom"][1]))
+    return m
+
+
+@pytest.mark.parametrize("tag", ["full", "ragged"])
+@pytest.mark.parametrize("kind", ["real", "arb"])
+def test_oracle_coarse_transforms_match_reference(tag, kind):
+    """Transforms::channel_xyzfft 'B'/'F' (src/fft/transforms.cpp:452-582),
+    full spectrum (Nyquist halve/mirror) and ragged, realisable and arbitrary."""
+    d = dict(np.load(os.path.join(GOLDEN, "golden_coarse.npz")))
+    m = _coarse_case(d, tag)
+    U, phys, back = d[f"{tag}_{kind}_U"], d[f"{tag}_{kind}_phys"], d[f"{tag}_{kind}_back"]
+    assert _rel_max(orc.coarse_backward(m, U), phys) <= 1e-14
+    assert _rel_max(orc.coarse_forward(m, phys), back) <= 1e-14
+
+
+def test_oracle_output_reduction_matches_reference():
+    """FieldIO::to_physical + Statistics::reduce + Diagnostics::evaluate
+    (src/io/field_io.cpp:199-220, src/sim/statistics.cpp:55-110,
+    src/sim/diagnostics.cpp:14-80) on a 16x17x16 state."""
+    m, p, d = load("golden_reduce.npz")
+    u = list(d["u"])
+    vp, pp = orc.to_physical(m, u, d["p"])
+    for k in range(3):
+        assert _rel_max(vp[k], d["phys"][k]) <= 1e-14
+    assert _rel_max(pp, d["phys"][3]) <= 1e-14
+    planes = orc.plane_moments(vp, pp)
+    ref = d["planes"]
+    scale = plane_sum_scale(vp, pp)
+    assert np.all(np.abs(planes - ref) <= 1e-13 * scale)
+    assert np.all(d["flags"] == 1.0)
+    ekt, tke, div = orc.diagnostics(m, orc.make_constants(m, p.Re), ref, u)
+    v = d["values"]
+    assert abs(ekt - v[0]) <= 1e-14 * v[0] and abs(tke - v[1]) <= 1e-13 * v[1]
+    assert abs(div - v[2]) <= 1e-12 * max(v[2], 1e-300) + 1e-16 and v[3] == 1.0
