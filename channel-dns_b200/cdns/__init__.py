@@ -56,6 +56,9 @@ _SIGNATURES = {
     "cdns_get_velocity": [ctypes.c_void_p, ctypes.c_void_p],
     "cdns_get_pressure": [ctypes.c_void_p, ctypes.c_void_p],
     "cdns_set_velocity_bc": [ctypes.c_void_p, ctypes.c_void_p],
+    "cdns_set_pressure": [ctypes.c_void_p, ctypes.c_void_p],
+    "cdns_transform_coarse": [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
+    "cdns_output_reduce": [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
     "cdns_set_velocity_device": [ctypes.c_void_p, ctypes.c_void_p],
     "cdns_get_velocity_device": [ctypes.c_void_p, ctypes.c_void_p],
     "cdns_step": [ctypes.c_void_p, ctypes.c_int],
@@ -323,6 +326,38 @@ class Context:
         _check(lib().cdns_solve(self._h, g, _ptr(rhs), _ptr(pbc), _ptr(vbc), _ptr(p), _ptr(v),
                                 _ptr(units)))
         return p, v, units[:ncy].copy(), units[ncy:].copy()
+
+    def set_pressure(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, dtype=np.complex128)
+        _check(lib().cdns_set_pressure(self._h, _ptr(p)))
+
+    # ---- coarse grid and output reduction ----
+    def transform_coarse(self, direction: str, data: np.ndarray) -> np.ndarray:
+        """Transforms::channel_xyzfft of one scalar field: 'B' spectral ->
+        physical [NZ][NY+1][NX], 'F' the inverse."""
+        m = self.mesh
+        if direction == "B":
+            src = np.ascontiguousarray(data, dtype=np.complex128)
+            out = np.empty((m.NZ, m.NY + 1, m.NX))
+        else:
+            src = np.ascontiguousarray(data, dtype=np.float64)
+            out = np.empty(m.spectral_shape, dtype=np.complex128)
+        _check(lib().cdns_transform_coarse(self._h, ord(direction), _ptr(src), _ptr(out)))
+        return out
+
+    def output_reduce(self, higher_moments: bool = True, snapshot: bool = False):
+        """The output branch on the device: plane sums [NY+1][20], diagnostics
+        (EKT, TKE, divergence L2, finite) and, with snapshot=True, the physical
+        u, v, w, p [4][NZ][NY+1][NX]."""
+        m = self.mesh
+        planes = np.empty((m.NY + 1, 20))
+        diag = np.empty(4)
+        phys = np.empty((4, m.NZ, m.NY + 1, m.NX)) if snapshot else None
+        _check(lib().cdns_output_reduce(self._h, int(higher_moments), _ptr(planes), _ptr(diag),
+                                        None if phys is None else _ptr(phys)))
+        values = {"ekt": float(diag[0]), "tke": float(diag[1]), "divergence_l2": float(diag[2]),
+                  "finite": bool(diag[3] == 1.0)}
+        return planes, values, phys
 
     # ---- discrete adjoint ----
     def adjoint_run(self, nsteps: int, checkpoint_interval: int, control: Optional[np.ndarray] = None,

@@ -35,14 +35,16 @@ void launch_yanalysis_scaled(const Dims &d, const double *cana, const double2 *F
 
 // ---- transforms.cu ----
 cudaError_t configure_transform_kernels(const Dims &d);
+// coarse = true: the coarse-grid conventions of a full spectrum's Nyquist
+// modes (channel_xyzfft) instead of the fine grid's (channel_xyzfft2).
 void launch_z_backward(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *F,
-                       double2 *G, int nf, cudaStream_t s);
+                       double2 *G, int nf, cudaStream_t s, bool coarse = false);
 void launch_x_cross(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G,
                     double2 *H, cudaStream_t s);
 void launch_z_forward(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *H,
-                      double2 *F, int nf, cudaStream_t s);
+                      double2 *F, int nf, cudaStream_t s, bool coarse = false);
 void launch_x_c2r(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G,
-                  double *phys, cudaStream_t s);
+                  double *phys, cudaStream_t s, bool coarse = false);
 // FP32 stage buffers (mixed precision); only meshes with register_forms(d)
 bool register_forms(const Dims &d);
 void launch_z_backward(const Dims &d, const double2 *roots, const float2 *F, float2 *G, int nf, cudaStream_t s);
@@ -51,7 +53,13 @@ void launch_x_cross(const Dims &d, const double2 *roots, const float2 *G, float2
                     cudaStream_t s);
 void launch_z_forward(const Dims &d, const double2 *roots, const float2 *H, float2 *F, int nf, cudaStream_t s);
 void launch_x_r2c(const Dims &d, const FftPlan &P, const double2 *roots, const double *phys,
-                  double2 *H, cudaStream_t s);
+                  double2 *H, cudaStream_t s, bool coarse = false);
+// Output reduction, x stage on the coarse grid (Dims of the coarse grid):
+// c2r of G[5] (u, v, w, p, div), per-point moments summed per block into
+// partial[NY+1][moment_blocks][22]; phys (may be null) receives u, v, w, p.
+int moment_blocks(const Dims &d);
+void launch_x_moments(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G, double *partial,
+                      double *phys, cudaStream_t s);
 // Transpose of x_cross about the forward fields G[6]: L[0..2] = lH in, L[0..5] = lG out.
 void launch_x_adjoint(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G, double2 *L,
                       cudaStream_t s);

@@ -33,10 +33,11 @@ int record_error(int code, const char *msg) {
 }  // namespace cdns
 
 namespace {
-
 const char *kStageNames[kStages] = {"curl", "y_synthesis", "z_backward", "x_cross",
                                     "z_forward", "y_analysis", "solve"};
+}  // namespace
 
+namespace cdns {
 bool plan_fft(int n, FftPlan &p) {
     p.n = n;
     p.nrad = 0;
@@ -56,7 +57,7 @@ bool plan_fft(int n, FftPlan &p) {
     }
     return true;
 }
-}  // namespace
+}  // namespace cdns
 
 
 namespace {
@@ -219,6 +220,7 @@ int cdns_create(const cdns_mesh_desc *m, const cdns_params *p, int precision, in
     cdns_ctx *c = new (std::nothrow) cdns_ctx();
     if (!c) return fail(CDNS_ERR_NOMEM, "host allocation failed");
     c->device = device;
+    c->mesh = *m;
     Dims &d = c->d;
     d.NX2 = m->NX2; d.NY2 = m->NY2; d.NZ2 = m->NZ2;
     d.NXS = m->NXS; d.NYS = m->NYS; d.NZS = m->NZS;
@@ -365,6 +367,7 @@ int cdns_destroy(cdns_ctx *c) {
         if (g) cudaGraphExecDestroy(g);
     for (auto ev : c->ev) cudaEventDestroy(ev);
     adjoint_release(c->adj);
+    output_release(c->outw);
     for (void *p : c->allocs) cudaFree(p);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -420,6 +423,14 @@ int cdns_get_pressure(cdns_ctx *c, double *p) {
     if (!c || !p) return fail(CDNS_ERR_ARG, "null argument");
     DeviceGuard guard(c->device);
     CK(cudaMemcpyAsync(p, c->p, sizeof(double2) * c->d.Ns, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return CDNS_OK;
+}
+
+int cdns_set_pressure(cdns_ctx *c, const double *p) {
+    if (!c || !p) return fail(CDNS_ERR_ARG, "null argument");
+    DeviceGuard guard(c->device);
+    CK(cudaMemcpyAsync(c->p, p, sizeof(double2) * c->d.Ns, cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return CDNS_OK;
 }
@@ -692,7 +703,7 @@ int cdns_get_stream(cdns_ctx *c, void **stream) {
 
 int cdns_device_bytes(cdns_ctx *c, size_t *b) {
     if (!c || !b) return fail(CDNS_ERR_ARG, "null argument");
-    *b = c->bytes + adjoint_bytes(c->adj);
+    *b = c->bytes + adjoint_bytes(c->adj) + output_bytes(c->outw);
     return CDNS_OK;
 }
 

@@ -22,6 +22,11 @@ constexpr int kMaxProfSteps = 256;
 struct AdjointWork;   // adjoint_run.cu
 void adjoint_release(AdjointWork *w);
 size_t adjoint_bytes(const AdjointWork *w);
+struct OutputWork;    // output.cu
+void output_release(OutputWork *w);
+size_t output_bytes(const OutputWork *w);
+// Radix plan of a length-n Stockham FFT (false if n has a prime factor > 13).
+bool plan_fft(int n, FftPlan &p);
 
 }  // namespace cdns
 
@@ -35,6 +40,7 @@ size_t adjoint_bytes(const AdjointWork *w);
 struct cdns_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cdns_mesh_desc mesh{};
     cdns::Dims d{};
     cdns::Tables t{};
     cdns::FftPlan px{}, pz{};
@@ -63,6 +69,7 @@ struct cdns_ctx {
     int prof_steps = 0;
     std::vector<cudaEvent_t> ev;
     cdns::AdjointWork *adj = nullptr;     // discrete-adjoint workspace, made on first use
+    cdns::OutputWork *outw = nullptr;     // coarse-grid output workspace, made on first use
 
     template <typename T> int alloc(T *&ptr, size_t count) {
         void *p = nullptr;

@@ -24,16 +24,28 @@ namespace cdns {
 // HBM into the NZ2 slots (negative Nyquist slot wins at a full z spectrum,
 // src/fft/transforms.cpp:715-732); the last pass writes z-physical rows.
 // ---------------------------------------------------------------------------
+// The coarse-grid transform (coarse = true, src/fft/transforms.cpp:560-572)
+// instead sums the two Nyquist coefficients into the shared slot.
 template <class C> struct ZExpandSrc {
     const C *Fp;   // one (field, y point) plane [kz][kx]
     int nkx, kx0, NZS, n;
+    bool coarse;
     __device__ __forceinline__ C operator()(int z, int line) const {
         const int kx = kx0 + line;
         if (kx >= nkx) return mkc<C>(0, 0);
         int kz;
-        if (z <= NZS) kz = (z == n - NZS) ? -NZS : z;
-        else if (z >= n - NZS) kz = z - n;
-        else return mkc<C>(0, 0);
+        if (z <= NZS) {
+            if (z == n - NZS) {
+                if (coarse) return cadd(Fp[(2 * NZS) * nkx + kx], Fp[kx]);
+                kz = -NZS;
+            } else {
+                kz = z;
+            }
+        } else if (z >= n - NZS) {
+            kz = z - n;
+        } else {
+            return mkc<C>(0, 0);
+        }
         return Fp[(kz + NZS) * nkx + kx];
     }
 };
@@ -54,15 +66,18 @@ template <class C> struct RowSrc {
     }
 };
 // Forward z: keep kz in [-NZS, NZS] scaled by 1/NZ2 (src/fft/transforms.cpp:658-665);
-// at a full z spectrum slot NZS feeds both kz = +NZS and kz = -NZS.
+// at a full z spectrum slot NZS feeds both kz = +NZS and kz = -NZS, halved on
+// the coarse grid (coarse = true, src/fft/transforms.cpp:506-511).
 template <class C> struct ZTruncDst {
     C *Fp;
     int nkx, kx0, NZS, n;
     typename CReal<C>::T invn;
+    bool coarse;
     __device__ __forceinline__ void operator()(int z, int line, C v) const {
         const int kx = kx0 + line;
         if (kx >= nkx) return;
-        const C s = cscale(invn, v);
+        C s = cscale(invn, v);
+        if (coarse && z <= NZS && z >= n - NZS) s = cscale((typename CReal<C>::T)0.5, s);
         if (z <= NZS) Fp[(z + NZS) * nkx + kx] = s;
         if (z >= n - NZS) Fp[(z - n + NZS) * nkx + kx] = s;
     }
@@ -70,7 +85,7 @@ template <class C> struct ZTruncDst {
 
 __global__ void __launch_bounds__(256, 2)
 k_z_backward(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 *__restrict__ F,
-             double2 *__restrict__ G, int TL) {
+             double2 *__restrict__ G, int TL, bool coarse) {
     extern __shared__ double2 sm[];
     const int n = d.NZ2;
     double2 *s_root = sm;
@@ -79,14 +94,14 @@ k_z_backward(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2
     const int f = blockIdx.z, j = blockIdx.y, kx0 = blockIdx.x * TL;
     for (int i = threadIdx.x; i < n; i += blockDim.x) s_root[i] = roots[i];
     __syncthreads();
-    const ZExpandSrc<double2> src{F + ((long long)f * d.ny2 + j) * d.fcol, d.nkx, kx0, d.NZS, n};
+    const ZExpandSrc<double2> src{F + ((long long)f * d.ny2 + j) * d.fcol, d.nkx, kx0, d.NZS, n, coarse};
     const RowDst<double2> dst{G + ((long long)f * d.ny2 + j) * (long long)n * d.nkx, d.nkx, kx0};
     fft_run<+1>(a, b, TL, P, s_root, src, dst);
 }
 
 __global__ void __launch_bounds__(256, 2)
 k_z_forward(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 *__restrict__ H,
-            double2 *__restrict__ F, int TL) {
+            double2 *__restrict__ F, int TL, bool coarse) {
     extern __shared__ double2 sm[];
     const int n = d.NZ2;
     double2 *s_root = sm;
@@ -96,7 +111,8 @@ k_z_forward(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 
     for (int i = threadIdx.x; i < n; i += blockDim.x) s_root[i] = roots[i];
     __syncthreads();
     const RowSrc<double2> src{H + ((long long)f * d.ny2 + j) * (long long)n * d.nkx, d.nkx, kx0};
-    const ZTruncDst<double2> dst{F + ((long long)f * d.ny2 + j) * d.fcol, d.nkx, kx0, d.NZS, n, 1.0 / (double)n};
+    const ZTruncDst<double2> dst{F + ((long long)f * d.ny2 + j) * d.fcol, d.nkx, kx0, d.NZS, n, 1.0 / (double)n,
+                                 coarse};
     fft_run<-1>(a, b, TL, P, s_root, src, dst);
 }
 
@@ -149,20 +165,22 @@ __device__ __forceinline__ void fft2_lines(int TL, const Twiddles<C> &tw, C *S, 
 
 template <int N1, int N2, class C>
 __global__ void __launch_bounds__(16 * 17)
-k_z_backward_r(Dims d, const double2 *__restrict__ roots, const C *__restrict__ F, C *__restrict__ G, int TL) {
+k_z_backward_r(Dims d, const double2 *__restrict__ roots, const C *__restrict__ F, C *__restrict__ G, int TL,
+               bool coarse) {
     extern __shared__ double2 sm_d[];
     constexpr int n = N1 * N2;
     C *S = reinterpret_cast<C *>(sm_d + n);
     const int f = blockIdx.z, j = blockIdx.y, kx0 = blockIdx.x * TL;
     const Twiddles<C> tw = load_twiddles<C>(sm_d, roots, n);
-    const ZExpandSrc<C> src{F + ((long long)f * d.ny2 + j) * d.fcol, d.nkx, kx0, d.NZS, n};
+    const ZExpandSrc<C> src{F + ((long long)f * d.ny2 + j) * d.fcol, d.nkx, kx0, d.NZS, n, coarse};
     const RowDst<C> dst{G + ((long long)f * d.ny2 + j) * (long long)n * d.nkx, d.nkx, kx0};
     fft2_lines<N1, N2, +1>(TL, tw, S, src, dst);
 }
 
 template <int N1, int N2, class C>
 __global__ void __launch_bounds__(16 * 17)
-k_z_forward_r(Dims d, const double2 *__restrict__ roots, const C *__restrict__ H, C *__restrict__ F, int TL) {
+k_z_forward_r(Dims d, const double2 *__restrict__ roots, const C *__restrict__ H, C *__restrict__ F, int TL,
+              bool coarse) {
     extern __shared__ double2 sm_d[];
     constexpr int n = N1 * N2;
     C *S = reinterpret_cast<C *>(sm_d + n);
@@ -171,7 +189,7 @@ k_z_forward_r(Dims d, const double2 *__restrict__ roots, const C *__restrict__ H
     const RowSrc<C> src{H + ((long long)f * d.ny2 + j) * (long long)n * d.nkx, d.nkx, kx0};
     // FP32: no 1/NZ2 here (not exact in FP32); the FP64 y analysis applies 1/(NX2 NZ2)
     const ZTruncDst<C> dst{F + ((long long)f * d.ny2 + j) * d.fcol, d.nkx, kx0, d.NZS, n,
-                           (typename CReal<C>::T)(sizeof(C) == 8 ? 1.0 : 1.0 / (double)n)};
+                           (typename CReal<C>::T)(sizeof(C) == 8 ? 1.0 : 1.0 / (double)n), coarse};
     fft2_lines<N1, N2, -1>(TL, tw, S, src, dst);
 }
 
@@ -599,12 +617,216 @@ k_x_adjoint_r(Dims d, const double2 *__restrict__ roots, const double2 *__restri
 }
 
 // ---------------------------------------------------------------------------
+// Output reduction, x stage (coarse grid): c2r of the five z-physical fields
+// u, v, w, p, div of RW rows (z, j) per block, then per point the moment
+// terms of Statistics::reduce (src/sim/statistics.cpp:58-86) and div^2 of
+// Diagnostics::evaluate (src/sim/diagnostics.cpp:62-72), summed over the
+// block's points into partial[j][blockIdx.x][kMomentSlots]:
+//   0-3 u v w p, 4-6 uu vv ww, 7-9 uv vw wu, 10-12 pu pv pw, 13 pp,
+//   14-16 u^3 v^3 w^3, 17-19 u^4 v^4 w^4, 20 div^2, 21 finite flag (1/0),
+// with p = p_raw - (uu + vv + ww)/2.  If phys is set the block also writes
+// u, v, w, p_raw to phys[4][NZ][NY+1][NX] (the snapshot of to_physical).
+// Lines per row: (u, v), (w, p), (div, 0); a full-spectrum Nyquist bin is
+// doubled (the coarse c2r convention).
+// ---------------------------------------------------------------------------
+constexpr int kMomentSlots = 22;
+
+struct MomentAcc {
+    double s[21];
+    bool ok;
+    __device__ __forceinline__ void init() {
+#pragma unroll
+        for (int k = 0; k < 21; ++k) s[k] = 0.0;
+        ok = true;
+    }
+    __device__ __forceinline__ void add(double u, double v, double w, double praw, double dv) {
+        const double uu = u * u, vv = v * v, ww = w * w;
+        const double p = praw - 0.5 * (uu + vv + ww);
+        ok = ok && isfinite(u) && isfinite(v) && isfinite(w) && isfinite(praw) && isfinite(p) && isfinite(dv);
+        s[0] += u; s[1] += v; s[2] += w; s[3] += p;
+        s[4] += uu; s[5] += vv; s[6] += ww;
+        s[7] += u * v; s[8] += v * w; s[9] += w * u;
+        s[10] += p * u; s[11] += p * v; s[12] += p * w; s[13] += p * p;
+        s[14] += uu * u; s[15] += vv * v; s[16] += ww * w;
+        s[17] += uu * uu; s[18] += vv * vv; s[19] += ww * ww;
+        s[20] += dv * dv;
+    }
+    // block sum (fixed order) into out[0..21]; red holds 32 x kMomentSlots doubles
+    __device__ void store(double *red, double *out) {
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+        double f = ok ? 1.0 : 0.0;
+#pragma unroll
+        for (int k = 0; k < 21; ++k)
+            for (int m = 16; m > 0; m >>= 1) s[k] += __shfl_xor_sync(0xffffffffu, s[k], m);
+        for (int m = 16; m > 0; m >>= 1) f = fmin(f, __shfl_xor_sync(0xffffffffu, f, m));
+        if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < 21; ++k) red[wid * kMomentSlots + k] = s[k];
+            red[wid * kMomentSlots + 21] = f;
+        }
+        __syncthreads();
+        if (threadIdx.x < kMomentSlots) {
+            const int k = threadIdx.x;
+            double t = red[k];
+            for (int q = 1; q < nw; ++q) t = (k == 21) ? fmin(t, red[q * kMomentSlots + k]) : t + red[q * kMomentSlots + k];
+            out[k] = t;
+        }
+    }
+};
+
+template <int N1, int N2>
+__global__ void __launch_bounds__(16 * 3 * 4)
+k_x_moments_r(Dims d, const double2 *__restrict__ roots, const double2 *__restrict__ G, int RW,
+              double *__restrict__ partial, double *__restrict__ phys) {
+    using C = double2;
+    constexpr int n = N1 * N2;
+    constexpr int SP = N2 + 1;
+    extern __shared__ double2 sm_d[];
+    C *buf = sm_d + n;
+    __shared__ double red[32 * kMomentSlots];
+    const int L = 3 * RW;
+    const int slot = threadIdx.x >> 4, sub = threadIdx.x & 15;
+    const int j = blockIdx.y, z0 = blockIdx.x * RW;
+    const int nkx = d.nkx, nxs = d.NXS;
+    const long long fstride = (long long)d.ny2 * d.NZ2 * nkx;
+    const C *Gj = G + (long long)j * d.NZ2 * nkx;
+    const Twiddles<C> tw = load_twiddles<C>(sm_d, roots, n);
+    const int nyq = (n % 2 == 0) ? n / 2 : -1;
+    C v[N1 > N2 ? N1 : N2];
+    const bool act1 = slot < L && sub < N2;
+    if (act1) {
+        const int r = slot / 3, q = slot - (slot / 3) * 3;
+        const int z = z0 + r;
+        const C *rowA = Gj + (long long)z * nkx + (2 * q) * fstride;
+        const C *rowB = rowA + fstride;
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) {
+            const int m = sub + N2 * n1;
+            C x = mk(0.0, 0.0);
+            if (z < d.NZ2) {
+                const int mm = m <= nxs ? m : n - m;
+                if (m <= nxs || (m >= n - nxs && m != nyq)) {
+                    C A = rowA[mm], B = q < 2 ? rowB[mm] : mk(0.0, 0.0);
+                    if (mm == 0 || mm == nyq) {
+                        A.y = 0.0;
+                        B.y = 0.0;
+                    }
+                    if (mm == nyq) {
+                        A.x *= 2.0;
+                        B.x *= 2.0;
+                    }
+                    x = m <= nxs ? mk(A.x - B.y, A.y + B.x) : mk(A.x + B.y, B.x - A.y);
+                }
+            }
+            v[n1] = x;
+        }
+    }
+    __syncthreads();
+    if (act1) {
+        C(&w)[N1] = reinterpret_cast<C(&)[N1]>(v);
+        dft_reg<N1, +1>(w, tw, N2);
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1)
+            buf[(slot * N1 + k1) * SP + sub] = (k1 == 0 || sub == 0) ? w[k1] : tw.template mul<+1>(w[k1], sub * k1);
+    }
+    __syncthreads();
+    const bool act2 = slot < L && sub < N1;
+    if (act2) {
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) v[n2] = buf[(slot * N1 + sub) * SP + n2];
+    }
+    __syncthreads();
+    if (act2) {
+        C(&w)[N2] = reinterpret_cast<C(&)[N2]>(v);
+        dft_reg<N2, +1>(w, tw, N1);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) buf[slot * n + sub + N1 * k2] = w[k2];
+    }
+    __syncthreads();
+    MomentAcc acc;
+    acc.init();
+    const int ny1 = d.ny2;
+    for (int i = threadIdx.x; i < RW * n; i += blockDim.x) {
+        const int r = i / n, x = i - (i / n) * n;
+        const int z = z0 + r;
+        if (z >= d.NZ2) continue;
+        const C a = buf[(3 * r) * n + x], b = buf[(3 * r + 1) * n + x], c = buf[(3 * r + 2) * n + x];
+        acc.add(a.x, a.y, b.x, b.y, c.x);
+        if (phys) {
+            const long long o = ((long long)z * ny1 + j) * n + x, fs = (long long)d.NZ2 * ny1 * n;
+            phys[o] = a.x;
+            phys[fs + o] = a.y;
+            phys[2 * fs + o] = b.x;
+            phys[3 * fs + o] = b.y;
+        }
+    }
+    acc.store(red, partial + ((long long)j * gridDim.x + blockIdx.x) * kMomentSlots);
+}
+
+// Stockham form of k_x_moments_r for any NX.
+__global__ void __launch_bounds__(256)
+k_x_moments(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 *__restrict__ G, int RW,
+            double *__restrict__ partial, double *__restrict__ phys) {
+    extern __shared__ double2 sm[];
+    __shared__ double red[32 * kMomentSlots];
+    const int n = d.NX2;
+    double2 *s_root = sm;
+    const int L = 3 * RW;
+    double2 *a = sm + n;
+    double2 *b = a + n * L;
+    const int j = blockIdx.y, z0 = blockIdx.x * RW;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s_root[i] = roots[i];
+    const long long fstride = (long long)d.ny2 * d.NZ2 * d.nkx;
+    const double2 *Gj = G + (long long)j * d.NZ2 * d.nkx;
+    const int nyq = (n % 2 == 0) ? n / 2 : -1;
+    for (int i = threadIdx.x; i < n * L; i += blockDim.x) {
+        const int k = i / L, line = i - (i / L) * L;
+        const int r = line / 3, q = line - (line / 3) * 3;
+        const int z = z0 + r;
+        double2 A = mk(0, 0), B = mk(0, 0);
+        int m;
+        bool mirror;
+        if (k <= d.NXS) { m = k; mirror = false; }
+        else if (k >= n - d.NXS && k != nyq) { m = n - k; mirror = true; }
+        else { m = -1; mirror = false; }
+        if (m >= 0 && z < d.NZ2) {
+            const double2 *row = Gj + (long long)z * d.nkx + m + (2 * q) * fstride;
+            A = row[0];
+            if (q < 2) B = row[fstride];
+            if (m == 0 || m == nyq) { A.y = 0.0; B.y = 0.0; }
+            if (m == nyq) { A.x *= 2.0; B.x *= 2.0; }
+        }
+        a[i] = mirror ? mk(A.x + B.y, B.x - A.y) : mk(A.x - B.y, A.y + B.x);
+    }
+    __syncthreads();
+    const double2 *res = fft_lines<+1>(a, b, L, P, s_root);
+    MomentAcc acc;
+    acc.init();
+    const int ny1 = d.ny2;
+    for (int i = threadIdx.x; i < RW * n; i += blockDim.x) {
+        const int r = i / n, x = i - (i / n) * n;
+        const int z = z0 + r;
+        if (z >= d.NZ2) continue;
+        const double2 p0 = res[x * L + 3 * r], p1 = res[x * L + 3 * r + 1], p2 = res[x * L + 3 * r + 2];
+        acc.add(p0.x, p0.y, p1.x, p1.y, p2.x);
+        if (phys) {
+            const long long o = ((long long)z * ny1 + j) * n + x, fs = (long long)d.NZ2 * ny1 * n;
+            phys[o] = p0.x;
+            phys[fs + o] = p0.y;
+            phys[2 * fs + o] = p1.x;
+            phys[3 * fs + o] = p1.y;
+        }
+    }
+    acc.store(red, partial + ((long long)j * gridDim.x + blockIdx.x) * kMomentSlots);
+}
+
+// ---------------------------------------------------------------------------
 // Single-field x transforms for the standalone fine transform (tests and
 // to-physical output): c2r / r2c of one real field [z][j][x].
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(128)
 k_x_c2r(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 *__restrict__ G,
-        double *__restrict__ phys, int RW) {
+        double *__restrict__ phys, int RW, double nyq_scale) {
     extern __shared__ double2 sm[];
     const int n = d.NX2;
     double2 *s_root = sm;
@@ -627,6 +849,7 @@ k_x_c2r(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 *__r
             if (za < d.NZ2 && za < z0 + RW) A = G[((long long)j * d.NZ2 + za) * d.nkx + m];
             if (zb < d.NZ2 && zb < z0 + RW) B = G[((long long)j * d.NZ2 + zb) * d.nkx + m];
             if (m == 0 || m == nyq) { A.y = 0.0; B.y = 0.0; }
+            if (m == nyq) { A.x *= nyq_scale; B.x *= nyq_scale; }
         }
         a[i] = mirror ? mk(A.x + B.y, B.x - A.y) : mk(A.x - B.y, A.y + B.x);
     }
@@ -643,7 +866,7 @@ k_x_c2r(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 *__r
 
 __global__ void __launch_bounds__(128)
 k_x_r2c(Dims d, FftPlan P, const double2 *__restrict__ roots, const double *__restrict__ phys,
-        double2 *__restrict__ H, int RW) {
+        double2 *__restrict__ H, int RW, double nyq_scale) {
     extern __shared__ double2 sm[];
     const int n = d.NX2;
     double2 *s_root = sm;
@@ -672,7 +895,7 @@ k_x_r2c(Dims d, FftPlan P, const double2 *__restrict__ roots, const double *__re
         const double2 Pm = res[km * L + (r >> 1)];
         const double2 out = (r & 1) ? mk(0.5 * (P0.y + Pm.y), -0.5 * (P0.x - Pm.x))
                                     : mk(0.5 * (P0.x + Pm.x), 0.5 * (P0.y - Pm.y));
-        H[((long long)j * d.NZ2 + z) * d.nkx + k] = cscale(invn, out);
+        H[((long long)j * d.NZ2 + z) * d.nkx + k] = cscale(2 * k == n ? invn * nyq_scale : invn, out);
     }
 }
 
@@ -795,16 +1018,26 @@ size_t smem_xsingle(const Dims &d) {
 // (FP64 only).
 template <typename Fn> bool with_xsplit(int nx2, Fn &&fn) {
     switch (nx2) {
+    case 32: fn(std::integral_constant<int, 4>{}, std::integral_constant<int, 8>{}); return true;
     case 48: fn(std::integral_constant<int, 6>{}, std::integral_constant<int, 8>{}); return true;
+    case 64: fn(std::integral_constant<int, 8>{}, std::integral_constant<int, 8>{}); return true;
     case 72: fn(std::integral_constant<int, 8>{}, std::integral_constant<int, 9>{}); return true;
     case 96: fn(std::integral_constant<int, 8>{}, std::integral_constant<int, 12>{}); return true;
     case 144: fn(std::integral_constant<int, 12>{}, std::integral_constant<int, 12>{}); return true;
     case 192: fn(std::integral_constant<int, 12>{}, std::integral_constant<int, 16>{}); return true;
+    case 128: fn(std::integral_constant<int, 8>{}, std::integral_constant<int, 16>{}); return true;
     case 196: fn(std::integral_constant<int, 14>{}, std::integral_constant<int, 14>{}); return true;
     default: return false;
     }
 }
 constexpr int kRWr = 4;
+constexpr int kRWm = 4;    // rows per block of the output-reduction x stage
+size_t smem_xmoments_r(int n1, int n2) {
+    const size_t L = 3 * kRWm;
+    const size_t s1 = L * n1 * (n2 + 1), s2 = L * n1 * n2;
+    return sizeof(double2) * (n1 * n2 + (s1 > s2 ? s1 : s2));
+}
+size_t smem_xmoments(const Dims &d) { return sizeof(double2) * (size_t)d.NX2 * (1 + 2 * 3 * kRWm); }
 size_t smem_zfft_r(const Dims &d, int n1, int n2, size_t elem) {
     return sizeof(double2) * n1 * n2 + elem * ((size_t)n1 * n2 * z_lines(d));
 }
@@ -826,6 +1059,7 @@ template <class C> cudaError_t configure_register_forms(const Dims &d) {
         constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
         e = raise_smem(k_x_cross_r<N1, N2, C, sizeof(C) == 8>, smem_xcross_r(N1, N2, sizeof(C)));
         if (e == cudaSuccess && sizeof(C) == 16) e = raise_smem(k_x_adjoint_r<N1, N2>, smem_xadjoint_r(N1, N2));
+        if (e == cudaSuccess && sizeof(C) == 16) e = raise_smem(k_x_moments_r<N1, N2>, smem_xmoments_r(N1, N2));
     });
     if (e != cudaSuccess) return e;
     with_xsplit(d.NZ2, [&](auto a, auto b) {
@@ -855,19 +1089,23 @@ cudaError_t configure_transform_kernels(const Dims &d) {
     if (e != cudaSuccess) return e;
     e = raise_smem(k_x_adjoint, (int)smem_xadjoint(d));
     if (e != cudaSuccess) return e;
+    e = raise_smem(k_x_moments, (int)smem_xmoments(d));
+    if (e != cudaSuccess) return e;
     e = raise_smem(k_x_c2r, (int)smem_xsingle(d));
     if (e != cudaSuccess) return e;
     e = raise_smem(k_x_r2c, (int)smem_xsingle(d));
     return e;
 }
 
-template <class C> bool z_backward_r(const Dims &d, const double2 *roots, const C *F, C *G, int nf, cudaStream_t s) {
+template <class C>
+bool z_backward_r(const Dims &d, const double2 *roots, const C *F, C *G, int nf, cudaStream_t s,
+                  bool coarse = false) {
     const int tl = z_lines(d);
     dim3 grid((d.nkx + tl - 1) / tl, d.ny2, nf);
     return with_xsplit(d.NZ2, [&](auto a, auto b) {
         constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
         k_z_backward_r<N1, N2, C><<<grid, (N1 > N2 ? N1 : N2) * tl, smem_zfft_r(d, N1, N2, sizeof(C)), s>>>(
-            d, roots, F, G, tl);
+            d, roots, F, G, tl, coarse);
     });
 }
 template <class C, bool MEAN>
@@ -879,22 +1117,24 @@ bool x_cross_r(const Dims &d, const double2 *roots, const C *G, C *H, const doub
             d, roots, G, H, kRWr, mean);
     });
 }
-template <class C> bool z_forward_r(const Dims &d, const double2 *roots, const C *H, C *F, int nf, cudaStream_t s) {
+template <class C>
+bool z_forward_r(const Dims &d, const double2 *roots, const C *H, C *F, int nf, cudaStream_t s,
+                 bool coarse = false) {
     const int tl = z_lines(d);
     dim3 grid((d.nkx + tl - 1) / tl, d.ny2, nf);
     return with_xsplit(d.NZ2, [&](auto a, auto b) {
         constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
         k_z_forward_r<N1, N2, C><<<grid, (N1 > N2 ? N1 : N2) * tl, smem_zfft_r(d, N1, N2, sizeof(C)), s>>>(
-            d, roots, H, F, tl);
+            d, roots, H, F, tl, coarse);
     });
 }
 
 void launch_z_backward(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *F,
-                       double2 *G, int nf, cudaStream_t s) {
-    if (z_backward_r(d, roots, F, G, nf, s)) return;
+                       double2 *G, int nf, cudaStream_t s, bool coarse) {
+    if (z_backward_r(d, roots, F, G, nf, s, coarse)) return;
     const int tl = z_lines(d);
     dim3 grid((d.nkx + tl - 1) / tl, d.ny2, nf);
-    k_z_backward<<<grid, 256, smem_zfft(d), s>>>(d, P, roots, F, G, tl);
+    k_z_backward<<<grid, 256, smem_zfft(d), s>>>(d, P, roots, F, G, tl, coarse);
 }
 
 void launch_x_cross(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G,
@@ -905,11 +1145,11 @@ void launch_x_cross(const Dims &d, const FftPlan &P, const double2 *roots, const
 }
 
 void launch_z_forward(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *H,
-                      double2 *F, int nf, cudaStream_t s) {
-    if (z_forward_r(d, roots, H, F, nf, s)) return;
+                      double2 *F, int nf, cudaStream_t s, bool coarse) {
+    if (z_forward_r(d, roots, H, F, nf, s, coarse)) return;
     const int tl = z_lines(d);
     dim3 grid((d.nkx + tl - 1) / tl, d.ny2, nf);
-    k_z_forward<<<grid, 256, smem_zfft(d), s>>>(d, P, roots, H, F, tl);
+    k_z_forward<<<grid, 256, smem_zfft(d), s>>>(d, P, roots, H, F, tl, coarse);
 }
 
 // FP32 stage buffers (mixed precision): register forms only.
@@ -936,16 +1176,31 @@ void launch_x_adjoint(const Dims &d, const FftPlan &P, const double2 *roots, con
     k_x_adjoint<<<grid, 256, smem_xadjoint(d), s>>>(d, P, roots, G, L, kRWa);
 }
 
+int moment_blocks(const Dims &d) { return (d.NZ2 + kRWm - 1) / kRWm; }
+
+void launch_x_moments(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G, double *partial,
+                      double *phys, cudaStream_t s) {
+    dim3 grid(moment_blocks(d), d.ny2);
+    const bool reg = with_xsplit(d.NX2, [&](auto a, auto b) {
+        constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
+        k_x_moments_r<N1, N2><<<grid, 16 * 3 * kRWm, smem_xmoments_r(N1, N2), s>>>(d, roots, G, kRWm, partial, phys);
+    });
+    if (reg) return;
+    k_x_moments<<<grid, 256, smem_xmoments(d), s>>>(d, P, roots, G, kRWm, partial, phys);
+}
+
+// The coarse grid doubles (c2r) / halves (r2c) a full-spectrum x Nyquist bin
+// (src/fft/transforms.cpp:486-487, 574-576); the fine grid does not.
 void launch_x_c2r(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G,
-                  double *phys, cudaStream_t s) {
+                  double *phys, cudaStream_t s, bool coarse) {
     dim3 grid((d.NZ2 + kRWs - 1) / kRWs, d.ny2);
-    k_x_c2r<<<grid, 128, smem_xsingle(d), s>>>(d, P, roots, G, phys, kRWs);
+    k_x_c2r<<<grid, 128, smem_xsingle(d), s>>>(d, P, roots, G, phys, kRWs, coarse ? 2.0 : 1.0);
 }
 
 void launch_x_r2c(const Dims &d, const FftPlan &P, const double2 *roots, const double *phys,
-                  double2 *H, cudaStream_t s) {
+                  double2 *H, cudaStream_t s, bool coarse) {
     dim3 grid((d.NZ2 + kRWs - 1) / kRWs, d.ny2);
-    k_x_r2c<<<grid, 128, smem_xsingle(d), s>>>(d, P, roots, phys, H, kRWs);
+    k_x_r2c<<<grid, 128, smem_xsingle(d), s>>>(d, P, roots, phys, H, kRWs, coarse ? 0.5 : 1.0);
 }
 
 }  // namespace cdns

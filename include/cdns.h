@@ -93,6 +93,9 @@ int cdns_destroy(cdns_ctx *ctx);
 int cdns_set_velocity(cdns_ctx *ctx, const double *velocity);
 int cdns_get_velocity(cdns_ctx *ctx, double *velocity);
 int cdns_get_pressure(cdns_ctx *ctx, double *pressure);
+/* Replace the pressure of the last step (read by cdns_get_pressure and the
+ * output reduction; the step itself does not read it). */
+int cdns_set_pressure(cdns_ctx *ctx, const double *pressure);
 int cdns_set_velocity_bc(cdns_ctx *ctx, const double *bc);
 int cdns_set_velocity_device(cdns_ctx *ctx, const double *velocity_dev);
 int cdns_get_velocity_device(cdns_ctx *ctx, double *velocity_dev);
@@ -143,6 +146,28 @@ int cdns_transform_fine(cdns_ctx *ctx, int direction, const double *in, double *
  * device) race and must be serialised by the caller. */
 int cdns_transform_fine_backward_noalloc(const cdns_mesh_desc *mesh, const double *spectral,
                                          double *physical, void *stream);
+
+/* Coarse-grid transform of one scalar field, Transforms::channel_xyzfft
+ * (src/fft/transforms.cpp:452-582): direction 'B' spectral [2*NZS+1][NYS+1][NXS+1]
+ * -> physical [NZ][NY+1][NX], 'F' the inverse; a full spectrum (NXS = NX/2,
+ * NZS = NZ/2) takes the reference's Nyquist halve/mirror convention. */
+int cdns_transform_coarse(cdns_ctx *ctx, int direction, const double *in, double *out);
+
+/* The output branch of Simulation::run (src/sim/simulation.cpp:226-235) on
+ * the device, for the context's current velocity and pressure:
+ * FieldIO::to_physical (src/io/field_io.cpp:199-220), Statistics::reduce
+ * (src/sim/statistics.cpp:55-110) and Diagnostics::evaluate
+ * (src/sim/diagnostics.cpp:38-80).  Writes, each if not NULL:
+ *   plane_sums [NY+1][20]  PlaneMoments::sum per y plane (sums 7..19 zero
+ *                          unless higher_moments, as Statistics::reduce);
+ *   diagnostics[4]         EKT, TKE, divergence L2, finite (1 or 0);
+ *   physical [4][NZ][NY+1][NX]  the snapshot u, v, w, p of to_physical.
+ * Only the plane sums (and the snapshot, if asked for) cross to the host;
+ * the physical fields are formed and reduced on the GPU.  The reference's
+ * Statistics::accumulate(planes, dpdx, dpdz) and Diagnostics::append take
+ * these values unchanged. */
+int cdns_output_reduce(cdns_ctx *ctx, int higher_moments, double *plane_sums, double *diagnostics,
+                       double *physical);
 
 /* EqSolvePV::setup(g) followed by the fused solve (solve_modes with fused
  * RHS divergence and sigma correction, src/solver/eqsolve_pv.cpp:311-450)

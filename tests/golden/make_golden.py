@@ -20,8 +20,9 @@ on small seeded inputs and stores inputs and outputs as compressed npz files:
                         spectrum (Nyquist halve/mirror branches, 16x17x16)
                         and a ragged one (NXS=5, NZS=6): a realisable and an
                         arbitrary spectrum each.
-  golden_reduce.npz     the output branch on a 16x17x16 state: physical
-                        u, v, w, p, plane sums, finite flags, EKT/TKE/div_L2.
+  golden_reduce.npz     the output branch on a 16x17x16 state (a divergence-free
+                        field plus a non-solenoidal part): physical u, v, w,
+                        p, plane sums, finite flags, EKT/TKE/div_L2.
 
 Usage: python tests/golden/make_golden.py [name ...]   (needs oracle/_ref built;
 names: step example nonlinear solve fine coarse reduce, default all)
@@ -67,6 +68,8 @@ def coarse_and_reduce(which):
         u = divergence_free_field(m, p, seed=61, amp=0.1, spectrum="k53", mean="loglaw")
         rng = np.random.default_rng(62)
         pres = orc.coarse_forward(m, rng.standard_normal((m.NZ, m.NY + 1, m.NX)))
+        # a non-solenoidal part, so that the divergence norm is O(1) and not round-off
+        u = [uc + orc.coarse_forward(m, 0.3 * rng.standard_normal((m.NZ, m.NY + 1, m.NX))) for uc in u]
         phys, planes, flags, values = ref_io.reduce(m, p, u, pres)
         np.savez_compressed(os.path.join(HERE, "golden_reduce.npz"), **mesh_dict(m, p), u=np.stack(u),
                             p=pres, phys=phys, planes=planes, flags=flags, values=values)

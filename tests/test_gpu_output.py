@@ -1,0 +1,117 @@
+"""Coarse-grid transform and the device-side output reduction (cdns_transform_coarse,
+cdns_output_reduce) against the reference's own channel_xyzfft, to_physical,
+Statistics::reduce and Diagnostics::evaluate (golden fixtures made by
+tests/golden/make_golden.py from the reference sources), and against the
+oracle at the Re_tau180 size."""
+import os
+
+import numpy as np
+import pytest
+
+import cdns
+from golden_io import GOLDEN, load
+from oracle_cases import channel_case, divergence_free_field, orc, retau180_case
+from test_gpu_parity import ctx_for
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_max(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def plane_scale(vp, pp):
+    """Per moment, the largest plane sum of |term|: the round-off scale of
+    plane sums that cancel (mean-free components) or that sample the
+    round-off of the no-slip walls (high powers of values ~1e-14)."""
+    a = [np.abs(x) for x in vp]
+    s = orc.plane_moments(a, np.abs(pp) + (a[0] ** 2 + a[1] ** 2 + a[2] ** 2))
+    return s.max(axis=0)[None, :]
+
+
+@pytest.mark.parametrize("tag", ["full", "ragged"])
+@pytest.mark.parametrize("kind", ["real", "arb"])
+def test_coarse_transform_matches_reference(tag, kind):
+    """Full spectrum (Nyquist halve/mirror branches) and ragged (NXS < NX/2),
+    realisable and arbitrary spectra."""
+    d = dict(np.load(os.path.join(GOLDEN, "golden_coarse.npz")))
+    mm = [int(v) for v in d[f"{tag}_mesh"]]
+    m = orc.Mesh(*mm, float(d[f"{tag}_dom"][0]), float(d[f"{tag}_dom"][1]))
+    _, p = channel_case(16)
+    c = ctx_for(m, p)
+    U, phys, back = d[f"{tag}_{kind}_U"], d[f"{tag}_{kind}_phys"], d[f"{tag}_{kind}_back"]
+    assert rel_max(c.transform_coarse("B", U), phys) <= 1e-13
+    assert rel_max(c.transform_coarse("F", phys), back) <= 1e-13
+
+
+@pytest.mark.parametrize("n", [32, 48])
+def test_coarse_transform_matches_oracle(n):
+    """Register-form sizes (NX = NZ = 32 = 4 x 8; 48 = 6 x 8)."""
+    m, p = channel_case(n)
+    rng = np.random.default_rng(n)
+    U = orc.coarse_forward(m, rng.standard_normal((m.NZ, m.NY + 1, m.NX)))
+    c = ctx_for(m, p)
+    P = c.transform_coarse("B", U)
+    assert rel_max(P, orc.coarse_backward(m, U)) <= 1e-13
+    assert rel_max(c.transform_coarse("F", P), orc.coarse_forward(m, P)) <= 1e-13
+
+
+def test_output_reduction_matches_reference():
+    m, p, d = load("golden_reduce.npz")
+    c = ctx_for(m, p)
+    c.set_velocity(np.stack(list(d["u"]), axis=-1))
+    c.set_pressure(d["p"])
+    planes, values, phys = c.output_reduce(higher_moments=True, snapshot=True)
+    for k in range(4):
+        assert rel_max(phys[k], d["phys"][k]) <= 1e-13
+    vp = [phys[0], phys[1], phys[2]]
+    assert np.all(np.abs(planes - d["planes"]) <= 1e-12 * plane_scale(vp, phys[3]))
+    ref = d["values"]
+    assert abs(values["ekt"] - ref[0]) <= 1e-13 * ref[0]
+    assert abs(values["tke"] - ref[1]) <= 1e-12 * ref[1]
+    assert ref[2] > 0.1 and abs(values["divergence_l2"] - ref[2]) <= 1e-12 * ref[2]
+    assert values["finite"] and ref[3] == 1.0
+    # without higher moments, Statistics::reduce leaves sums 7..19 at zero
+    low, _, _ = c.output_reduce(higher_moments=False)
+    assert np.array_equal(low[:, :7], planes[:, :7]) and not low[:, 7:].any()
+
+
+def test_output_reduction_reports_nonfinite():
+    m, p, d = load("golden_reduce.npz")
+    c = ctx_for(m, p)
+    u = np.stack(list(d["u"]), axis=-1)
+    u[2, 3, 1, 0] = np.inf
+    c.set_velocity(u)
+    c.set_pressure(d["p"])
+    _, values, _ = c.output_reduce()
+    assert not values["finite"]
+
+
+@pytest.mark.slow
+def test_output_reduction_retau180():
+    """128 x 129 x 128 coarse grid after 5 steps of the Re_tau180 case: plane
+    sums, diagnostics and snapshot against the oracle on the same state; the
+    plane mean of u equals the Chebyshev mean profile at each point."""
+    m, p = retau180_case()
+    c = ctx_for(m, p)
+    u0 = divergence_free_field(m, p, seed=1, amp=0.1, spectrum="k53", mean="loglaw")
+    c.set_velocity(np.stack(u0, axis=-1))
+    c.run(1, 5)
+    c.synchronize()
+    u = c.get_velocity()
+    pr = c.get_pressure()
+    planes, values, phys = c.output_reduce(snapshot=True)
+    vel = [u[..., k] for k in range(3)]
+    vp, pp = orc.to_physical(m, vel, pr)
+    for k in range(3):
+        assert rel_max(phys[k], vp[k]) <= 1e-12
+    assert rel_max(phys[3], pp) <= 1e-12
+    ref = orc.plane_moments(vp, pp)
+    assert np.all(np.abs(planes - ref) <= 1e-12 * plane_scale(vp, pp))
+    ekt, tke, div = orc.diagnostics(m, orc.make_constants(m, p.Re), ref, vel)
+    assert abs(values["ekt"] - ekt) <= 1e-12 * ekt and abs(values["tke"] - tke) <= 1e-12 * tke
+    # a solenoidal field: both divergence norms are round-off
+    assert values["divergence_l2"] <= 1e-9 and div <= 1e-9
+    yj = np.cos(np.pi * np.arange(m.NY + 1) / m.NY)
+    mean_u = np.polynomial.chebyshev.chebval(yj, u[m.NZS, :, 0, 0].real)
+    assert np.abs(planes[:, 0] / (m.NX * m.NZ) - mean_u).max() <= 1e-11 * np.abs(mean_u).max()

@@ -93,10 +93,10 @@ def test_oracle_output_reduction_matches_reference():
     assert _rel_max(pp, d["phys"][3]) <= 1e-14
     planes = orc.plane_moments(vp, pp)
     ref = d["planes"]
-    scale = plane_sum_scale(vp, pp)
-    assert np.all(np.abs(planes - ref) <= 1e-13 * scale)
+    scale = plane_sum_scale(vp, pp).max(axis=0)   # per moment: its largest plane
+    assert np.all(np.abs(planes - ref) <= 1e-13 * scale[None, :])
     assert np.all(d["flags"] == 1.0)
     ekt, tke, div = orc.diagnostics(m, orc.make_constants(m, p.Re), ref, u)
     v = d["values"]
     assert abs(ekt - v[0]) <= 1e-14 * v[0] and abs(tke - v[1]) <= 1e-13 * v[1]
-    assert abs(div - v[2]) <= 1e-12 * max(v[2], 1e-300) + 1e-16 and v[3] == 1.0
+    assert v[2] > 0.1 and abs(div - v[2]) <= 1e-12 * v[2] and v[3] == 1.0
