@@ -59,6 +59,9 @@ _SIGNATURES = {
     "cdns_set_pressure": [ctypes.c_void_p, ctypes.c_void_p],
     "cdns_transform_coarse": [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
     "cdns_output_reduce": [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+    "cdns_statistics_sample": [ctypes.c_void_p],
+    "cdns_statistics_read": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong), ctypes.c_void_p, ctypes.c_void_p],
+    "cdns_statistics_reset": [ctypes.c_void_p],
     "cdns_set_velocity_device": [ctypes.c_void_p, ctypes.c_void_p],
     "cdns_get_velocity_device": [ctypes.c_void_p, ctypes.c_void_p],
     "cdns_step": [ctypes.c_void_p, ctypes.c_int],
@@ -358,6 +361,21 @@ class Context:
         values = {"ekt": float(diag[0]), "tke": float(diag[1]), "divergence_l2": float(diag[2]),
                   "finite": bool(diag[3] == 1.0)}
         return planes, values, phys
+
+    def statistics_sample(self) -> None:
+        """Queue a statistics sample of the current state (no host sync)."""
+        _check(lib().cdns_statistics_sample(self._h))
+
+    def statistics_read(self):
+        """(count, (dpdx_mean, dpdz_mean), means [20][NY+1]) of the samples so far."""
+        n = ctypes.c_longlong(0)
+        dp = np.zeros(2)
+        means = np.zeros((20, self.mesh.NY + 1))
+        _check(lib().cdns_statistics_read(self._h, ctypes.byref(n), _ptr(dp), _ptr(means)))
+        return int(n.value), (float(dp[0]), float(dp[1])), means
+
+    def statistics_reset(self) -> None:
+        _check(lib().cdns_statistics_reset(self._h))
 
     # ---- discrete adjoint ----
     def adjoint_run(self, nsteps: int, checkpoint_interval: int, control: Optional[np.ndarray] = None,

@@ -35,6 +35,8 @@ struct OutputWork {
     double *phys = nullptr;      // [4][NZ][NY+1][NX] snapshot (made on first request)
     unsigned *flag = nullptr;    // spectral finite check
     std::vector<double> ccw;     // Clenshaw-Curtis weights / 2
+    double *stats = nullptr;     // running means [20][NY+1] + dpdx, dpdz means
+    long long count = 0;         // samples accumulated
 };
 
 void output_release(OutputWork *w) {
@@ -122,6 +124,40 @@ __global__ void k_plane_finalize(int nblocks, const double *__restrict__ partial
     double t = p[k];
     for (int b = 1; b < nblocks; ++b) t = (k == 21) ? fmin(t, p[b * K + k]) : t + p[b * K + k];
     planes[j * K + k] = t;
+}
+
+// Statistics::accumulate (src/sim/statistics.cpp:117-139) on the device:
+// running means (old * count + sample) / (count + 1) of the plane moments
+// scaled by 1/(NX NZ), in the layout [20][NY+1]:
+//   0-2 velocity mean, 3 pressure mean, 4-9 velocity second moments (uu vv
+//   ww uv vw wu), 10 pressure second, 11-13 pressure-velocity, 14-16
+//   velocity third, 17-19 velocity fourth; then the dpdx and dpdz means.
+__global__ void k_stats_accumulate(int ny1, double scale, long long count, const double *__restrict__ planes,
+                                   const double *__restrict__ dpdx, double *__restrict__ stats) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const double cn = (double)count, cn1 = (double)(count + 1);
+    auto upd = [&](int slot, double sample) {
+        double &o = stats[(long long)slot * ny1 + j];
+        o = (o * cn + sample) / cn1;
+    };
+    if (j < ny1) {
+        const double *sm = planes + (long long)j * 22;
+        upd(3, sm[3] * scale);
+        upd(10, sm[13] * scale);
+        for (int c = 0; c < 3; ++c) {
+            upd(c, sm[c] * scale);
+            upd(4 + c, sm[4 + c] * scale);
+            upd(7 + c, sm[7 + c] * scale);
+            upd(11 + c, sm[10 + c] * scale);
+            upd(14 + c, sm[14 + c] * scale);
+            upd(17 + c, sm[17 + c] * scale);
+        }
+    }
+    if (j == 0) {
+        double *dm = stats + 20LL * ny1;
+        dm[0] = (dm[0] * cn + dpdx[0]) / cn1;
+        dm[1] = (dm[1] * cn + dpdx[1]) / cn1;
+    }
 }
 
 size_t div_smem(const Dims &d) { return sizeof(double2) * (size_t)d.ncy * kColsPerBlock; }
@@ -233,11 +269,30 @@ int ensure_output(cdns_ctx *c, bool snapshot) {
         CK(cudaGetLastError());   // (limits are only ever raised: the fine-grid launches stay valid)
     }
     OutputWork *w = c->outw;
+    if (!w->stats) {
+        int r = oalloc(c, w, w->stats, 20 * (size_t)w->dc.ny2 + 2);
+        if (r) return r;
+    }
     if (snapshot && !w->phys) {
         const Dims &dc = w->dc;
         int r = oalloc(c, w, w->phys, 4 * (size_t)dc.NZ2 * dc.ny2 * dc.NX2);
         if (r) return r;
     }
+    return CDNS_OK;
+}
+
+// Plane sums of the current state into w->planes (stream-ordered, no sync).
+int enqueue_reduction(cdns_ctx *c, bool snapshot) {
+    OutputWork *w = c->outw;
+    const Dims &d = c->d, &dc = w->dc;
+    cudaStream_t s = c->stream;
+    CK(cudaMemsetAsync(w->flag, 0, sizeof(unsigned), s));
+    launch_divergence(d, c->t, c->U[c->cur], c->p, w->pd, w->flag, s);
+    launch_ysynth(dc, w->tc, c->U[c->cur], w->pd, 3, 5, w->F, s);
+    launch_z_backward(dc, w->pz, w->tc.root_z, w->F, w->G, 5, s, true);
+    launch_x_moments(dc, w->px, w->tc.root_x, w->G, w->partial, snapshot ? w->phys : nullptr, s);
+    k_plane_finalize<<<dc.ny2, 32, 0, s>>>(moment_blocks(dc), w->partial, w->planes);
+    CK(cudaGetLastError());
     return CDNS_OK;
 }
 
@@ -253,18 +308,11 @@ int cdns_output_reduce(cdns_ctx *c, int higher, double *plane_sums, double *diag
     if (!c->have_velocity) return fail(CDNS_ERR_STATE, "cdns_output_reduce before cdns_set_velocity");
     DeviceGuard guard(c->device);
     int r = ensure_output(c, physical != nullptr);
-    if (r) return r;
+    if (r || (r = enqueue_reduction(c, physical != nullptr))) return r;
     OutputWork *w = c->outw;
-    const Dims &d = c->d, &dc = w->dc;
+    const Dims &dc = w->dc;
     cudaStream_t s = c->stream;
-    CK(cudaMemsetAsync(w->flag, 0, sizeof(unsigned), s));
-    launch_divergence(d, c->t, c->U[c->cur], c->p, w->pd, w->flag, s);
-    launch_ysynth(dc, w->tc, c->U[c->cur], w->pd, 3, 5, w->F, s);
-    launch_z_backward(dc, w->pz, w->tc.root_z, w->F, w->G, 5, s, true);
-    launch_x_moments(dc, w->px, w->tc.root_x, w->G, w->partial, physical ? w->phys : nullptr, s);
     const int ny1 = dc.ny2;
-    k_plane_finalize<<<ny1, 32, 0, s>>>(moment_blocks(dc), w->partial, w->planes);
-    CK(cudaGetLastError());
     std::vector<double> pl((size_t)ny1 * 22);
     unsigned flag = 0;
     CK(cudaMemcpyAsync(pl.data(), w->planes, pl.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -305,6 +353,52 @@ int cdns_output_reduce(cdns_ctx *c, int higher, double *plane_sums, double *diag
         diag[2] = l2;
         diag[3] = finite ? 1.0 : 0.0;
     }
+    return CDNS_OK;
+}
+
+int cdns_statistics_sample(cdns_ctx *c) {
+    if (!c) return fail(CDNS_ERR_ARG, "null context");
+    if (!c->have_velocity) return fail(CDNS_ERR_STATE, "cdns_statistics_sample before cdns_set_velocity");
+    DeviceGuard guard(c->device);
+    int r = ensure_output(c, false);
+    if (r || (r = enqueue_reduction(c, false))) return r;
+    OutputWork *w = c->outw;
+    const Dims &dc = w->dc;
+    const double scale = 1.0 / ((double)dc.NX2 * (double)dc.NZ2);
+    k_stats_accumulate<<<(dc.ny2 + 127) / 128, 128, 0, c->stream>>>(dc.ny2, scale, w->count, w->planes, c->dpdx,
+                                                                      w->stats);
+    CK(cudaGetLastError());
+    ++w->count;
+    return CDNS_OK;
+}
+
+int cdns_statistics_read(cdns_ctx *c, long long *count, double *dp_means, double *means) {
+    if (!c) return fail(CDNS_ERR_ARG, "null context");
+    DeviceGuard guard(c->device);
+    int r = ensure_output(c, false);
+    if (r) return r;
+    OutputWork *w = c->outw;
+    const size_t n = 20 * (size_t)w->dc.ny2;
+    std::vector<double> h(n + 2);
+    CK(cudaMemcpyAsync(h.data(), w->stats, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (count) *count = w->count;
+    if (dp_means) {
+        dp_means[0] = h[n];
+        dp_means[1] = h[n + 1];
+    }
+    if (means) std::copy(h.begin(), h.begin() + n, means);
+    return CDNS_OK;
+}
+
+int cdns_statistics_reset(cdns_ctx *c) {
+    if (!c) return fail(CDNS_ERR_ARG, "null context");
+    DeviceGuard guard(c->device);
+    int r = ensure_output(c, false);
+    if (r) return r;
+    OutputWork *w = c->outw;
+    CK(cudaMemsetAsync(w->stats, 0, (20 * (size_t)w->dc.ny2 + 2) * sizeof(double), c->stream));
+    w->count = 0;
     return CDNS_OK;
 }
 

@@ -169,6 +169,20 @@ int cdns_transform_coarse(cdns_ctx *ctx, int direction, const double *in, double
 int cdns_output_reduce(cdns_ctx *ctx, int higher_moments, double *plane_sums, double *diagnostics,
                        double *physical);
 
+/* Statistics sampling on the device (the `sample` branch of Simulation::run,
+ * src/sim/simulation.cpp:227-250).  cdns_statistics_sample queues on the
+ * context stream, with no host synchronisation, the reduction of the current
+ * state and Statistics::accumulate's running-mean update
+ * (src/sim/statistics.cpp:117-139) with the last step's dp/dx and dp/dz.
+ * cdns_statistics_read returns the sample count, the (dpdx, dpdz) means and
+ * means [20][NY+1]: velocity mean u v w, pressure mean, velocity second
+ * moments uu vv ww uv vw wu, pressure second, pressure-velocity pu pv pw,
+ * velocity third and fourth moments (u v w each) -- the arrays
+ * Statistics::write prints; cdns_statistics_reset starts over. */
+int cdns_statistics_sample(cdns_ctx *ctx);
+int cdns_statistics_read(cdns_ctx *ctx, long long *count, double *dp_means, double *means);
+int cdns_statistics_reset(cdns_ctx *ctx);
+
 /* EqSolvePV::setup(g) followed by the fused solve (solve_modes with fused
  * RHS divergence and sigma correction, src/solver/eqsolve_pv.cpp:311-450)
  * of a given velocity RHS [..][3], pressure wall data [..][2][..] and velocity

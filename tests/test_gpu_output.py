@@ -115,3 +115,32 @@ def test_output_reduction_retau180():
     yj = np.cos(np.pi * np.arange(m.NY + 1) / m.NY)
     mean_u = np.polynomial.chebyshev.chebval(yj, u[m.NZS, :, 0, 0].real)
     assert np.abs(planes[:, 0] / (m.NX * m.NZ) - mean_u).max() <= 1e-11 * np.abs(mean_u).max()
+
+
+def test_statistics_sampling_matches_host_accumulate():
+    """cdns_statistics_sample (device-side Statistics::accumulate) against the
+    reference's update rule applied on the host to the plane sums of the same
+    states, over 5 steps of a 32^3 channel."""
+    m, p = channel_case(32)
+    c = ctx_for(m, p)
+    c.set_velocity(np.stack(divergence_free_field(m, p, seed=3, amp=0.1, spectrum="k53", mean="loglaw"), axis=-1))
+    ny1, scale = m.NY + 1, 1.0 / (m.NX * m.NZ)
+    host = np.zeros((20, ny1))
+    dpm = np.zeros(2)
+    # means slot <- plane-sum index (Statistics::accumulate, statistics.cpp:121-136)
+    src = [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 13, 10, 11, 12, 14, 15, 16, 17, 18, 19]
+    for it in range(1, 6):
+        c.step(it)
+        c.synchronize()
+        planes, _, _ = c.output_reduce()
+        dpdx = c.dpdx()
+        for slot, k in enumerate(src):
+            host[slot] = (host[slot] * (it - 1) + planes[:, k] * scale) / it
+        dpm = (dpm * (it - 1) + np.array(dpdx)) / it
+        c.statistics_sample()
+    n, dp, means = c.statistics_read()
+    assert n == 5
+    assert np.allclose(np.array(dp), dpm, rtol=1e-15, atol=0.0)
+    assert np.allclose(means, host, rtol=1e-14, atol=0.0)
+    c.statistics_reset()
+    assert c.statistics_read()[0] == 0
