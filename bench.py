@@ -344,6 +344,7 @@ def main():
     ap.add_argument("--ensemble-members", type=int, default=64)
     ap.add_argument("--ensemble-steps", type=int, default=200)
     ap.add_argument("--no-adjoint", action="store_true", help="skip the discrete-adjoint arm")
+    ap.add_argument("--no-output", action="store_true", help="skip the statistics-sampling arm")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -415,6 +416,50 @@ def main():
     peak, peak_kind = measured_peak()
     achieved = sb[top] / (per_launch[top] * 1e-3) / 1e9
     step_model = step_bytes_model(mesh)
+
+    # ---- statistics sampled every step (device-side output reduction) ------
+    output = None
+    if not args.no_output:
+        KS = min(K, 200)
+        ctx.statistics_reset()
+        ctx.set_velocity(host_u.numpy())
+        ctx.run(1, W)
+        ctx.statistics_sample()
+        ctx.synchronize()
+        torch.cuda.synchronize()
+        o0 = torch.cuda.Event(enable_timing=True)
+        o1 = torch.cuda.Event(enable_timing=True)
+        o2 = torch.cuda.Event(enable_timing=True)
+        o0.record(stream)
+        for it in range(W + 1, W + KS + 1):
+            ctx.step(it)
+            ctx.statistics_sample()
+        o1.record(stream)
+        for _ in range(KS):
+            ctx.statistics_sample()
+        o2.record(stream)
+        ctx.synchronize()
+        torch.cuda.synchronize()
+        ms_sampled = o0.elapsed_time(o1) / KS
+        ms_sample = o1.elapsed_time(o2) / KS
+        ny1, nzc, nxc = mesh.NY + 1, mesh.NZ, mesh.NX
+        ns = (2 * mesh.NZS + 1) * (mesh.NYS + 1) * (mesh.NXS + 1)
+        ncol = (2 * mesh.NZS + 1) * (mesh.NXS + 1)
+        # divergence (u, v, w, p in; p, div out) + y synthesis (5 fields) + z (5) + fused x/moments (5 in)
+        red_bytes = 16 * (6 * ns + 5 * ns + 2 * 5 * ny1 * ncol + 2 * 5 * ny1 * nzc * (mesh.NXS + 1))
+        t0 = time.perf_counter()
+        for _ in range(20):
+            ctx.output_reduce()
+        ms_sync = (time.perf_counter() - t0) * 1e3 / 20
+        output = {"workload": "statistics sampled every step (to_physical + Statistics::reduce + accumulate "
+                              "on the 128x129x128 coarse grid)",
+                  "steps_per_s_sampled": world * 1000.0 / ms_sampled, "ms_per_sampled_step": ms_sampled,
+                  "ms_per_sample": ms_sample, "sample_overhead_vs_step": ms_sample / ms_per_step,
+                  "sample_bytes": red_bytes,
+                  "sample_hbm_frac": red_bytes / (ms_sample * 1e-3) / 1e9 / peak,
+                  "output_reduce_call_ms": ms_sync,
+                  "note": "output_reduce_call_ms: the synchronous call (plane sums and diagnostics to the "
+                          "host), host wall clock; the others CUDA events on the context stream"}
 
     # ---- mixed FP32/FP64 arm: throughput and error after 1000 steps ------
     mixed = None
@@ -530,6 +575,7 @@ def main():
             "mixed": mixed,
             "ensemble": ensemble,
             "adjoint": adjoint,
+            "statistics": output,
             "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": KE, "finite": finite,
                     "protocol": "upload + steps 1..K one call each with dpdx readback + download"},
