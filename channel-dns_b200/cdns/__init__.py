@@ -60,6 +60,11 @@ _SIGNATURES = {
     "cdns_transform_coarse": [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
     "cdns_output_reduce": [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
     "cdns_statistics_sample": [ctypes.c_void_p],
+    "cdns_tune": [ctypes.c_void_p],
+    "cdns_get_tuning": [ctypes.c_void_p, ctypes.c_void_p],
+    "cdns_wisdom_export": [ctypes.c_char_p],
+    "cdns_wisdom_import": [ctypes.c_char_p],
+    "cdns_wisdom_forget": [],
     "cdns_statistics_read": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong), ctypes.c_void_p, ctypes.c_void_p],
     "cdns_statistics_reset": [ctypes.c_void_p],
     "cdns_set_velocity_device": [ctypes.c_void_p, ctypes.c_void_p],
@@ -377,6 +382,18 @@ class Context:
     def statistics_reset(self) -> None:
         _check(lib().cdns_statistics_reset(self._h))
 
+    # ---- launch-shape tuning ----
+    def tune(self) -> None:
+        _check(lib().cdns_tune(self._h))
+
+    def tuning(self) -> dict:
+        """{"z_lines": kx lines per z-transform block (0: rule), "y_synthesis":
+        "fft" or "matrix", "y_analysis": "fft" or "matrix"}."""
+        out = np.zeros(3, dtype=np.int32)
+        _check(lib().cdns_get_tuning(self._h, out.ctypes.data_as(ctypes.c_void_p)))
+        return {"z_lines": int(out[0]), "y_synthesis": "fft" if out[1] else "matrix",
+                "y_analysis": "fft" if out[2] else "matrix"}
+
     # ---- discrete adjoint ----
     def adjoint_run(self, nsteps: int, checkpoint_interval: int, control: Optional[np.ndarray] = None,
                     gradient: bool = True, weights: Optional[np.ndarray] = None):
@@ -521,6 +538,18 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def wisdom_export(path: str) -> None:
+    _check(lib().cdns_wisdom_export(path.encode()))
+
+
+def wisdom_import(path: str) -> None:
+    _check(lib().cdns_wisdom_import(path.encode()))
+
+
+def wisdom_forget() -> None:
+    _check(lib().cdns_wisdom_forget())
 
 
 def version() -> str:

@@ -219,6 +219,7 @@ void nonlinear_adjoint(cdns_ctx *c, const double2 *G6, const double2 *lN, const 
     AdjointWork *w = c->adj;
     Tables ta = c->t;
     ta.csyn = w->csyn_t;   // includes 1/(NX2 NZ2): the transposed x and z analysis scalings
+    ta.yform = 0;          // the transposed tables run in the matrix form
     launch_ysynth(d, ta, lN, nullptr, 3, 3, w->AF, s);
     launch_z_backward(d, c->pz, c->t.root_z, w->AF, w->AG, 3, s);
     launch_x_adjoint(d, c->px, c->t.root_x, G6, w->AG, s);

@@ -22,6 +22,7 @@ struct Dims {
                          // ncol, rounded up to even for FP32 stages (16-byte rows)
     int nyh;             // NY2/2+1 (half of the y points, symmetric pairs)
     long long Ns;        // nkz*ncy*nkx complex values per spectral component
+    int ztl;             // kx lines per block of the z transforms (0: the padding rule)
 };
 
 // Read-only per-context tables in device memory.
@@ -34,6 +35,9 @@ struct Tables {
     const double *cana;   // Chebyshev analysis matrix (chebyshev.cu)
     const double2 *root_x;  // [NX2] exp(-2 pi i k / NX2)
     const double2 *root_z;  // [NZ2] exp(-2 pi i k / NZ2)
+    const double2 *root_y;  // [NY2] exp(-2 pi i k / NY2) (FFT form of the Chebyshev transforms)
+    int yform;              // Chebyshev transforms in the FFT (DCT-I) form where NY2 splits:
+                            // bit 0 the synthesis, bit 1 the analysis (else the FP64 MMA products)
 };
 
 struct FftPlan {

@@ -54,6 +54,12 @@ void launch_x_cross(const Dims &d, const double2 *roots, const float2 *G, float2
 void launch_z_forward(const Dims &d, const double2 *roots, const float2 *H, float2 *F, int nf, cudaStream_t s);
 void launch_x_r2c(const Dims &d, const FftPlan &P, const double2 *roots, const double *phys,
                   double2 *H, cudaStream_t s, bool coarse = false);
+// Chebyshev synthesis (ana = false: spectral src0/src1 as in launch_ysynth ->
+// F) or analysis (ana = true: F in src0 -> spectral) in the FFT (DCT-I) form;
+// false if NY2 has no register split (the caller takes the matrix form).
+bool ydct_available(const Dims &d, const Tables &t);
+bool launch_ydct(const Dims &d, const Tables &t, const double2 *src0, const double2 *src1, int nsplit, int nf,
+                 double2 *out, bool ana, cudaStream_t s);
 // Output reduction, x stage on the coarse grid (Dims of the coarse grid):
 // c2r of G[5] (u, v, w, p, div), per-point moments summed per block into
 // partial[NY+1][moment_blocks][22]; phys (may be null) receives u, v, w, p.

@@ -564,6 +564,7 @@ void ysynth(const Dims &d, const Tables &t, const double2 *src0, const double2 *
 }
 void launch_ysynth(const Dims &d, const Tables &t, const double2 *src0, const double2 *src1, int nsplit,
                    int nf, double2 *F, cudaStream_t s) {
+    if ((t.yform & 1) && launch_ydct(d, t, src0, src1, nsplit, nf, F, false, s)) return;
     ysynth(d, t, src0, src1, nsplit, nf, F, static_cast<double *>(nullptr), s);
 }
 void launch_ysynth(const Dims &d, const Tables &t, const double2 *src0, const double2 *src1, int nsplit,
@@ -587,6 +588,7 @@ void yanalysis(const Dims &d, const Tables &t, const CI *F, double2 *S, int nf, 
     yanalysis(d, t.cana, F, S, nf, sxz / (2.0 * d.NY2), sxz / (double)d.NY2, s);
 }
 void launch_yanalysis(const Dims &d, const Tables &t, const double2 *F, double2 *S, int nf, cudaStream_t s) {
+    if ((t.yform & 2) && launch_ydct(d, t, F, nullptr, 0, nf, S, true, s)) return;
     yanalysis(d, t, F, S, nf, s);
 }
 void launch_yanalysis(const Dims &d, const Tables &t, const float2 *F, double2 *S, int nf, cudaStream_t s) {

@@ -4,6 +4,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -290,12 +291,12 @@ int cdns_create(const cdns_mesh_desc *m, const cdns_params *p, int precision, in
         }
         return rr;
     };
-    const auto rx = roots(d.NX2), rz = roots(d.NZ2);
+    const auto rx = roots(d.NX2), rz = roots(d.NZ2), ry = roots(d.NY2);
     double *tab = nullptr;
     // every table starts on a 256-byte boundary (double2 tables need 16)
     auto rup = [](size_t n) { return (n + 31) / 32 * 32; };
     const size_t ntab = rup(d.nkx) + rup(d.nkz) + 3 * rup(d.ncy) + rup(cosy.size()) +
-                        rup(2 * (size_t)d.NX2) + rup(2 * (size_t)d.NZ2);
+                        rup(2 * (size_t)d.NX2) + rup(2 * (size_t)d.NZ2) + rup(2 * (size_t)d.NY2);
     if ((r = c->alloc(tab, ntab))) return bail(r);
     size_t o = 0;
     auto put = [&](const void *src, size_t count) {
@@ -311,7 +312,10 @@ int cdns_create(const cdns_mesh_desc *m, const cdns_params *p, int precision, in
     auto pc = put(cosy.data(), cosy.size()); c->t.cosy = pc.first;
     auto px = put(rx.data(), 2 * rx.size()); c->t.root_x = reinterpret_cast<const double2 *>(px.first);
     auto pzz = put(rz.data(), 2 * rz.size()); c->t.root_z = reinterpret_cast<const double2 *>(pzz.first);
-    if (pw.second || pz.second || pl.second || pd.second || pr.second || pc.second || px.second || pzz.second)
+    auto pyy = put(ry.data(), 2 * ry.size()); c->t.root_y = reinterpret_cast<const double2 *>(pyy.first);
+
+    if (pw.second || pz.second || pl.second || pd.second || pr.second || pc.second || px.second || pzz.second ||
+        pyy.second)
         return bail(CDNS_ERR_CUDA);
     {
         size_t nsyn, nana;
@@ -354,6 +358,7 @@ int cdns_create(const cdns_mesh_desc *m, const cdns_params *p, int precision, in
     bc[(2 * 1 + 0) * nc + zc] = make_double2(p->V_Microblow0, 0.0);
     bc[(2 * 1 + 1) * nc + zc] = make_double2(p->V_Microblow0, 0.0);
     if ((r = upload(c, c->bc_v, bc.data(), bc.size() * sizeof(double2)))) return bail(r);
+    if ((r = tune_context(c, false))) return bail(r);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(fail(CDNS_ERR_CUDA, "sync"));
     *out = c;
     return CDNS_OK;

@@ -100,6 +100,8 @@ void enqueue_nonlinear(cdns_ctx *c, const double2 *u, double2 *N, bool prof, int
                        double2 *G_fp64 = nullptr);
 // Solver state of c for wall-normal Helmholtz constant g_v (no-op if current).
 int do_setup(cdns_ctx *c, double g_v);
+// Launch shapes of c (z line width, Chebyshev transform forms): cached or timed (tune.cu).
+int tune_context(cdns_ctx *c, bool force);
 
 struct DeviceGuard {
     int prev = -1;

@@ -230,15 +230,16 @@ int ensure_output(cdns_ctx *c, bool snapshot) {
             }
             return rr;
         };
-        const auto rx = roots(dc.NX2), rz = roots(dc.NZ2);
+        const auto rx = roots(dc.NX2), rz = roots(dc.NZ2), ry = roots(dc.NY2);
         size_t nsyn, nana;
         cheb_table_sizes(dc, &nsyn, &nana);
         double *cy = nullptr, *csyn = nullptr, *cana = nullptr;
-        double2 *rxd = nullptr, *rzd = nullptr;
+        double2 *rxd = nullptr, *rzd = nullptr, *ryd = nullptr;
         const size_t Ns = (size_t)d.Ns, ny1 = dc.ny2;
         int r = 0;
         if ((r = oalloc(c, w, cy, cosy.size())) || (r = oalloc(c, w, csyn, nsyn)) || (r = oalloc(c, w, cana, nana)) ||
             (r = oalloc(c, w, rxd, rx.size())) || (r = oalloc(c, w, rzd, rz.size())) ||
+            (r = oalloc(c, w, ryd, ry.size())) ||
             (r = oalloc(c, w, w->pd, 2 * Ns)) || (r = oalloc(c, w, w->F, 5 * ny1 * d.ncol)) ||
             (r = oalloc(c, w, w->G, 5 * ny1 * dc.NZ2 * d.nkx)) ||
             (r = oalloc(c, w, w->partial, ny1 * moment_blocks(dc) * 22)) ||
@@ -247,6 +248,7 @@ int ensure_output(cdns_ctx *c, bool snapshot) {
         CK(cudaMemcpyAsync(cy, cosy.data(), cosy.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
         CK(cudaMemcpyAsync(rxd, rx.data(), rx.size() * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
         CK(cudaMemcpyAsync(rzd, rz.data(), rz.size() * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(ryd, ry.data(), ry.size() * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
         launch_cheb_tables(dc, cy, csyn, cana, c->stream);
         w->tc = c->t;
         w->tc.cosy = cy;
@@ -254,6 +256,7 @@ int ensure_output(cdns_ctx *c, bool snapshot) {
         w->tc.cana = cana;
         w->tc.root_x = rxd;
         w->tc.root_z = rzd;
+        w->tc.root_y = ryd;
         w->ccw = clenshaw_curtis(dc.NY2);
         CK(configure_transform_kernels(dc));
         CK(configure_cheb_kernels(dc));

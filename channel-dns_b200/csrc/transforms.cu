@@ -194,6 +194,150 @@ k_z_forward_r(Dims d, const double2 *__restrict__ roots, const C *__restrict__ H
 }
 
 // ---------------------------------------------------------------------------
+// Chebyshev synthesis and analysis as a DCT-I of N + 1 points, N = NY2 =
+// N1 x N2, through one length-N complex FFT per column (FP64).  For x_0..x_N,
+//   Y_j = (x_0 + (-1)^j x_N)/2 + sum_{n=1}^{N-1} x_n cos(pi n j / N):
+// with y_n = (x_n + x_{N-n})/2 - sin(pi n / N)(x_n - x_{N-n}) (n < N) and
+// Z = DFT_N(y), the even outputs are Y_2k = (Z_k + Z_{N-k})/2 and the odd ones
+// follow by a prefix sum, Y_{2k+1} = Y_1 + sum_{q=1..k} i (Z_q - Z_{N-q})/2,
+// with Y_1 = (x_0 - x_N)/2 + sum_{n=1}^{N-1} x_n cos(pi n / N).
+//   synthesis (ANA = false): x_0 = 2 c_0, x_k = c_k (k <= NYS), 0 beyond;
+//             f_j = Y_j for j = 0..N (the doubled c_0 and the z expansion's
+//             0.5 of the reference cancel, as in k_ysynth).
+//   analysis  (ANA = true):  x_j = F_j;  S_0 = Y_0 / N, S_k = 2 Y_k / N
+//             (the scalings 1/(2 NY2) and 1/NY2 with the DCT-I's doubled
+//             interior sum), k <= NYS.
+// Block = one (field, kz) plane x TL kx lines; loads and stores run along kx.
+// Shared memory: twiddles [N], x then the FFT exchange then the outputs
+// [(N+1)][TL], Z [N][TL], Y_1 [TL].  16 threads per line in the scan phases.
+// ---------------------------------------------------------------------------
+struct YdctSrc {
+    const double2 *X;
+    const double *cosy;
+    int TL, N;
+    __device__ __forceinline__ double2 operator()(int n, int l) const {
+        const double2 a = X[n * TL + l], b = X[(N - n) * TL + l];
+        const double s = cosy[(n + (3 * N) / 2) % (2 * N)];   // sin(pi n / N)
+        return csub(cscale(0.5, cadd(a, b)), cscale(s, csub(a, b)));
+    }
+};
+struct YdctDst {
+    double2 *Z;
+    int TL;
+    __device__ __forceinline__ void operator()(int k, int l, double2 v) const { Z[k * TL + l] = v; }
+};
+
+template <int N1, int N2, bool ANA>
+__global__ void __launch_bounds__(16 * 17)
+k_ydct_r(Dims d, const double2 *__restrict__ roots, const double *__restrict__ cosy, const double2 *src0,
+         const double2 *src1, int nsplit, double2 *__restrict__ out, int TL) {
+    constexpr int N = N1 * N2;
+    extern __shared__ double2 sm_d[];
+    double2 *X = sm_d + N;
+    double2 *Z = X + (N + 1) * TL;
+    double2 *Y1 = Z + N * TL;
+    const int f = blockIdx.z, kzi = blockIdx.y, kx0 = blockIdx.x * TL;
+    const int t = threadIdx.x, nt = blockDim.x;
+    const int nkx = d.nkx, ncy = d.ncy;
+    const Twiddles<double2> tw = load_twiddles<double2>(sm_d, roots, N);
+    // ---- x_n, n = 0..N ------------------------------------------------------
+    if (!ANA) {
+        const double2 *S = (f < nsplit ? src0 + (long long)f * d.Ns : src1 + (long long)(f - nsplit) * d.Ns) +
+                           (long long)kzi * ncy * nkx;
+        for (int i = t; i < (N + 1) * TL; i += nt) {
+            const int n = i / TL, l = i - (i / TL) * TL, kx = kx0 + l;
+            double2 v = (n < ncy && kx < nkx) ? S[(long long)n * nkx + kx] : mk(0.0, 0.0);
+            X[i] = n == 0 ? cadd(v, v) : v;
+        }
+    } else {
+        const double2 *F = src0 + (long long)f * d.ny2 * d.fcol + (long long)kzi * nkx;
+        for (int i = t; i < (N + 1) * TL; i += nt) {
+            const int n = i / TL, l = i - (i / TL) * TL, kx = kx0 + l;
+            X[i] = kx < nkx ? F[(long long)n * d.fcol + kx] : mk(0.0, 0.0);
+        }
+    }
+    __syncthreads();
+    const int l = t >> 4, sub = t & 15;
+    // ---- Y_1 per line (16 threads) -------------------------------------------
+    {
+        double2 acc = mk(0.0, 0.0);
+        if (l < TL) {
+            for (int n = 1 + sub; n < N; n += 16) acc = cadd(acc, cscale(cosy[n], X[n * TL + l]));
+            if (sub == 0) acc = cadd(acc, cscale(0.5, csub(X[l], X[N * TL + l])));
+        }
+#pragma unroll
+        for (int m = 8; m > 0; m >>= 1) {
+            acc.x += __shfl_xor_sync(0xffffffffu, acc.x, m, 16);
+            acc.y += __shfl_xor_sync(0xffffffffu, acc.y, m, 16);
+        }
+        if (l < TL && sub == 0) Y1[l] = acc;
+    }
+    // ---- Z = DFT_N(y) (the exchange buffer aliases X: read before its barrier)
+    fft2_lines<N1, N2, -1>(TL, tw, X, YdctSrc{X, cosy, TL, N}, YdctDst{Z, TL});
+    __syncthreads();
+    // ---- outputs into X: even from Z pairs, odd by a prefix scan -----------
+    constexpr int M = N / 2 - 1;            // odd outputs beyond Y_1: k = 1..M
+    constexpr int CH = (M + 15) / 16;       // chunk of k per thread
+    if (l < TL) {
+        for (int k = sub; k <= N / 2; k += 16) {
+            const double2 zk = Z[k * TL + l], zm = Z[((N - k) % N) * TL + l];
+            X[(2 * k) * TL + l] = cscale(0.5, cadd(zk, zm));
+        }
+    }
+    {
+        double2 part[CH];
+        double2 run = mk(0.0, 0.0);
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            const int k = 1 + sub * CH + c;
+            if (l < TL && k <= M) {
+                const double2 dz = csub(Z[k * TL + l], Z[(N - k) * TL + l]);
+                run = cadd(run, mk(-0.5 * dz.y, 0.5 * dz.x));   // i (Z_k - Z_{N-k}) / 2
+            }
+            part[c] = run;
+        }
+        // exclusive scan of the chunk totals over the 16 lanes of the line
+        double2 ex = run;
+#pragma unroll
+        for (int m = 1; m < 16; m <<= 1) {
+            const double ux = __shfl_up_sync(0xffffffffu, ex.x, m, 16);
+            const double uy = __shfl_up_sync(0xffffffffu, ex.y, m, 16);
+            if (sub >= m) {
+                ex.x += ux;
+                ex.y += uy;
+            }
+        }
+        double2 carry = mk(__shfl_up_sync(0xffffffffu, ex.x, 1, 16), __shfl_up_sync(0xffffffffu, ex.y, 1, 16));
+        if (sub == 0) carry = mk(0.0, 0.0);
+        if (l < TL) {
+            const double2 y1 = Y1[l];
+            if (sub == 0) X[1 * TL + l] = y1;
+#pragma unroll
+            for (int c = 0; c < CH; ++c) {
+                const int k = 1 + sub * CH + c;
+                if (k <= M) X[(2 * k + 1) * TL + l] = cadd(y1, cadd(carry, part[c]));
+            }
+        }
+    }
+    __syncthreads();
+    // ---- store along kx ------------------------------------------------------
+    if (!ANA) {
+        double2 *Fo = out + (long long)f * d.ny2 * d.fcol + (long long)kzi * nkx;
+        for (int i = t; i < (N + 1) * TL; i += nt) {
+            const int j = i / TL, ll = i - (i / TL) * TL, kx = kx0 + ll;
+            if (kx < nkx) Fo[(long long)j * d.fcol + kx] = X[i];
+        }
+    } else {
+        double2 *So = out + (long long)f * d.Ns + (long long)kzi * ncy * nkx;
+        const double s0 = 1.0 / (double)N, sk = 2.0 / (double)N;
+        for (int i = t; i < ncy * TL; i += nt) {
+            const int k = i / TL, ll = i - (i / TL) * TL, kx = kx0 + ll;
+            if (kx < nkx) So[(long long)k * nkx + kx] = cscale(k == 0 ? s0 : sk, X[i]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // K3: inverse x FFT of the six fields, u x omega, forward x FFT of the three
 // products.  Block = RW rows (z, j); real rows are packed in pairs into one
 // complex line (a + i b); c2r drops the imaginary parts of the DC and Nyquist
@@ -997,13 +1141,24 @@ constexpr int kRWs = 8;
 
 // Lines per z-FFT block: the width in [8, 17] that tiles NXS+1 with the least
 // padding (13 for 65 modes).
+constexpr int kMaxZLines = 17;   // z-transform (and y FFT form) kx lines per block: 8..17
 int z_lines(const Dims &d) {
+    if (d.ztl >= 8 && d.ztl <= kMaxZLines) return d.ztl;
     int best = 16, waste = 1 << 30;
     for (int tl = 17; tl >= 8; --tl) {
         const int w = ((d.nkx + tl - 1) / tl) * tl - d.nkx;
         if (w < waste) { waste = w; best = tl; }
     }
     return best;
+}
+
+size_t smem_ydct(const Dims &d, int n) {
+    return sizeof(double2) * ((size_t)n + (size_t)(2 * n + 2) * z_lines(d));
+}
+// Dims with the widest line tile, for raising the kernels' shared-memory limits
+Dims widest_lines(Dims d) {
+    d.ztl = kMaxZLines;
+    return d;
 }
 
 size_t smem_zfft(const Dims &d) { return sizeof(double2) * (size_t)d.NZ2 * (1 + 2 * z_lines(d)); }
@@ -1064,10 +1219,21 @@ template <class C> cudaError_t configure_register_forms(const Dims &d) {
     if (e != cudaSuccess) return e;
     with_xsplit(d.NZ2, [&](auto a, auto b) {
         constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
-        const int sm = (int)smem_zfft_r(d, N1, N2, sizeof(C));
+        const int sm = (int)smem_zfft_r(widest_lines(d), N1, N2, sizeof(C));
         e = raise_smem(k_z_backward_r<N1, N2, C>, sm);
         if (e == cudaSuccess)
             e = raise_smem(k_z_forward_r<N1, N2, C>, sm);
+    });
+    return e;
+}
+
+cudaError_t configure_ydct(const Dims &d) {
+    cudaError_t e = cudaSuccess;
+    with_xsplit(d.NY2, [&](auto a, auto b) {
+        constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
+        const int sm = (int)smem_ydct(widest_lines(d), N1 * N2);
+        e = raise_smem(k_ydct_r<N1, N2, true>, sm);
+        if (e == cudaSuccess) e = raise_smem(k_ydct_r<N1, N2, false>, sm);
     });
     return e;
 }
@@ -1079,11 +1245,13 @@ bool register_forms(const Dims &d) {
 cudaError_t configure_transform_kernels(const Dims &d) {
     cudaError_t e = configure_register_forms<double2>(d);
     if (e != cudaSuccess) return e;
+    e = configure_ydct(d);
+    if (e != cudaSuccess) return e;
     e = configure_register_forms<float2>(d);
     if (e != cudaSuccess) return e;
-    e = raise_smem(k_z_backward, (int)smem_zfft(d));
+    e = raise_smem(k_z_backward, (int)smem_zfft(widest_lines(d)));
     if (e != cudaSuccess) return e;
-    e = raise_smem(k_z_forward, (int)smem_zfft(d));
+    e = raise_smem(k_z_forward, (int)smem_zfft(widest_lines(d)));
     if (e != cudaSuccess) return e;
     e = raise_smem(k_x_cross, (int)smem_xcross(d));
     if (e != cudaSuccess) return e;
@@ -1174,6 +1342,25 @@ void launch_x_adjoint(const Dims &d, const FftPlan &P, const double2 *roots, con
     if (reg) return;
     dim3 grid((d.NZ2 + kRWa - 1) / kRWa, d.ny2);
     k_x_adjoint<<<grid, 256, smem_xadjoint(d), s>>>(d, P, roots, G, L, kRWa);
+}
+
+bool ydct_available(const Dims &d, const Tables &t) {
+    return t.root_y && d.NY2 % 2 == 0 && with_xsplit(d.NY2, [](auto, auto) {});
+}
+
+bool launch_ydct(const Dims &d, const Tables &t, const double2 *src0, const double2 *src1, int nsplit, int nf,
+                 double2 *out, bool ana, cudaStream_t s) {
+    if (!ydct_available(d, t)) return false;
+    const int tl = z_lines(d);
+    dim3 grid((d.nkx + tl - 1) / tl, d.nkz, nf);
+    return with_xsplit(d.NY2, [&](auto a, auto b) {
+        constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
+        const size_t sm = smem_ydct(d, N1 * N2);
+        if (ana)
+            k_ydct_r<N1, N2, true><<<grid, 16 * tl, sm, s>>>(d, t.root_y, t.cosy, src0, src1, nsplit, out, tl);
+        else
+            k_ydct_r<N1, N2, false><<<grid, 16 * tl, sm, s>>>(d, t.root_y, t.cosy, src0, src1, nsplit, out, tl);
+    });
 }
 
 int moment_blocks(const Dims &d) { return (d.NZ2 + kRWm - 1) / kRWm; }

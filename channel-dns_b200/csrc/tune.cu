@@ -1,0 +1,238 @@
+// Launch-shape autotuner for sm_100a: the analogue of the reference's FFTW
+// planning with MEASURE and its wisdom files (src/fft/transforms.cpp:190-278,
+// src/fft/wisdom.cpp:11-32).
+//
+// For each mesh, the first FP64 context times on its own device buffers, with
+// CUDA events on its stream,
+//   - the kx lines per block of the z transforms (8..17): the z synthesis of
+//     the six nonlinear-term fields plus the z analysis of three, and
+//   - the Chebyshev synthesis (six fields) and analysis (three fields) in the
+//     matrix form (FP64 MMA products) and in the FFT form (DCT-I through one
+//     length-NY2 FFT per column; meshes whose NY2 has a register split),
+// keeps the fastest of each, and caches the choice for the process under a key
+// of the mesh and the device.  cdns_wisdom_export / cdns_wisdom_import write
+// and read that cache as JSON so that later processes skip the timing.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <sstream>
+
+#include "context.cuh"
+
+namespace cdns {
+
+namespace {
+
+struct Choice {
+    int ztl = 0;     // 0: the padding rule
+    int yform = 0;   // bit 0 synthesis, bit 1 analysis in the FFT form
+};
+
+std::mutex g_mu;
+std::map<std::string, Choice> g_wisdom;
+
+std::string mesh_key(const cdns_ctx *c) {
+    cudaDeviceProp prop{};
+    cudaGetDeviceProperties(&prop, c->device);
+    const Dims &d = c->d;
+    char buf[256];
+    std::snprintf(buf, sizeof buf, "%s/%d|%d,%d,%d|%d,%d,%d", prop.name, prop.multiProcessorCount, d.NX2, d.NY2,
+                  d.NZ2, d.NXS, d.NYS, d.NZS);
+    return buf;
+}
+
+// Best (minimum) of `reps` timed runs of fn on the context stream, in ms.
+template <typename Fn> int time_min(cdns_ctx *c, int reps, Fn fn, float &best) {
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    best = 1e30f;
+    fn();   // warm-up
+    for (int r = 0; r < reps; ++r) {
+        CK(cudaEventRecord(a, c->stream));
+        fn();
+        CK(cudaEventRecord(b, c->stream));
+        CK(cudaEventSynchronize(b));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, a, b));
+        if (ms < best) best = ms;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    CK(cudaGetLastError());
+    return CDNS_OK;
+}
+
+int measure(cdns_ctx *c, Choice &out) {
+    const Dims base = c->d;
+    cudaStream_t s = c->stream;
+    const int reps = 3;
+    // z transforms: 6 fields backward + 3 forward, as in the step
+    float best = 1e30f;
+    int best_tl = 0;
+    for (int tl = 8; tl <= 17; ++tl) {
+        Dims d = base;
+        d.ztl = tl;
+        float ms;
+        int r = time_min(c, reps, [&] {
+            launch_z_backward(d, c->pz, c->t.root_z, c->F, c->G, 6, s);
+            launch_z_forward(d, c->pz, c->t.root_z, c->H, c->F, 3, s);
+        }, ms);
+        if (r) return r;
+        if (ms < best) {
+            best = ms;
+            best_tl = tl;
+        }
+    }
+    out.ztl = best_tl;
+    Dims d = base;
+    d.ztl = best_tl;
+    out.yform = 0;
+    if (ydct_available(d, c->t)) {
+        Tables t = c->t;
+        float m_syn, f_syn, m_ana, f_ana;
+        int r = 0;
+        t.yform = 0;
+        if ((r = time_min(c, reps, [&] { launch_ysynth(d, t, c->U[0], c->om, 3, 6, c->F, s); }, m_syn))) return r;
+        if ((r = time_min(c, reps, [&] { launch_yanalysis(d, t, c->F, c->aux, 3, s); }, m_ana))) return r;
+        t.yform = 3;
+        if ((r = time_min(c, reps, [&] { launch_ysynth(d, t, c->U[0], c->om, 3, 6, c->F, s); }, f_syn))) return r;
+        if ((r = time_min(c, reps, [&] { launch_yanalysis(d, t, c->F, c->aux, 3, s); }, f_ana))) return r;
+        out.yform = (f_syn < m_syn ? 1 : 0) | (f_ana < m_ana ? 2 : 0);
+    }
+    return CDNS_OK;
+}
+
+void apply(cdns_ctx *c, const Choice &ch) {
+    c->d.ztl = ch.ztl;
+    c->t.yform = ch.yform;
+    // CDNS_Y_TRANSFORM=matrix|fft fixes the Chebyshev form (comparisons, tests)
+    if (const char *e = std::getenv("CDNS_Y_TRANSFORM")) {
+        if (std::strcmp(e, "matrix") == 0) c->t.yform = 0;
+        else if (std::strcmp(e, "fft") == 0) c->t.yform = 3;
+    }
+}
+
+}  // namespace
+
+// Picks the launch shapes of an FP64 context: from the process cache or the
+// wisdom, else by timing (unless CDNS_TUNE=0, which keeps the fixed rules).
+int tune_context(cdns_ctx *c, bool force) {
+    if (c->mixed) return CDNS_OK;   // FP32 stage buffers keep the rule-based shapes
+    const std::string key = mesh_key(c);
+    Choice ch;
+    bool have = false;
+    if (!force) {
+        std::lock_guard<std::mutex> lk(g_mu);
+        auto it = g_wisdom.find(key);
+        if (it != g_wisdom.end()) {
+            ch = it->second;
+            have = true;
+        }
+    }
+    const char *env = std::getenv("CDNS_TUNE");
+    if (!have && !force && env && std::strcmp(env, "0") == 0) {
+        apply(c, Choice{});
+        return CDNS_OK;
+    }
+    if (!have) {
+        int r = measure(c, ch);
+        if (r) return r;
+        std::lock_guard<std::mutex> lk(g_mu);
+        g_wisdom[key] = ch;
+    }
+    apply(c, ch);
+    return CDNS_OK;
+}
+
+}  // namespace cdns
+
+using namespace cdns;
+
+extern "C" {
+
+int cdns_tune(cdns_ctx *c) {
+    if (!c) return fail(CDNS_ERR_ARG, "null context");
+    DeviceGuard guard(c->device);
+    for (auto &g : c->graph)
+        if (g) {
+            cudaGraphExecDestroy(g);   // captured with the previous shapes
+            g = nullptr;
+        }
+    int r = tune_context(c, true);
+    if (r) return r;
+    CK(cudaStreamSynchronize(c->stream));
+    return CDNS_OK;
+}
+
+int cdns_get_tuning(cdns_ctx *c, int *out) {
+    if (!c || !out) return fail(CDNS_ERR_ARG, "null argument");
+    out[0] = c->d.ztl;
+    out[1] = c->t.yform & 1;
+    out[2] = (c->t.yform >> 1) & 1;
+    return CDNS_OK;
+}
+
+int cdns_wisdom_export(const char *path) {
+    if (!path) return fail(CDNS_ERR_ARG, "null path");
+    std::ostringstream o;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        o << "{\"cdns_wisdom\": 1, \"entries\": [";
+        bool first = true;
+        for (const auto &kv : g_wisdom) {
+            o << (first ? "" : ", ") << "{\"key\": \"" << kv.first << "\", \"ztl\": " << kv.second.ztl
+              << ", \"yform\": " << kv.second.yform << "}";
+            first = false;
+        }
+        o << "]}\n";
+    }
+    // write beside and rename, as the reference's wisdom export does
+    const std::string tmp = std::string(path) + ".tmp";
+    {
+        std::ofstream f(tmp, std::ios::trunc);
+        if (!f) return fail(CDNS_ERR_ARG, std::string("cannot write ") + tmp);
+        f << o.str();
+        if (!f) return fail(CDNS_ERR_ARG, std::string("cannot write ") + tmp);
+    }
+    if (std::rename(tmp.c_str(), path) != 0) return fail(CDNS_ERR_ARG, std::string("cannot rename to ") + path);
+    return CDNS_OK;
+}
+
+int cdns_wisdom_import(const char *path) {
+    if (!path) return fail(CDNS_ERR_ARG, "null path");
+    std::ifstream f(path);
+    if (!f) return fail(CDNS_ERR_ARG, std::string("cannot read ") + path);
+    std::stringstream ss;
+    ss << f.rdbuf();
+    const std::string t = ss.str();
+    if (t.find("\"cdns_wisdom\": 1") == std::string::npos) return fail(CDNS_ERR_ARG, "not a cdns wisdom file");
+    std::map<std::string, Choice> got;
+    size_t pos = 0;
+    while ((pos = t.find("{\"key\": \"", pos)) != std::string::npos) {
+        pos += 9;
+        const size_t end = t.find('"', pos);
+        if (end == std::string::npos) return fail(CDNS_ERR_ARG, "malformed wisdom entry");
+        const std::string key = t.substr(pos, end - pos);
+        Choice ch;
+        if (std::sscanf(t.c_str() + end, "\", \"ztl\": %d, \"yform\": %d}", &ch.ztl, &ch.yform) != 2 ||
+            ch.ztl < 0 || ch.ztl > 17 || (ch.ztl != 0 && ch.ztl < 8) || ch.yform < 0 || ch.yform > 3)
+            return fail(CDNS_ERR_ARG, "malformed wisdom entry");
+        got[key] = ch;
+        pos = end;
+    }
+    std::lock_guard<std::mutex> lk(g_mu);
+    for (const auto &kv : got) g_wisdom[kv.first] = kv.second;
+    return CDNS_OK;
+}
+
+int cdns_wisdom_forget(void) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_wisdom.clear();
+    return CDNS_OK;
+}
+
+}  // extern "C"

@@ -46,11 +46,13 @@ def test_mixed_nonlinear_term_48():
     assert np.abs(B32 - B64).max() <= 1e-5 * scale
 
 
-def test_mixed_stage_buffers_are_fp32_rounded():
+def test_mixed_stage_buffers_are_fp32_rounded(monkeypatch):
     """The synthesised vorticity of the mixed path is the FP64 one rounded to
     FP32 (fields 3-5 of the synthesis buffer; 0-2 are reused by the forward z
     transform), except the (kz, kx) = (0, 0) mean profile, which stays FP64
-    outside the FP32 stages and is zero there."""
+    outside the FP32 stages and is zero there.  Both synthesise in the matrix
+    form (the FP32 stages have no FFT form)."""
+    monkeypatch.setenv("CDNS_Y_TRANSFORM", "matrix")
     m, p = channel_case(32)
     u = np.stack(divergence_free_field(m, p, seed=2, amp=0.05, kmax=4), axis=-1)
     c64, c32 = ctx_for(m, p), mixed_ctx_for(m, p)
