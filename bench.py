@@ -258,11 +258,14 @@ def run_ensemble(members: int, K: int, W: int, precision: int, device: int, seed
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     points = int(sum(int(n) * (int(n) + 1) * int(n) for n in sizes))
+    tunings = {}
+    for ctx, n in zip(batch.members, sizes):
+        tunings.setdefault(str(int(n)), ctx.tuning())
     batch.close()
     return {"members": members, "steps": K, "ms_per_batch_step": ms / K,
             "grid_points_steps_per_s": points * K / (ms / 1000.0), "grid_points": points,
             "sizes": {str(n): int((sizes == n).sum()) for n in (32, 48, 64, 96)},
-            "re_tau_range": [float(res.min()), float(res.max())]}
+            "re_tau_range": [float(res.min()), float(res.max())], "tuning": tunings}
 
 
 def run_adjoint(device: int, seed: int, reps: int = 3) -> dict:
@@ -559,7 +562,7 @@ def main():
             "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": K,
             "warmup": W, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(WORKLOAD, parallelism=f"replicas{world}",
+            "config": dict(WORKLOAD, parallelism=f"replicas{world}", tuning=ctx.tuning(),
                            grid_points_steps_per_s=value * 128 * 129 * 128,
                            product_points_steps_per_s=value * 196 * 193 * 196,
                            step_model_bytes=step_model,

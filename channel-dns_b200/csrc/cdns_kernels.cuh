@@ -61,11 +61,11 @@ bool ydct_available(const Dims &d, const Tables &t);
 bool launch_ydct(const Dims &d, const Tables &t, const double2 *src0, const double2 *src1, int nsplit, int nf,
                  double2 *out, bool ana, cudaStream_t s);
 // Output reduction, x stage on the coarse grid (Dims of the coarse grid):
-// c2r of G[5] (u, v, w, p, div), per-point moments summed per block into
-// partial[NY+1][moment_blocks][22]; phys (may be null) receives u, v, w, p.
+// c2r of G[nf] (u, v, w, p and, if nf = 5, div), per-point moments summed per
+// block into partial[NY+1][moment_blocks][22]; phys (may be null) receives u, v, w, p.
 int moment_blocks(const Dims &d);
 void launch_x_moments(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G, double *partial,
-                      double *phys, cudaStream_t s);
+                      double *phys, int nf, cudaStream_t s);
 // Transpose of x_cross about the forward fields G[6]: L[0..2] = lH in, L[0..5] = lG out.
 void launch_x_adjoint(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G, double2 *L,
                       cudaStream_t s);

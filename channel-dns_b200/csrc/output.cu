@@ -285,15 +285,23 @@ int ensure_output(cdns_ctx *c, bool snapshot) {
 }
 
 // Plane sums of the current state into w->planes (stream-ordered, no sync).
-int enqueue_reduction(cdns_ctx *c, bool snapshot) {
+// check = true adds the divergence (sum 20) and the spectral finite check of
+// a check step; a statistics sample needs neither and synthesises u, v, w, p
+// straight from the state.
+int enqueue_reduction(cdns_ctx *c, bool snapshot, bool check) {
     OutputWork *w = c->outw;
     const Dims &d = c->d, &dc = w->dc;
     cudaStream_t s = c->stream;
     CK(cudaMemsetAsync(w->flag, 0, sizeof(unsigned), s));
-    launch_divergence(d, c->t, c->U[c->cur], c->p, w->pd, w->flag, s);
-    launch_ysynth(dc, w->tc, c->U[c->cur], w->pd, 3, 5, w->F, s);
-    launch_z_backward(dc, w->pz, w->tc.root_z, w->F, w->G, 5, s, true);
-    launch_x_moments(dc, w->px, w->tc.root_x, w->G, w->partial, snapshot ? w->phys : nullptr, s);
+    if (check) {
+        launch_divergence(d, c->t, c->U[c->cur], c->p, w->pd, w->flag, s);
+        launch_ysynth(dc, w->tc, c->U[c->cur], w->pd, 3, 5, w->F, s);
+    } else {
+        launch_ysynth(dc, w->tc, c->U[c->cur], c->p, 3, 4, w->F, s);
+    }
+    const int nf = check ? 5 : 4;
+    launch_z_backward(dc, w->pz, w->tc.root_z, w->F, w->G, nf, s, true);
+    launch_x_moments(dc, w->px, w->tc.root_x, w->G, w->partial, snapshot ? w->phys : nullptr, nf, s);
     k_plane_finalize<<<dc.ny2, 32, 0, s>>>(moment_blocks(dc), w->partial, w->planes);
     CK(cudaGetLastError());
     return CDNS_OK;
@@ -311,7 +319,7 @@ int cdns_output_reduce(cdns_ctx *c, int higher, double *plane_sums, double *diag
     if (!c->have_velocity) return fail(CDNS_ERR_STATE, "cdns_output_reduce before cdns_set_velocity");
     DeviceGuard guard(c->device);
     int r = ensure_output(c, physical != nullptr);
-    if (r || (r = enqueue_reduction(c, physical != nullptr))) return r;
+    if (r || (r = enqueue_reduction(c, physical != nullptr, true))) return r;
     OutputWork *w = c->outw;
     const Dims &dc = w->dc;
     cudaStream_t s = c->stream;
@@ -364,7 +372,7 @@ int cdns_statistics_sample(cdns_ctx *c) {
     if (!c->have_velocity) return fail(CDNS_ERR_STATE, "cdns_statistics_sample before cdns_set_velocity");
     DeviceGuard guard(c->device);
     int r = ensure_output(c, false);
-    if (r || (r = enqueue_reduction(c, false))) return r;
+    if (r || (r = enqueue_reduction(c, false, false))) return r;
     OutputWork *w = c->outw;
     const Dims &dc = w->dc;
     const double scale = 1.0 / ((double)dc.NX2 * (double)dc.NZ2);

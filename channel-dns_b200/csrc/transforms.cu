@@ -762,7 +762,8 @@ k_x_adjoint_r(Dims d, const double2 *__restrict__ roots, const double2 *__restri
 
 // ---------------------------------------------------------------------------
 // Output reduction, x stage (coarse grid): c2r of the five z-physical fields
-// u, v, w, p, div of RW rows (z, j) per block, then per point the moment
+// u, v, w, p, div (nf = 5; nf = 4: no divergence, div taken as 0) of RW rows
+// (z, j) per block, then per point the moment
 // terms of Statistics::reduce (src/sim/statistics.cpp:58-86) and div^2 of
 // Diagnostics::evaluate (src/sim/diagnostics.cpp:62-72), summed over the
 // block's points into partial[j][blockIdx.x][kMomentSlots]:
@@ -821,7 +822,7 @@ struct MomentAcc {
 template <int N1, int N2>
 __global__ void __launch_bounds__(16 * 3 * 4)
 k_x_moments_r(Dims d, const double2 *__restrict__ roots, const double2 *__restrict__ G, int RW,
-              double *__restrict__ partial, double *__restrict__ phys) {
+              double *__restrict__ partial, double *__restrict__ phys, int nf) {
     using C = double2;
     constexpr int n = N1 * N2;
     constexpr int SP = N2 + 1;
@@ -850,7 +851,7 @@ k_x_moments_r(Dims d, const double2 *__restrict__ roots, const double2 *__restri
             if (z < d.NZ2) {
                 const int mm = m <= nxs ? m : n - m;
                 if (m <= nxs || (m >= n - nxs && m != nyq)) {
-                    C A = rowA[mm], B = q < 2 ? rowB[mm] : mk(0.0, 0.0);
+                    C A = (2 * q < nf) ? rowA[mm] : mk(0.0, 0.0), B = q < 2 ? rowB[mm] : mk(0.0, 0.0);
                     if (mm == 0 || mm == nyq) {
                         A.y = 0.0;
                         B.y = 0.0;
@@ -910,7 +911,7 @@ k_x_moments_r(Dims d, const double2 *__restrict__ roots, const double2 *__restri
 // Stockham form of k_x_moments_r for any NX.
 __global__ void __launch_bounds__(256)
 k_x_moments(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 *__restrict__ G, int RW,
-            double *__restrict__ partial, double *__restrict__ phys) {
+            double *__restrict__ partial, double *__restrict__ phys, int nf) {
     extern __shared__ double2 sm[];
     __shared__ double red[32 * kMomentSlots];
     const int n = d.NX2;
@@ -935,7 +936,7 @@ k_x_moments(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 
         else { m = -1; mirror = false; }
         if (m >= 0 && z < d.NZ2) {
             const double2 *row = Gj + (long long)z * d.nkx + m + (2 * q) * fstride;
-            A = row[0];
+            if (2 * q < nf) A = row[0];
             if (q < 2) B = row[fstride];
             if (m == 0 || m == nyq) { A.y = 0.0; B.y = 0.0; }
             if (m == nyq) { A.x *= 2.0; B.x *= 2.0; }
@@ -1366,14 +1367,15 @@ bool launch_ydct(const Dims &d, const Tables &t, const double2 *src0, const doub
 int moment_blocks(const Dims &d) { return (d.NZ2 + kRWm - 1) / kRWm; }
 
 void launch_x_moments(const Dims &d, const FftPlan &P, const double2 *roots, const double2 *G, double *partial,
-                      double *phys, cudaStream_t s) {
+                      double *phys, int nf, cudaStream_t s) {
     dim3 grid(moment_blocks(d), d.ny2);
     const bool reg = with_xsplit(d.NX2, [&](auto a, auto b) {
         constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
-        k_x_moments_r<N1, N2><<<grid, 16 * 3 * kRWm, smem_xmoments_r(N1, N2), s>>>(d, roots, G, kRWm, partial, phys);
+        k_x_moments_r<N1, N2><<<grid, 16 * 3 * kRWm, smem_xmoments_r(N1, N2), s>>>(d, roots, G, kRWm, partial, phys,
+                                                                                 nf);
     });
     if (reg) return;
-    k_x_moments<<<grid, 256, smem_xmoments(d), s>>>(d, P, roots, G, kRWm, partial, phys);
+    k_x_moments<<<grid, 256, smem_xmoments(d), s>>>(d, P, roots, G, kRWm, partial, phys, nf);
 }
 
 // The coarse grid doubles (c2r) / halves (r2c) a full-spectrum x Nyquist bin
