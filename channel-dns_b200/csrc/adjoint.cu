@@ -177,7 +177,7 @@ struct AdjArgs {
 };
 
 template <int E>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kThreads, E <= 2 ? 2 : 1)
 k_solve_adj(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, AdjArgs A) {
     extern __shared__ double2 tile[];   // [4][ncy][TC]
     __shared__ double2 red[TC][TC][4];  // [warp][column][lc0, lc1, lsg0, lsg1]

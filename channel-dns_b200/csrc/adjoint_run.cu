@@ -285,8 +285,13 @@ int cdns_adjoint_run(cdns_ctx *c, int nsteps, int kck, int objective, const doub
     auto slot = [&](int seg, int it) { return w->gs + ((size_t)(seg & 1) * kck + (it - seg * kck - 1)) * gsz; };
     for (int it = 1; it <= nsteps; ++it) {
         if (grad && (it - 1) % kck == 0 && (r = save_checkpoint(c, (size_t)(it - 1) / kck))) return r;
-        double2 *G = (grad && it > s_last) ? slot(nseg - 1, it) : c->G;
-        forward_step(c, it, state_for(it), G, true);
+        if (it >= 3 && !(grad && it > s_last)) {
+            // steady steps into the context's own buffers: its captured step graphs
+            if ((r = one_step(c, it))) return r;
+        } else {
+            double2 *G = (grad && it > s_last) ? slot(nseg - 1, it) : c->G;
+            forward_step(c, it, state_for(it), G, true);
+        }
         if (shear) launch_wall_shear(d, c->U[c->cur], c->pp.Re, w->jbuf + it - 1, s);
     }
     CK(cudaGetLastError());

@@ -160,7 +160,7 @@ int do_setup(cdns_ctx *c, double g_v) {
 
 }  // namespace cdns
 
-namespace {
+namespace cdns {
 int one_step(cdns_ctx *c, int it) {
     if (!c->have_velocity) return fail(CDNS_ERR_STATE, "cdns_step before cdns_set_velocity");
     if (it < 1) return fail(CDNS_ERR_ARG, "iteration must be >= 1");
@@ -196,7 +196,7 @@ int one_step(cdns_ctx *c, int it) {
     return CDNS_OK;
 }
 
-}  // namespace
+}  // namespace cdns
 
 extern "C" {
 

@@ -100,6 +100,8 @@ void enqueue_nonlinear(cdns_ctx *c, const double2 *u, double2 *N, bool prof, int
                        double2 *G_fp64 = nullptr);
 // Solver state of c for wall-normal Helmholtz constant g_v (no-op if current).
 int do_setup(cdns_ctx *c, double g_v);
+// One step of cdns_step: setup if g changed, then the step (graph replay for it >= 3).
+int one_step(cdns_ctx *c, int it);
 // Launch shapes of c (z line width, Chebyshev transform forms): cached or timed (tune.cu).
 int tune_context(cdns_ctx *c, bool force);
 
