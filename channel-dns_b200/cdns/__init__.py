@@ -61,6 +61,10 @@ _SIGNATURES = {
     "cdns_output_reduce": [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
     "cdns_statistics_sample": [ctypes.c_void_p],
     "cdns_tune": [ctypes.c_void_p],
+    "cdns_write_restart": [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_longlong, ctypes.c_double, ctypes.c_int],
+    "cdns_read_restart": [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_longlong),
+                          ctypes.POINTER(ctypes.c_double)],
+    "cdns_write_physical": [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_longlong, ctypes.c_double, ctypes.c_int],
     "cdns_get_tuning": [ctypes.c_void_p, ctypes.c_void_p],
     "cdns_wisdom_export": [ctypes.c_char_p],
     "cdns_wisdom_import": [ctypes.c_char_p],
@@ -381,6 +385,20 @@ class Context:
 
     def statistics_reset(self) -> None:
         _check(lib().cdns_statistics_reset(self._h))
+
+    # ---- restart and physical files (the reference's formats) ----
+    def write_restart(self, path: str, step: int, time: float, text: bool = False) -> None:
+        _check(lib().cdns_write_restart(self._h, path.encode(), step, time, int(text)))
+
+    def read_restart(self, path: str):
+        """Sets the velocity from a restart file; returns (step, time)."""
+        s = ctypes.c_longlong(0)
+        t = ctypes.c_double(0.0)
+        _check(lib().cdns_read_restart(self._h, path.encode(), ctypes.byref(s), ctypes.byref(t)))
+        return int(s.value), float(t.value)
+
+    def write_physical(self, path: str, step: int, time: float, text: bool = False) -> None:
+        _check(lib().cdns_write_physical(self._h, path.encode(), step, time, int(text)))
 
     # ---- launch-shape tuning ----
     def tune(self) -> None:

@@ -169,6 +169,19 @@ int cdns_transform_coarse(cdns_ctx *ctx, int direction, const double *in, double
 int cdns_output_reduce(cdns_ctx *ctx, int higher_moments, double *plane_sums, double *diagnostics,
                        double *physical);
 
+/* Restart and physical-field files in the reference's formats (FieldIO,
+ * src/io/field_io.cpp:121-427, single rank), from and into the device state:
+ * text = 0 binary v1 (the driver's field_S_ 0.bin / field_P_ 0.bin), 1 text
+ * (*.dat).  The restart holds the velocity [..spectral..][3]; the physical
+ * file the to_physical snapshot u, v, w, p on the coarse grid.
+ * cdns_read_restart takes either form (it probes the magic), checks the
+ * header against the mesh and the payload for finite values, and sets the
+ * velocity (a first-order restart, as cdns_set_velocity).  Files are written
+ * beside the target and renamed over it. */
+int cdns_write_restart(cdns_ctx *ctx, const char *path, long long step, double time, int text);
+int cdns_read_restart(cdns_ctx *ctx, const char *path, long long *step, double *time);
+int cdns_write_physical(cdns_ctx *ctx, const char *path, long long step, double time, int text);
+
 /* Statistics sampling on the device (the `sample` branch of Simulation::run,
  * src/sim/simulation.cpp:227-250).  cdns_statistics_sample queues on the
  * context stream, with no host synchronisation, the reduction of the current

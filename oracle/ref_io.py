@@ -192,6 +192,24 @@ def reduce(m, p, velocity, pressure):
     return phys, planes, flags, values
 
 
+def dump(m, p, velocity, pressure, ntpit: int, time: float) -> dict:
+    """The reference's FieldIO files (format "both") of a state: returns
+    {file name: bytes} for field_S_ 0.bin/.dat and field_P_ 0.bin/.dat."""
+    d = tempfile.mkdtemp(prefix="cdns_ref_")
+    write_config(d, m, p, 1)
+    inp = os.path.join(d, "st.bin")
+    with open(inp, "wb") as fh:
+        fh.write(np.stack(velocity, axis=-1).astype("<c16").tobytes())
+        fh.write(np.asarray(pressure).astype("<c16").tobytes())
+    subprocess.run([RUNNER, "dump", d, inp, str(int(ntpit)), repr(float(time))], check=True, capture_output=True)
+    out = {}
+    for name in ("field_S_ 0.bin", "field_S_ 0.dat", "field_P_ 0.bin", "field_P_ 0.dat"):
+        with open(os.path.join(d, name), "rb") as fh:
+            out[name] = fh.read()
+    _rmtree(d)
+    return out
+
+
 def solve(m, p, g, rhs_v, bc_p, bc_v):
     d = tempfile.mkdtemp(prefix="cdns_ref_")
     write_config(d, m, p, 1)

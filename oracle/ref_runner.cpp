@@ -22,6 +22,10 @@
 //       FieldIO::to_physical, Statistics::reduce(higher, validate) and
 //       Diagnostics::evaluate; writes the physical u, v, w, p, the plane sums
 //       [NY+1][20], the plane finite flags and (EKT, TKE, div_L2, finite).
+//   ref_runner dump <run-dir> <state.bin> <ntpit> <time>
+//       FieldIO (format "both") on a given velocity and pressure: write_restart
+//       and, of the to_physical snapshot, write_physical, into <run-dir>
+//       (src/io/field_io.cpp:241-309): field_S_ 0.bin/.dat, field_P_ 0.bin/.dat.
 //   ref_runner solve <run-dir> <g> <rhs.bin> <out.bin>
 //       EqSolvePV::setup(g) then the fused solve_modes with fused RHS and
 //       sigma correction (src/solver/eqsolve_pv.cpp:311-450); input is the
@@ -81,7 +85,7 @@ void fill(Array4D<std::complex<double>> &f, const std::complex<double> *src) {
 
 int main(int argc, char **argv) {
     if (argc < 4) {
-        std::cerr << "usage: ref_runner run|nonlinear|fine|coarse|reduce|solve <run-dir> ...\n";
+        std::cerr << "usage: ref_runner run|nonlinear|fine|coarse|reduce|dump|solve <run-dir> ...\n";
         return 2;
     }
     const std::string mode = argv[1];
@@ -178,6 +182,21 @@ int main(int argc, char **argv) {
             const double v[4] = {values.ekt, values.tke, values.divergence_l2, values.finite ? 1.0 : 0.0};
             write(out, v, 4);
             return out ? 0 : 1;
+        }
+        if (mode == "dump" && argc >= 6) {
+            VectorField velocity = make_vector_field(mesh);
+            ScalarField pressure = make_scalar_field(mesh);
+            std::vector<std::complex<double>> buf(velocity.size() + pressure.size());
+            read_all(argv[3], buf);
+            fill(velocity, buf.data());
+            fill(pressure, buf.data() + velocity.size());
+            const std::int64_t ntpit = std::atoll(argv[4]);
+            const double t = std::atof(argv[5]);
+            FieldIO io(mesh, fft, dir, &mpi, OutputFormat::Both);
+            const auto &snapshot = io.to_physical(velocity, pressure, nullptr);
+            io.write_restart(ntpit, t, velocity);
+            io.write_physical(ntpit, t, snapshot);
+            return 0;
         }
         if (mode == "solve" && argc >= 6) {
             const double g = std::atof(argv[3]);

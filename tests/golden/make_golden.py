@@ -20,12 +20,14 @@ on small seeded inputs and stores inputs and outputs as compressed npz files:
                         spectrum (Nyquist halve/mirror branches, 16x17x16)
                         and a ragged one (NXS=5, NZS=6): a realisable and an
                         arbitrary spectrum each.
+  golden_files.npz      the reference's restart and physical files (field_S_,
+                        field_P_; binary v1 and text) of a 16x17x16 state.
   golden_reduce.npz     the output branch on a 16x17x16 state (a divergence-free
                         field plus a non-solenoidal part): physical u, v, w,
                         p, plane sums, finite flags, EKT/TKE/div_L2.
 
 Usage: python tests/golden/make_golden.py [name ...]   (needs oracle/_ref built;
-names: step example nonlinear solve fine coarse reduce, default all)
+names: step example nonlinear solve fine coarse reduce files, default all)
 """
 import os
 import sys
@@ -75,10 +77,27 @@ def coarse_and_reduce(which):
                             p=pres, phys=phys, planes=planes, flags=flags, values=values)
 
 
+def dump_files(which):
+    """golden_files.npz: the reference's restart and physical files (binary v1
+    and text) of a 16x17x16 state, as byte arrays, with the state."""
+    if "files" not in which:
+        return
+    m, p = channel_case(16)
+    u = divergence_free_field(m, p, seed=71, amp=0.1, spectrum="k53", mean="loglaw")
+    rng = np.random.default_rng(72)
+    pres = orc.coarse_forward(m, rng.standard_normal((m.NZ, m.NY + 1, m.NX)))
+    files = ref_io.dump(m, p, u, pres, 1234, 0.0625)
+    np.savez_compressed(os.path.join(HERE, "golden_files.npz"), **mesh_dict(m, p), u=np.stack(u), p=pres,
+                        ntpit=1234, time=0.0625,
+                        **{k.replace(" ", "_").replace(".", "_"): np.frombuffer(v, dtype=np.uint8)
+                           for k, v in files.items()})
+
+
 def main(which):
     if not ref_io.available():
         raise SystemExit("oracle/_ref is not built: run make -C oracle")
     coarse_and_reduce(which)
+    dump_files(which)
     if "step" not in which:
         print("golden fixtures written to", HERE)
         return
@@ -132,4 +151,4 @@ def _cheb_1my2(ncy):
 
 
 if __name__ == "__main__":
-    main(set(sys.argv[1:]) or {"step", "example", "nonlinear", "solve", "fine", "coarse", "reduce"})
+    main(set(sys.argv[1:]) or {"step", "example", "nonlinear", "solve", "fine", "coarse", "reduce", "files"})
