@@ -228,27 +228,31 @@ def ensemble_case(n: int, re: float):
     return mesh, params
 
 
-def run_ensemble(members: int, K: int, W: int, precision: int, device: int, seed: int) -> dict:
+def run_ensemble(members: int, K: int, W: int, precision: int, device: int, seed: int, world: int = 1,
+                 rank: int = 0, dist=None) -> dict:
     """Ensemble form: `members` channels with N drawn from {32, 48, 64, 96} and
-    Re_tau from U[100, 180] (seeded), laminar profile + 5 % divergence-free
-    perturbation on |k| <= 4; K graph-replayed steady steps after W warm-up
-    steps, timed with CUDA events on the batch stream."""
+    Re_tau from U[100, 180] (seeded, cdns.ensemble.members), laminar profile +
+    5 % divergence-free perturbation on |k| <= 4; K graph-replayed steady steps
+    after W warm-up steps, timed with CUDA events on the batch stream.  On N
+    GPUs the members are partitioned over the ranks by estimated bytes per step
+    (replicas only: no data crosses ranks); the time is the max over ranks."""
     import numpy as np
     import torch
     import cdns
+    from cdns.ensemble import imbalance, rank_members
     from cdns.fields import divergence_free_field
-    rng = np.random.default_rng(3)
-    sizes = rng.choice([32, 48, 64, 96], size=members)
-    res = rng.uniform(100.0, 180.0, size=members)
-    cases = [ensemble_case(int(n), float(r)) for n, r in zip(sizes, res)]
+    mine = rank_members(members, world, rank)
+    cases = [ensemble_case(n, re) for _, n, re in mine]
     batch = cdns.Batch([c[0] for c in cases], [c[1] for c in cases], device=device, precision=precision)
-    for i, (ctx, (mesh, params)) in enumerate(zip(batch.members, cases)):
+    for ctx, (i, _, _), (mesh, params) in zip(batch.members, mine, cases):
         u = divergence_free_field(mesh, params, seed=seed + i, amp=0.05, kmax=4)
         ctx.set_velocity(np.stack(u, axis=-1))
     batch.run(1, W)
     batch.synchronize()
     stream = torch.cuda.ExternalStream(batch.stream_ptr(), device=device)
     torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -257,15 +261,24 @@ def run_ensemble(members: int, K: int, W: int, precision: int, device: int, seed
     batch.synchronize()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
+    sizes = np.array([n for _, n, _ in mine], dtype=np.int64)
     points = int(sum(int(n) * (int(n) + 1) * int(n) for n in sizes))
     tunings = {}
     for ctx, n in zip(batch.members, sizes):
         tunings.setdefault(str(int(n)), ctx.tuning())
     batch.close()
+    if dist is not None:
+        t = torch.tensor([ms, float(points)], device=f"cuda:{device}", dtype=torch.float64)
+        tmax = t.clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        ms, points = float(tmax[0].item()), int(t[1].item())
+    res = np.array([re for _, _, re in mine])
     return {"members": members, "steps": K, "ms_per_batch_step": ms / K,
             "grid_points_steps_per_s": points * K / (ms / 1000.0), "grid_points": points,
+            "members_per_rank": len(mine), "partition_imbalance": imbalance(members, world),
             "sizes": {str(n): int((sizes == n).sum()) for n in (32, 48, 64, 96)},
-            "re_tau_range": [float(res.min()), float(res.max())], "tuning": tunings}
+            "re_tau_range": [float(res.min()), float(res.max())] if len(res) else None, "tuning": tunings}
 
 
 def run_adjoint(device: int, seed: int, reps: int = 3) -> dict:
@@ -522,7 +535,7 @@ def main():
         ensemble = {}
         for label, prec in (("fp64", cdns.PRECISION_FP64), ("mixed", cdns.PRECISION_MIXED)):
             ensemble[label] = run_ensemble(args.ensemble_members, args.ensemble_steps, W, prec, local,
-                                           1000 + rank)
+                                           1000, world, rank, dist)
 
     # ---- discrete-adjoint arm: gradient cost against the forward run ------
     adjoint = None
