@@ -406,11 +406,12 @@ class Context:
 
     def tuning(self) -> dict:
         """{"z_lines": kx lines per z-transform block (0: rule), "y_synthesis":
-        "fft" or "matrix", "y_analysis": "fft" or "matrix"}."""
-        out = np.zeros(3, dtype=np.int32)
+        "fft" or "matrix", "y_analysis": "fft" or "matrix", "x_rows": rows per
+        x-stage block (0: 4)}."""
+        out = np.zeros(4, dtype=np.int32)
         _check(lib().cdns_get_tuning(self._h, out.ctypes.data_as(ctypes.c_void_p)))
         return {"z_lines": int(out[0]), "y_synthesis": "fft" if out[1] else "matrix",
-                "y_analysis": "fft" if out[2] else "matrix"}
+                "y_analysis": "fft" if out[2] else "matrix", "x_rows": int(out[3])}
 
     # ---- discrete adjoint ----
     def adjoint_run(self, nsteps: int, checkpoint_interval: int, control: Optional[np.ndarray] = None,

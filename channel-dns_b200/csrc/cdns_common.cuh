@@ -23,6 +23,7 @@ struct Dims {
     int nyh;             // NY2/2+1 (half of the y points, symmetric pairs)
     long long Ns;        // nkz*ncy*nkx complex values per spectral component
     int ztl;             // kx lines per block of the z transforms (0: the padding rule)
+    int xrw;             // (z, y) rows per block of the register-form x stage (0: 4)
 };
 
 // Read-only per-context tables in device memory.

@@ -1279,11 +1279,12 @@ bool z_backward_r(const Dims &d, const double2 *roots, const C *F, C *G, int nf,
 }
 template <class C, bool MEAN>
 bool x_cross_r(const Dims &d, const double2 *roots, const C *G, C *H, const double *mean, cudaStream_t s) {
+    const int rw = (d.xrw == 2 || d.xrw == 4) ? d.xrw : kRWr;   // even, at most kRWr
     return with_xsplit(d.NX2, [&](auto a, auto b) {
         constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
-        dim3 grid((d.NZ2 + kRWr - 1) / kRWr, d.ny2);
-        k_x_cross_r<N1, N2, C, MEAN><<<grid, 16 * 3 * kRWr, smem_xcross_r(N1, N2, sizeof(C)), s>>>(
-            d, roots, G, H, kRWr, mean);
+        dim3 grid((d.NZ2 + rw - 1) / rw, d.ny2);
+        k_x_cross_r<N1, N2, C, MEAN><<<grid, 16 * 3 * rw, smem_xcross_r(N1, N2, sizeof(C)), s>>>(
+            d, roots, G, H, rw, mean);
     });
 }
 template <class C>

@@ -6,6 +6,7 @@
 // CUDA events on its stream,
 //   - the kx lines per block of the z transforms (8..17): the z synthesis of
 //     the six nonlinear-term fields plus the z analysis of three, and
+//   - the rows per block (2 or 4) of the register-form x stage,
 //   - the Chebyshev synthesis (six fields) and analysis (three fields) in the
 //     matrix form (FP64 MMA products) and in the FFT form (DCT-I through one
 //     length-NY2 FFT per column; meshes whose NY2 has a register split),
@@ -29,6 +30,7 @@ namespace {
 struct Choice {
     int ztl = 0;     // 0: the padding rule
     int yform = 0;   // bit 0 synthesis, bit 1 analysis in the FFT form
+    int xrw = 0;     // rows per block of the register-form x stage (0: 4)
 };
 
 std::mutex g_mu;
@@ -90,6 +92,21 @@ int measure(cdns_ctx *c, Choice &out) {
     out.ztl = best_tl;
     Dims d = base;
     d.ztl = best_tl;
+    // x stage: 2 or 4 rows per block (smaller blocks couple fewer warps at each barrier)
+    {
+        float best_x = 1e30f;
+        for (int rw : {4, 2}) {
+            Dims dx = d;
+            dx.xrw = rw;
+            float ms;
+            int r = time_min(c, reps, [&] { launch_x_cross(dx, c->px, c->t.root_x, c->G, c->H, s); }, ms);
+            if (r) return r;
+            if (ms < best_x) {
+                best_x = ms;
+                out.xrw = rw;
+            }
+        }
+    }
     out.yform = 0;
     if (ydct_available(d, c->t)) {
         Tables t = c->t;
@@ -108,6 +125,7 @@ int measure(cdns_ctx *c, Choice &out) {
 
 void apply(cdns_ctx *c, const Choice &ch) {
     c->d.ztl = ch.ztl;
+    c->d.xrw = ch.xrw;
     c->t.yform = ch.yform;
     // CDNS_Y_TRANSFORM=matrix|fft fixes the Chebyshev form (comparisons, tests)
     if (const char *e = std::getenv("CDNS_Y_TRANSFORM")) {
@@ -173,6 +191,7 @@ int cdns_get_tuning(cdns_ctx *c, int *out) {
     out[0] = c->d.ztl;
     out[1] = c->t.yform & 1;
     out[2] = (c->t.yform >> 1) & 1;
+    out[3] = c->d.xrw;
     return CDNS_OK;
 }
 
@@ -185,7 +204,7 @@ int cdns_wisdom_export(const char *path) {
         bool first = true;
         for (const auto &kv : g_wisdom) {
             o << (first ? "" : ", ") << "{\"key\": \"" << kv.first << "\", \"ztl\": " << kv.second.ztl
-              << ", \"yform\": " << kv.second.yform << "}";
+              << ", \"yform\": " << kv.second.yform << ", \"xrw\": " << kv.second.xrw << "}";
             first = false;
         }
         o << "]}\n";
@@ -218,8 +237,11 @@ int cdns_wisdom_import(const char *path) {
         if (end == std::string::npos) return fail(CDNS_ERR_ARG, "malformed wisdom entry");
         const std::string key = t.substr(pos, end - pos);
         Choice ch;
-        if (std::sscanf(t.c_str() + end, "\", \"ztl\": %d, \"yform\": %d}", &ch.ztl, &ch.yform) != 2 ||
-            ch.ztl < 0 || ch.ztl > 17 || (ch.ztl != 0 && ch.ztl < 8) || ch.yform < 0 || ch.yform > 3)
+        int n = std::sscanf(t.c_str() + end, "\", \"ztl\": %d, \"yform\": %d, \"xrw\": %d}", &ch.ztl,
+                            &ch.yform, &ch.xrw);
+        if (n == 2) ch.xrw = 0;   // entries written before the x-stage choice existed
+        if (n < 2 || ch.ztl < 0 || ch.ztl > 17 || (ch.ztl != 0 && ch.ztl < 8) || ch.yform < 0 || ch.yform > 3 ||
+            (ch.xrw != 0 && ch.xrw != 2 && ch.xrw != 4))
             return fail(CDNS_ERR_ARG, "malformed wisdom entry");
         got[key] = ch;
         pos = end;

@@ -206,13 +206,14 @@ int cdns_solve(cdns_ctx *ctx, double g, const double *rhs_velocity, const double
 
 /* Launch-shape autotuning (the analogue of FFTW planning and wisdom,
  * src/fft/transforms.cpp:190-278, src/fft/wisdom.cpp:11-32).  An FP64 context
- * picks, at creation, the kx lines per block of its z transforms and the form
+ * picks, at creation, the kx lines per block of its z transforms, the rows per
+ * block of its x stage and the form
  * of its Chebyshev synthesis and analysis (FP64 MMA matrix products or one
  * length-NY2 FFT per column), by timing the candidates on its own buffers the
  * first time a mesh is seen on a device in the process (CDNS_TUNE=0 in the
  * environment keeps fixed rules; CDNS_Y_TRANSFORM=matrix|fft fixes the
  * Chebyshev form).  cdns_tune times again; cdns_get_tuning writes
- * {z lines, synthesis FFT form, analysis FFT form} into out[3];
+ * {z lines, synthesis FFT form, analysis FFT form, x-stage rows} into out[4];
  * cdns_wisdom_export / _import save and load the choices as JSON (host-only
  * calls); cdns_wisdom_forget empties the process cache. */
 int cdns_tune(cdns_ctx *ctx);
