@@ -52,7 +52,7 @@ typedef enum {
  * FP32 (the y synthesis/analysis accumulate in FP64 and round to or from FP32
  * at the stage boundary); the curl, the tau solves, the influence and sigma
  * corrections, the pressure wall data and the mean-flow update stay FP64.
- * MIXED needs NX2 and NZ2 in {48, 72, 96, 144, 192, 196}. */
+ * MIXED needs NX2 and NZ2 in {32, 48, 64, 72, 96, 128, 144, 192, 196}. */
 typedef enum { CDNS_PRECISION_FP64 = 0, CDNS_PRECISION_MIXED = 1 } cdns_precision;
 
 /* Mesh, mirrors MeshParm (src/core/params.hpp:6-11) + XL/ZL
