@@ -242,7 +242,7 @@ int cdns_create(const cdns_mesh_desc *m, const cdns_params *p, int precision, in
     }
     if (precision == CDNS_PRECISION_MIXED && !register_forms(d)) {
         delete c;
-        return fail(CDNS_ERR_ARG, "mixed precision needs NX2 and NZ2 in {48, 72, 96, 144, 192, 196}");
+        return fail(CDNS_ERR_ARG, "mixed precision needs NX2 and NZ2 in {32, 48, 64, 72, 96, 128, 144, 192, 196}");
     }
     c->mixed = precision == CDNS_PRECISION_MIXED;
     d.fcol = c->mixed ? d.ncol + (d.ncol & 1) : d.ncol;
