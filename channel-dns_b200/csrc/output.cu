@@ -14,7 +14,10 @@
 // to HBM unless a snapshot is asked for.  Only (NY+1) x 22 plane sums come
 // back to the host, where EKT, TKE and the divergence L2 norm are formed in
 // the reference's order.
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
 
 #include "context.cuh"
 #include "warp_columns.cuh"
@@ -270,6 +273,36 @@ int ensure_output(cdns_ctx *c, bool snapshot) {
         }
         CK(e);
         CK(cudaGetLastError());   // (limits are only ever raised: the fine-grid launches stay valid)
+        // Chebyshev synthesis form on the coarse grid (four fields, as a statistics
+        // sample): the faster of the matrix and FFT forms, timed here (cf. tune.cu)
+        w->tc.yform = 0;
+        Tables tf = w->tc;
+        tf.yform = 3;
+        if (ydct_available(dc, tf) && !std::getenv("CDNS_Y_TRANSFORM")) {
+            cudaEvent_t a, b;
+            CK(cudaEventCreate(&a));
+            CK(cudaEventCreate(&b));
+            float best[2] = {1e30f, 1e30f};
+            for (int form = 0; form < 2; ++form) {
+                const Tables &tt = form ? tf : w->tc;
+                launch_ysynth(dc, tt, c->U[0], c->p, 3, 4, w->F, c->stream);   // warm-up
+                for (int rep = 0; rep < 3; ++rep) {
+                    CK(cudaEventRecord(a, c->stream));
+                    launch_ysynth(dc, tt, c->U[0], c->p, 3, 4, w->F, c->stream);
+                    CK(cudaEventRecord(b, c->stream));
+                    CK(cudaEventSynchronize(b));
+                    float ms = 0.f;
+                    CK(cudaEventElapsedTime(&ms, a, b));
+                    best[form] = std::min(best[form], ms);
+                }
+            }
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+            if (best[1] < best[0]) w->tc.yform = 1;
+        } else if (const char *e = std::getenv("CDNS_Y_TRANSFORM")) {
+            if (std::strcmp(e, "fft") == 0) w->tc.yform = 3;
+        }
+        CK(cudaGetLastError());
     }
     OutputWork *w = c->outw;
     if (!w->stats) {
