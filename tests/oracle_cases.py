@@ -2,7 +2,7 @@
 
 The cases restate the reference's test fixtures by value (the example case
 used by its unit tests: 32^3 grid, NXS=NZS=16, NYS=30, XL=ZL=10, Re=2800,
-constant flow rate, V_Microblow0=1e-3) and the north-star workloads (the
+constant flow rate, V_Microblow0=1e-3) and the benchmark workloads (the
 4pi x 2 x 2pi channel at Re_tau=180 with a 3/2-dealiased product grid).
 """
 from __future__ import annotations
@@ -35,7 +35,7 @@ def example_case(NXS=16, NYS=30, NZS=16, N2=32, a_v1=1.0, b_v1=0.0, N=32):
 
 
 def channel_case(n: int, Re: float = 180.0, dt: float = 5e-5):
-    """North-star channel: N x (N+1) x N base grid, NXS=NZS=N/2, NYS=N-2,
+    """Benchmark channel: N x (N+1) x N base grid, NXS=NZS=N/2, NYS=N-2,
     3/2 product grid, 4pi x 2 x 2pi, fixed pressure gradient."""
     n2 = 3 * n // 2
     m = orc.Mesh(n, n, n, n // 2, n - 2, n // 2, n2, n2, n2, 4.0 * PI, 2.0 * PI)
