@@ -35,6 +35,7 @@ struct Choice {
 
 std::mutex g_mu;
 std::map<std::string, Choice> g_wisdom;
+std::once_flag g_env_import;
 
 std::string mesh_key(const cdns_ctx *c) {
     cudaDeviceProp prop{};
@@ -135,11 +136,29 @@ void apply(cdns_ctx *c, const Choice &ch) {
 }
 
 }  // namespace
+}  // namespace cdns
+
+extern "C" int cdns_wisdom_import(const char *path);
+extern "C" int cdns_wisdom_export(const char *path);
+
+namespace cdns {
 
 // Picks the launch shapes of an FP64 context: from the process cache or the
 // wisdom, else by timing (unless CDNS_TUNE=0, which keeps the fixed rules).
+// CDNS_WISDOM=<file> imports that file once per process (if it exists) and
+// exports the cache to it after every new measurement, so that a later run --
+// a profiled one, whose timings would mislead the tuner -- reuses the choices.
 int tune_context(cdns_ctx *c, bool force) {
     if (c->mixed) return CDNS_OK;   // FP32 stage buffers keep the rule-based shapes
+    const char *wfile = std::getenv("CDNS_WISDOM");
+    if (wfile && *wfile) {
+        std::call_once(g_env_import, [&] {
+            if (std::FILE *f = std::fopen(wfile, "r")) {
+                std::fclose(f);
+                cdns_wisdom_import(wfile);   // a malformed file leaves the cache as it is
+            }
+        });
+    }
     const std::string key = mesh_key(c);
     Choice ch;
     bool have = false;
@@ -159,8 +178,11 @@ int tune_context(cdns_ctx *c, bool force) {
     if (!have) {
         int r = measure(c, ch);
         if (r) return r;
-        std::lock_guard<std::mutex> lk(g_mu);
-        g_wisdom[key] = ch;
+        {
+            std::lock_guard<std::mutex> lk(g_mu);
+            g_wisdom[key] = ch;
+        }
+        if (wfile && *wfile && (r = cdns_wisdom_export(wfile))) return r;
     }
     apply(c, ch);
     return CDNS_OK;
