@@ -218,6 +218,15 @@ def _ptr(a: np.ndarray) -> ctypes.c_void_p:
     return ctypes.c_void_p(a.ctypes.data)
 
 
+def _input(a, shape, dtype, name: str) -> np.ndarray:
+    """`a` as a C-contiguous array of `dtype`; ValueError unless its shape is
+    `shape`, the number of values the C call reads."""
+    a = np.ascontiguousarray(a, dtype=dtype)
+    if a.shape != tuple(shape):
+        raise ValueError(f"{name} must have shape {tuple(shape)}, got {a.shape}")
+    return a
+
+
 # cdns_precision (include/cdns.h)
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
@@ -263,9 +272,7 @@ class Context:
 
     # ---- state hand-over (reference layout) ----
     def set_velocity(self, u: np.ndarray) -> None:
-        u = np.ascontiguousarray(u, dtype=np.complex128)
-        if u.shape != self.mesh.spectral_shape + (3,):
-            raise ValueError(f"velocity must have shape {self.mesh.spectral_shape + (3,)}")
+        u = _input(u, self.mesh.spectral_shape + (3,), np.complex128, "velocity")
         _check(lib().cdns_set_velocity(self._h, _ptr(u)))
 
     def get_velocity(self) -> np.ndarray:
@@ -308,8 +315,8 @@ class Context:
 
     # ---- pieces of the hot path ----
     def nonlinear(self, u: np.ndarray):
-        u = np.ascontiguousarray(u, dtype=np.complex128)
         nkz, ncy, nkx = self.mesh.spectral_shape
+        u = _input(u, (nkz, ncy, nkx, 3), np.complex128, "velocity")
         N = np.empty((nkz, ncy, nkx, 3), dtype=np.complex128)
         B = np.empty((nkz, 2, nkx), dtype=np.complex128)
         _check(lib().cdns_nonlinear(self._h, _ptr(u), _ptr(N), _ptr(B)))
@@ -317,10 +324,10 @@ class Context:
 
     def transform_fine(self, direction: str, data: np.ndarray) -> np.ndarray:
         if direction == "B":
-            src = np.ascontiguousarray(data, dtype=np.complex128)
+            src = _input(data, self.mesh.spectral_shape, np.complex128, "spectral field")
             out = np.empty(self.mesh.fine_shape, dtype=np.float64)
         elif direction == "F":
-            src = np.ascontiguousarray(data, dtype=np.float64)
+            src = _input(data, self.mesh.fine_shape, np.float64, "physical field")
             out = np.empty(self.mesh.spectral_shape, dtype=np.complex128)
         else:
             raise ValueError("direction must be 'B' or 'F'")
@@ -329,9 +336,9 @@ class Context:
 
     def solve(self, g: float, rhs: np.ndarray, pressure_bc: np.ndarray, velocity_bc: np.ndarray):
         nkz, ncy, nkx = self.mesh.spectral_shape
-        rhs = np.ascontiguousarray(rhs, dtype=np.complex128)
-        pbc = np.ascontiguousarray(pressure_bc, dtype=np.complex128)
-        vbc = np.ascontiguousarray(velocity_bc, dtype=np.complex128)
+        rhs = _input(rhs, (nkz, ncy, nkx, 3), np.complex128, "rhs")
+        pbc = _input(pressure_bc, (nkz, 2, nkx), np.complex128, "pressure_bc")
+        vbc = _input(velocity_bc, (nkz, 2, nkx, 3), np.complex128, "velocity_bc")
         p = np.empty((nkz, ncy, nkx), dtype=np.complex128)
         v = np.empty((nkz, ncy, nkx, 3), dtype=np.complex128)
         units = np.empty(2 * ncy)
@@ -340,7 +347,7 @@ class Context:
         return p, v, units[:ncy].copy(), units[ncy:].copy()
 
     def set_pressure(self, p: np.ndarray) -> None:
-        p = np.ascontiguousarray(p, dtype=np.complex128)
+        p = _input(p, self.mesh.spectral_shape, np.complex128, "pressure")
         _check(lib().cdns_set_pressure(self._h, _ptr(p)))
 
     # ---- coarse grid and output reduction ----
@@ -349,11 +356,13 @@ class Context:
         physical [NZ][NY+1][NX], 'F' the inverse."""
         m = self.mesh
         if direction == "B":
-            src = np.ascontiguousarray(data, dtype=np.complex128)
+            src = _input(data, m.spectral_shape, np.complex128, "spectral field")
             out = np.empty((m.NZ, m.NY + 1, m.NX))
-        else:
-            src = np.ascontiguousarray(data, dtype=np.float64)
+        elif direction == "F":
+            src = _input(data, (m.NZ, m.NY + 1, m.NX), np.float64, "physical field")
             out = np.empty(m.spectral_shape, dtype=np.complex128)
+        else:
+            raise ValueError("direction must be 'B' or 'F'")
         _check(lib().cdns_transform_coarse(self._h, ord(direction), _ptr(src), _ptr(out)))
         return out
 
@@ -423,8 +432,8 @@ class Context:
         time-averaged wall shear stress, or Re <weights, u^nsteps> when
         weights (velocity layout) are given.  Returns (J, gu, gbc)."""
         nkz, ncy, nkx = self.mesh.spectral_shape
-        ctl = None if control is None else np.ascontiguousarray(control, dtype=np.complex128)
-        wts = None if weights is None else np.ascontiguousarray(weights, dtype=np.complex128)
+        ctl = None if control is None else _input(control, (nkz, 2, nkx, 3), np.complex128, "control")
+        wts = None if weights is None else _input(weights, (nkz, ncy, nkx, 3), np.complex128, "weights")
         objective = OBJECTIVE_WALL_SHEAR if wts is None else OBJECTIVE_PROJECTION
         J = np.zeros(1)
         gu = np.empty((nkz, ncy, nkx, 3), dtype=np.complex128) if gradient else None
@@ -439,8 +448,8 @@ class Context:
         """Transpose of solve(): adjoints of (pressure, velocity) -> adjoints
         of (rhs, pressure_bc, velocity_bc)."""
         nkz, ncy, nkx = self.mesh.spectral_shape
-        lp = None if pressure_adj is None else np.ascontiguousarray(pressure_adj, dtype=np.complex128)
-        lv = np.ascontiguousarray(velocity_adj, dtype=np.complex128)
+        lp = None if pressure_adj is None else _input(pressure_adj, (nkz, ncy, nkx), np.complex128, "pressure_adj")
+        lv = _input(velocity_adj, (nkz, ncy, nkx, 3), np.complex128, "velocity_adj")
         lr = np.empty((nkz, ncy, nkx, 3), dtype=np.complex128)
         lpb = np.empty((nkz, 2, nkx), dtype=np.complex128)
         lvb = np.empty((nkz, 2, nkx, 3), dtype=np.complex128)
@@ -452,9 +461,10 @@ class Context:
                           pressure_bc_adj: Optional[np.ndarray] = None) -> np.ndarray:
         """Transpose of the linearisation of nonlinear() about u."""
         nkz, ncy, nkx = self.mesh.spectral_shape
-        u = np.ascontiguousarray(u, dtype=np.complex128)
-        ln = np.ascontiguousarray(nonlinear_adj, dtype=np.complex128)
-        lb = None if pressure_bc_adj is None else np.ascontiguousarray(pressure_bc_adj, dtype=np.complex128)
+        u = _input(u, (nkz, ncy, nkx, 3), np.complex128, "velocity")
+        ln = _input(nonlinear_adj, (nkz, ncy, nkx, 3), np.complex128, "nonlinear_adj")
+        lb = None if pressure_bc_adj is None else _input(pressure_bc_adj, (nkz, 2, nkx), np.complex128,
+                                                         "pressure_bc_adj")
         lu = np.empty((nkz, ncy, nkx, 3), dtype=np.complex128)
         _check(lib().cdns_nonlinear_adjoint(self._h, _ptr(u), _ptr(ln), None if lb is None else _ptr(lb),
                                             _ptr(lu)))

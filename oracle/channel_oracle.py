@@ -345,6 +345,50 @@ def diagnostics(m: Mesh, c: Constants, planes: np.ndarray, velocity) -> Tuple[fl
     return ekt, tke, math.sqrt(div_sq)
 
 
+# Plane-sum index of each running mean, in the order Statistics::write prints
+# them: u v w, p, uu vv ww uv vw wu, pp, pu pv pw, uuu vvv www, uuuu vvvv wwww
+# (src/sim/statistics.cpp:121-136).
+STAT_SOURCE = (0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 13, 10, 11, 12, 14, 15, 16, 17, 18, 19)
+
+
+class Statistics:
+    """Running means of Statistics::accumulate (src/sim/statistics.cpp:3-5,
+    117-139): every mean becomes (old * count + sample) / (count + 1), the
+    samples being plane sums / (NX NZ) and the step's dp/dx, dp/dz."""
+
+    def __init__(self, m: Mesh):
+        self.ny1 = m.NY + 1
+        self.plane = float(m.NX * m.NZ)
+        self.count = 0
+        self.dp = np.zeros(2)
+        self.means = np.zeros((20, self.ny1))
+
+    @staticmethod
+    def _update(old, sample, count):
+        return (old * float(count) + sample) / float(count + 1)
+
+    def accumulate(self, planes: np.ndarray, dpdx: float, dpdz: float) -> None:
+        planes = np.asarray(planes, dtype=np.float64)
+        if planes.shape != (self.ny1, 20):   # statistics.cpp:118-119 leaves the state as it was
+            raise ValueError("plane moments size mismatch")
+        scale = 1.0 / self.plane
+        self.dp = self._update(self.dp, np.array([dpdx, dpdz], dtype=np.float64), self.count)
+        for slot, k in enumerate(STAT_SOURCE):
+            self.means[slot] = self._update(self.means[slot], planes[:, k] * scale, self.count)
+        self.count += 1
+
+    def sample(self, velocity_phys, pressure_phys, dpdx: float, dpdz: float) -> None:
+        """Statistics::accumulate from physical fields (statistics.cpp:112-115);
+        a field of the wrong size raises before any mean changes (:95-99)."""
+        n = None
+        for f in list(velocity_phys) + [pressure_phys]:
+            if n is None:
+                n = np.shape(f)
+            if np.shape(f) != n or len(n) != 3 or n[1] != self.ny1 or n[0] * n[2] != self.plane:
+                raise ValueError("physical field size mismatch in statistics")
+        self.accumulate(plane_moments(velocity_phys, pressure_phys, True), dpdx, dpdz)
+
+
 # --------------------------------------------------------------------------
 # Spectral operators (src/solver/vector_ops.cpp)
 # Vector fields are tuples/lists of 3 arrays [nkz][ncy][nkx].

@@ -10,8 +10,9 @@ import pytest
 
 import cdns
 from golden_io import GOLDEN, load
-from oracle_cases import channel_case, divergence_free_field, orc, retau180_case
+from oracle_cases import channel_case, divergence_free_field, example_case, orc, retau180_case
 from test_gpu_parity import ctx_for
+from test_oracle_output_known_answers import UNIFORM_MEANS, diagnostics_fields, uniform_sample
 
 pytestmark = pytest.mark.gpu
 
@@ -124,23 +125,67 @@ def test_statistics_sampling_matches_host_accumulate():
     m, p = channel_case(32)
     c = ctx_for(m, p)
     c.set_velocity(np.stack(divergence_free_field(m, p, seed=3, amp=0.1, spectrum="k53", mean="loglaw"), axis=-1))
-    ny1, scale = m.NY + 1, 1.0 / (m.NX * m.NZ)
-    host = np.zeros((20, ny1))
-    dpm = np.zeros(2)
-    # means slot <- plane-sum index (Statistics::accumulate, statistics.cpp:121-136)
-    src = [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 13, 10, 11, 12, 14, 15, 16, 17, 18, 19]
+    host = orc.Statistics(m)
     for it in range(1, 6):
         c.step(it)
         c.synchronize()
         planes, _, _ = c.output_reduce()
-        dpdx = c.dpdx()
-        for slot, k in enumerate(src):
-            host[slot] = (host[slot] * (it - 1) + planes[:, k] * scale) / it
-        dpm = (dpm * (it - 1) + np.array(dpdx)) / it
+        host.accumulate(planes, *c.dpdx())
         c.statistics_sample()
     n, dp, means = c.statistics_read()
     assert n == 5
-    assert np.allclose(np.array(dp), dpm, rtol=1e-15, atol=0.0)
-    assert np.allclose(means, host, rtol=1e-14, atol=0.0)
+    assert np.allclose(np.array(dp), host.dp, rtol=1e-15, atol=0.0)
+    assert np.allclose(means, host.means, rtol=1e-14, atol=0.0)
     c.statistics_reset()
     assert c.statistics_read()[0] == 0
+
+
+def test_output_reduction_analytic_fields():
+    """tests/test_diagnostics.cpp:11-55 through cdns_output_reduce on the
+    example mesh (32^3, full spectrum): u = y cos(kx x), v = sin(kx x),
+    w = 2 cos(kz z), raw p = 5 + |v|^2/2 give EKT = NX NZ (NY+1) / 2,
+    TKE = 4/3, divergence L2 = sqrt(kx^2/6 + 2 kz^2) and a corrected-pressure
+    plane mean of 5."""
+    m, p = example_case()
+    vel, pr, want = diagnostics_fields(m)
+    c = ctx_for(m, p)
+    c.set_velocity(np.stack([orc.coarse_forward(m, f) for f in vel], axis=-1))
+    c.set_pressure(orc.coarse_forward(m, pr))
+    planes, values, _ = c.output_reduce(higher_moments=True)
+    assert values["finite"]
+    assert abs(values["ekt"] - want["ekt"]) <= 1e-8 * want["ekt"]
+    assert abs(values["tke"] - want["tke"]) <= 1e-12
+    assert abs(values["divergence_l2"] - want["divergence_l2"]) <= 1e-11
+    assert np.all(np.abs(planes[:, 3] / (m.NX * m.NZ) - want["pressure"]) <= 1e-13)
+
+
+def test_output_reduction_flags_discarded_infinite_imaginary_part():
+    """tests/test_diagnostics.cpp:57-69: an infinite imaginary part in the
+    pressure's kz = 0, T_0, kx = 0 coefficient -- a value the real transform
+    drops -- still marks the state non-finite."""
+    m, p = example_case()
+    c = ctx_for(m, p)
+    shape = m.spectral_shape()
+    c.set_velocity(np.zeros(shape + (3,), dtype=np.complex128))
+    pr = np.zeros(shape, dtype=np.complex128)
+    pr[m.NZS, 0, 0] = complex(0.0, np.inf)
+    c.set_pressure(pr)
+    _, values, _ = c.output_reduce()
+    assert not values["finite"]
+
+
+def test_statistics_uniform_samples():
+    """tests/test_statistics.cpp:62-111 through cdns_statistics_sample: the
+    uniform states v = (1, 2, 3), (3, 4, 5) with corrected pressure 4, 6 give
+    the exact means, cross moments and pressure moments."""
+    m, p = example_case()
+    c = ctx_for(m, p)
+    for sample in range(2):
+        vel, pr = uniform_sample(m, sample)
+        c.set_velocity(np.stack([orc.coarse_forward(m, f) for f in vel], axis=-1))
+        c.set_pressure(orc.coarse_forward(m, pr))
+        c.statistics_sample()
+    n, _, means = c.statistics_read()
+    assert n == 2
+    want = np.array(UNIFORM_MEANS, dtype=np.float64)[:, None]
+    assert np.allclose(means, np.broadcast_to(want, means.shape), rtol=1e-14, atol=0.0)
