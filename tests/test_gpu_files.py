@@ -83,3 +83,11 @@ def test_restart_reader_checks(tmp_path):
     text.write_text(bytes(d["field_S__0_dat"]).decode() + "(1,2)\n")
     with pytest.raises(cdns.CdnsError, match="extra"):
         c.read_restart(str(text))
+    # tests/test_field_io.cpp:99-120: a restart cut to 64 bytes, in either
+    # form, is rejected and leaves the state as it was
+    u = np.stack(list(d["u"]), axis=-1)
+    for key in ("field_S__0_bin", "field_S__0_dat"):
+        path.write_bytes(bytes(d[key])[:64])
+        with pytest.raises(cdns.CdnsError):
+            c.read_restart(str(path))
+        assert np.array_equal(c.get_velocity(), u)
