@@ -13,7 +13,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "cdns", "libcdns_cuda.so")
 SOURCES = ["context.cu", "chebyshev.cu", "transforms.cu", "solver.cu", "solver_setup.cu", "layout.cu", "noalloc.cu",
            "adjoint.cu", "adjoint_run.cu", "output.cu", "tune.cu",
-           "field_files.cu"]
+           "field_files.cu", "pencil.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -106,6 +106,14 @@ _SIGNATURES = {
     "cdns_batch_run": [ctypes.c_void_p, ctypes.c_int, ctypes.c_int],
     "cdns_batch_synchronize": [ctypes.c_void_p],
     "cdns_batch_stream": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)],
+    "cdns_pencil_layout": [ctypes.POINTER(MeshDesc), ctypes.c_int, ctypes.c_void_p],
+    "cdns_pencil_counts": [ctypes.POINTER(MeshDesc), ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                           ctypes.c_void_p],
+    "cdns_pencil_create": [ctypes.POINTER(MeshDesc), ctypes.POINTER(ParamsDesc), ctypes.c_int, ctypes.c_int,
+                           ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)],
+    "cdns_pencil_buffer": [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+                           ctypes.POINTER(ctypes.c_longlong)],
+    "cdns_pencil_stage": [ctypes.c_void_p, ctypes.c_int, ctypes.c_int],
 }
 
 
@@ -270,23 +278,28 @@ class Context:
     def handle(self) -> ctypes.c_void_p:
         return self._h
 
+    @property
+    def spectral_shape(self) -> Tuple[int, int, int]:
+        """[2 NZS + 1][NYS + 1][kx] of the spectral arrays this context holds."""
+        return self.mesh.spectral_shape
+
     # ---- state hand-over (reference layout) ----
     def set_velocity(self, u: np.ndarray) -> None:
-        u = _input(u, self.mesh.spectral_shape + (3,), np.complex128, "velocity")
+        u = _input(u, self.spectral_shape + (3,), np.complex128, "velocity")
         _check(lib().cdns_set_velocity(self._h, _ptr(u)))
 
     def get_velocity(self) -> np.ndarray:
-        out = np.empty(self.mesh.spectral_shape + (3,), dtype=np.complex128)
+        out = np.empty(self.spectral_shape + (3,), dtype=np.complex128)
         _check(lib().cdns_get_velocity(self._h, _ptr(out)))
         return out
 
     def get_pressure(self) -> np.ndarray:
-        out = np.empty(self.mesh.spectral_shape, dtype=np.complex128)
+        out = np.empty(self.spectral_shape, dtype=np.complex128)
         _check(lib().cdns_get_pressure(self._h, _ptr(out)))
         return out
 
     def set_velocity_bc(self, bc: np.ndarray) -> None:
-        nkz, _, nkx = self.mesh.spectral_shape
+        nkz, _, nkx = self.spectral_shape
         bc = np.ascontiguousarray(bc, dtype=np.complex128)
         if bc.shape != (nkz, 2, nkx, 3):
             raise ValueError("velocity BC must have shape [2*NZS+1][2][NXS+1][3]")
@@ -315,7 +328,7 @@ class Context:
 
     # ---- pieces of the hot path ----
     def nonlinear(self, u: np.ndarray):
-        nkz, ncy, nkx = self.mesh.spectral_shape
+        nkz, ncy, nkx = self.spectral_shape
         u = _input(u, (nkz, ncy, nkx, 3), np.complex128, "velocity")
         N = np.empty((nkz, ncy, nkx, 3), dtype=np.complex128)
         B = np.empty((nkz, 2, nkx), dtype=np.complex128)
@@ -324,18 +337,18 @@ class Context:
 
     def transform_fine(self, direction: str, data: np.ndarray) -> np.ndarray:
         if direction == "B":
-            src = _input(data, self.mesh.spectral_shape, np.complex128, "spectral field")
+            src = _input(data, self.spectral_shape, np.complex128, "spectral field")
             out = np.empty(self.mesh.fine_shape, dtype=np.float64)
         elif direction == "F":
             src = _input(data, self.mesh.fine_shape, np.float64, "physical field")
-            out = np.empty(self.mesh.spectral_shape, dtype=np.complex128)
+            out = np.empty(self.spectral_shape, dtype=np.complex128)
         else:
             raise ValueError("direction must be 'B' or 'F'")
         _check(lib().cdns_transform_fine(self._h, ord(direction), _ptr(src), _ptr(out)))
         return out
 
     def solve(self, g: float, rhs: np.ndarray, pressure_bc: np.ndarray, velocity_bc: np.ndarray):
-        nkz, ncy, nkx = self.mesh.spectral_shape
+        nkz, ncy, nkx = self.spectral_shape
         rhs = _input(rhs, (nkz, ncy, nkx, 3), np.complex128, "rhs")
         pbc = _input(pressure_bc, (nkz, 2, nkx), np.complex128, "pressure_bc")
         vbc = _input(velocity_bc, (nkz, 2, nkx, 3), np.complex128, "velocity_bc")
@@ -347,7 +360,7 @@ class Context:
         return p, v, units[:ncy].copy(), units[ncy:].copy()
 
     def set_pressure(self, p: np.ndarray) -> None:
-        p = _input(p, self.mesh.spectral_shape, np.complex128, "pressure")
+        p = _input(p, self.spectral_shape, np.complex128, "pressure")
         _check(lib().cdns_set_pressure(self._h, _ptr(p)))
 
     # ---- coarse grid and output reduction ----

@@ -188,7 +188,7 @@ k_solve_adj(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, AdjArgs
     const int S = ncy * TC;
     const int col0 = blockIdx.x * TC;
     const int tid = threadIdx.x, w = tid >> 5, L = tid & 31, p = L & 1;
-    const int zc = d.NZS * nkx;
+    const int zc = d.zc;
     const bool zero_mode = !A.solve_only;
 
     // ---- correction pass transposed: coalesced loads, per-column sums ------
@@ -242,7 +242,7 @@ k_solve_adj(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, AdjArgs
     if (col < ncol) {
         const int kzi = col / nkx, kx = col - kzi * nkx;
         const double ax = t.wavx[kx], az = t.wavz[kzi];
-        const bool zero_col = kzi == d.NZS && kx == 0;
+        const bool zero_col = col == d.zc;
         const long long cm = (long long)col * ncy;
         double2 lc0 = mk(0, 0), lc1 = mk(0, 0), lsg0 = mk(0, 0), lsg1 = mk(0, 0);
 #pragma unroll

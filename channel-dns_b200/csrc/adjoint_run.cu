@@ -250,6 +250,7 @@ extern "C" {
 int cdns_adjoint_run(cdns_ctx *c, int nsteps, int kck, int objective, const double *weights,
                      const double *control, double *J, double *grad_u, double *grad_bc) {
     if (!c) return fail(CDNS_ERR_ARG, "null context");
+    if (int r = require_whole(c)) return r;
     if (nsteps < 1 || kck < 1) return fail(CDNS_ERR_ARG, "nsteps and checkpoint_interval must be >= 1");
     if (objective != CDNS_OBJECTIVE_WALL_SHEAR && objective != CDNS_OBJECTIVE_PROJECTION)
         return fail(CDNS_ERR_ARG, "unknown objective");
@@ -375,6 +376,7 @@ int cdns_adjoint_run(cdns_ctx *c, int nsteps, int kck, int objective, const doub
 int cdns_solve_adjoint(cdns_ctx *c, double g, const double *lp, const double *lv, double *lrhs, double *lpbc,
                        double *lvbc) {
     if (!c || !lv || !lrhs || !lpbc || !lvbc) return fail(CDNS_ERR_ARG, "null argument");
+    if (int r = require_whole(c)) return r;
     DeviceGuard guard(c->device);
     const Dims &d = c->d;
     cudaStream_t s = c->stream;
@@ -402,6 +404,7 @@ int cdns_solve_adjoint(cdns_ctx *c, double g, const double *lp, const double *lv
 int cdns_nonlinear_adjoint(cdns_ctx *c, const double *velocity, const double *lN, const double *lpbc,
                            double *lu) {
     if (!c || !velocity || !lN || !lu) return fail(CDNS_ERR_ARG, "null argument");
+    if (int r = require_whole(c)) return r;
     int r = check_adjoint_mesh(c);
     if (r) return r;
     DeviceGuard guard(c->device);

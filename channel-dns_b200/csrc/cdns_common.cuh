@@ -24,6 +24,8 @@ struct Dims {
     long long Ns;        // nkz*ncy*nkx complex values per spectral component
     int ztl;             // kx lines per block of the z transforms (0: the padding rule)
     int xrw;             // (z, y) rows per block of the register-form x stage (0: 4)
+    int kx0;             // global kx of local column kx = 0 (a pencil rank's kx block; else 0)
+    int zc;              // local index of the (kz, kx) = (0, 0) column, -1 if not held here
 };
 
 // Read-only per-context tables in device memory.

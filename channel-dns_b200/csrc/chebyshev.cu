@@ -297,7 +297,7 @@ k_ysynth(Dims d, const double *__restrict__ csyn, int jp, const double2 *__restr
     __syncthreads();
     if (jok && par == 0) {
         CO *Ff = F + (long long)f * d.ny2 * d.fcol + col0;
-        const int zc = d.NZS * d.nkx;   // the (kz, kx) = (0, 0) column
+        const int zc = d.zc;   // the (kz, kx) = (0, 0) column
 #pragma unroll
         for (int mr = 0; mr < 2; ++mr) {
             const int j = j0 + 8 * mr + g;

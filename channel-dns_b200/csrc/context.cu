@@ -121,11 +121,9 @@ void enqueue_nonlinear(cdns_ctx *c, const double2 *u, double2 *N, bool prof, int
 
 }  // namespace cdns
 
-namespace {
-void enqueue_step_body(cdns_ctx *c, double a0, double a1, double b0, double b1, double g_v,
-                       bool prof, int slot) {
+namespace cdns {
+void enqueue_solve(cdns_ctx *c, double a0, double a1, double b0, double b1, double g_v) {
     const int k = c->cur;
-    enqueue_nonlinear(c, c->U[k], c->Nb[k], prof, slot);
     StepArgs a{};
     a.u = c->U[k];
     a.u_prev = c->U[1 - k];
@@ -144,6 +142,19 @@ void enqueue_step_body(cdns_ctx *c, double a0, double a1, double b0, double b1, 
     a.b0 = b0;
     a.b1 = b1;
     launch_step_solve(c->d, c->t, c->pp, g_v, c->st, a, c->stream);
+}
+
+int require_whole(const cdns_ctx *c) {
+    if (c && c->pen) return fail(CDNS_ERR_STATE, "a pencil rank context holds one kx block: use cdns_pencil_stage");
+    return CDNS_OK;
+}
+}  // namespace cdns
+
+namespace {
+void enqueue_step_body(cdns_ctx *c, double a0, double a1, double b0, double b1, double g_v,
+                       bool prof, int slot) {
+    enqueue_nonlinear(c, c->U[c->cur], c->Nb[c->cur], prof, slot);
+    enqueue_solve(c, a0, a1, b0, b1, g_v);
     if (prof) cudaEventRecord(c->ev[(size_t)slot * (kStages + 1) + kStages], c->stream);
 }
 
@@ -198,14 +209,18 @@ int one_step(cdns_ctx *c, int it) {
 
 }  // namespace cdns
 
-extern "C" {
-
-int cdns_create(const cdns_mesh_desc *m, const cdns_params *p, int precision, int device,
-                cdns_ctx **out) {
+namespace {
+// cdns_create's body; ranks > 1 (or ranks = 1 through cdns_pencil_create)
+// makes rank `rank` of a pencil decomposition: the spectral state of one kx
+// block plus the y-slab stage buffers (pencil.cu).
+int create_context(const cdns_mesh_desc *m, const cdns_params *p, int precision, int device, int ranks,
+                   int rank, cdns_ctx **out) {
     if (!m || !p || !out) return fail(CDNS_ERR_ARG, "null argument");
     *out = nullptr;
     if (precision != CDNS_PRECISION_FP64 && precision != CDNS_PRECISION_MIXED)
         return fail(CDNS_ERR_ARG, "unsupported precision mode");
+    if (ranks > 0 && precision != CDNS_PRECISION_FP64)
+        return fail(CDNS_ERR_ARG, "pencil ranks run the FP64 step");
     if (m->NYS < 4 || m->NXS < 0 || m->NZS < 0 || m->NY2 < m->NYS || m->NY2 < 2 ||
         m->NX2 < 2 * m->NXS || m->NZ2 < 2 * m->NZS || m->NX2 < 1 || m->NZ2 < 1 ||
         !(m->XL > 0) || !(m->ZL > 0))
@@ -226,7 +241,16 @@ int cdns_create(const cdns_mesh_desc *m, const cdns_params *p, int precision, in
     d.NX2 = m->NX2; d.NY2 = m->NY2; d.NZ2 = m->NZ2;
     d.NXS = m->NXS; d.NYS = m->NYS; d.NZS = m->NZS;
     d.nkx = m->NXS + 1; d.nkz = 2 * m->NZS + 1; d.ncy = m->NYS + 1; d.ny2 = m->NY2 + 1;
+    d.kx0 = 0;
+    if (ranks > 0) {
+        int j0, nj;
+        if (int r = pencil_blocks(*m, ranks, rank, d.kx0, d.nkx, j0, nj)) {
+            delete c;
+            return r;
+        }
+    }
     d.ncol = d.nkx * d.nkz;
+    d.zc = d.kx0 == 0 ? d.NZS * d.nkx : -1;
     d.nyh = m->NY2 / 2 + 1;
     d.Ns = (long long)d.nkz * d.ncy * d.nkx;
     if (!plan_fft(d.NX2, c->px) || !plan_fft(d.NZ2, c->pz)) {
@@ -267,7 +291,7 @@ int cdns_create(const cdns_mesh_desc *m, const cdns_params *p, int precision, in
     std::vector<double> wavx(d.nkx), wavz(d.nkz), WL(d.ncy, 0.0), WD(d.ncy, 0.0), WR(d.ncy, 0.0),
         cosy(2 * (size_t)d.NY2);
     const double alx = 2.0 * pi / m->XL, alz = 2.0 * pi / m->ZL;
-    for (int k = 0; k < d.nkx; ++k) wavx[k] = k * alx;
+    for (int k = 0; k < d.nkx; ++k) wavx[k] = (d.kx0 + k) * alx;
     for (int k = -d.NZS; k <= d.NZS; ++k) wavz[k + d.NZS] = k * alz;
     const int n = d.NYS;
     for (int iy = n; iy >= 2; --iy) {
@@ -354,14 +378,30 @@ int cdns_create(const cdns_mesh_desc *m, const cdns_params *p, int precision, in
     if (e != cudaSuccess) return bail(fail(CDNS_ERR_CUDA, cudaGetErrorString(e)));
     // velocity_boundary (src/sim/initial_bc.cpp:95-101): v = V_Microblow0 on the zero mode
     std::vector<double2> bc(6 * nc, make_double2(0, 0));
-    const int zc = d.NZS * d.nkx;
-    bc[(2 * 1 + 0) * nc + zc] = make_double2(p->V_Microblow0, 0.0);
-    bc[(2 * 1 + 1) * nc + zc] = make_double2(p->V_Microblow0, 0.0);
+    if (d.zc >= 0) {
+        bc[(2 * 1 + 0) * nc + d.zc] = make_double2(p->V_Microblow0, 0.0);
+        bc[(2 * 1 + 1) * nc + d.zc] = make_double2(p->V_Microblow0, 0.0);
+    }
     if ((r = upload(c, c->bc_v, bc.data(), bc.size() * sizeof(double2)))) return bail(r);
+    if (ranks > 0 && (r = pencil_init(c, ranks, rank))) return bail(r);
     if ((r = tune_context(c, false))) return bail(r);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(fail(CDNS_ERR_CUDA, "sync"));
     *out = c;
     return CDNS_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int cdns_create(const cdns_mesh_desc *m, const cdns_params *p, int precision, int device,
+                cdns_ctx **out) {
+    return create_context(m, p, precision, device, 0, 0, out);
+}
+
+int cdns_pencil_create(const cdns_mesh_desc *m, const cdns_params *p, int ranks, int rank, int device,
+                       cdns_ctx **out) {
+    if (ranks < 1) return fail(CDNS_ERR_ARG, "ranks must be >= 1");
+    return create_context(m, p, CDNS_PRECISION_FP64, device, ranks, rank, out);
 }
 
 int cdns_destroy(cdns_ctx *c) {
@@ -373,6 +413,7 @@ int cdns_destroy(cdns_ctx *c) {
     for (auto ev : c->ev) cudaEventDestroy(ev);
     adjoint_release(c->adj);
     output_release(c->outw);
+    pencil_release(c->pen);
     for (void *p : c->allocs) cudaFree(p);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -460,12 +501,14 @@ int cdns_set_velocity_bc(cdns_ctx *c, const double *bc) {
 
 int cdns_step(cdns_ctx *c, int iteration) {
     if (!c) return fail(CDNS_ERR_ARG, "null context");
+    if (int r = require_whole(c)) return r;
     DeviceGuard guard(c->device);
     return one_step(c, iteration);
 }
 
 int cdns_run(cdns_ctx *c, int first, int nsteps) {
     if (!c) return fail(CDNS_ERR_ARG, "null context");
+    if (int r = require_whole(c)) return r;
     if (nsteps < 0) return fail(CDNS_ERR_ARG, "negative step count");
     DeviceGuard guard(c->device);
     for (int i = 0; i < nsteps; ++i) {
@@ -501,6 +544,7 @@ int cdns_get_dpdx(cdns_ctx *c, double out[2]) {
 
 int cdns_nonlinear(cdns_ctx *c, const double *velocity, double *nl, double *pbc) {
     if (!c || !velocity || !nl) return fail(CDNS_ERR_ARG, "null argument");
+    if (int r = require_whole(c)) return r;
     DeviceGuard guard(c->device);
     const Dims &d = c->d;
     CK(cudaMemcpyAsync(c->aux2, velocity, sizeof(double2) * 3 * d.Ns, cudaMemcpyHostToDevice, c->stream));
@@ -525,6 +569,7 @@ int cdns_nonlinear(cdns_ctx *c, const double *velocity, double *nl, double *pbc)
 
 int cdns_transform_fine(cdns_ctx *c, int dir, const double *in, double *out) {
     if (!c || !in || !out) return fail(CDNS_ERR_ARG, "null argument");
+    if (int r = require_whole(c)) return r;
     DeviceGuard guard(c->device);
     const Dims &d = c->d;
     const size_t nphys = (size_t)d.NZ2 * d.ny2 * d.NX2;
@@ -603,6 +648,7 @@ int cdns_solve(cdns_ctx *c, double g, const double *rhs, const double *pbc, cons
 
 int cdns_profile_begin(cdns_ctx *c) {
     if (!c) return fail(CDNS_ERR_ARG, "null context");
+    if (int r = require_whole(c)) return r;
     DeviceGuard guard(c->device);
     if (c->ev.empty()) {
         c->ev.resize((size_t)kMaxProfSteps * (kStages + 1));

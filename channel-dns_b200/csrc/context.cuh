@@ -25,6 +25,13 @@ size_t adjoint_bytes(const AdjointWork *w);
 struct OutputWork;    // output.cu
 void output_release(OutputWork *w);
 size_t output_bytes(const OutputWork *w);
+struct PencilWork;    // pencil.cu
+void pencil_release(PencilWork *w);
+// Rank `rank` of a `ranks`-way pencil decomposition of mesh m: the kx block
+// [kx0, kx0 + nkx) and the fine-grid y slab [j0, j0 + nj) (the reference's
+// block rule, src/core/mesh.cpp:20-85).  Non-zero (with the error recorded)
+// if the decomposition would leave a rank an empty block.
+int pencil_blocks(const cdns_mesh_desc &m, int ranks, int rank, int &kx0, int &nkx, int &j0, int &nj);
 // Radix plan of a length-n Stockham FFT (false if n has a prime factor > 13).
 bool plan_fft(int n, FftPlan &p);
 
@@ -70,6 +77,7 @@ struct cdns_ctx {
     std::vector<cudaEvent_t> ev;
     cdns::AdjointWork *adj = nullptr;     // discrete-adjoint workspace, made on first use
     cdns::OutputWork *outw = nullptr;     // coarse-grid output workspace, made on first use
+    cdns::PencilWork *pen = nullptr;      // pencil rank: y-slab stage buffers and exchange maps
 
     template <typename T> int alloc(T *&ptr, size_t count) {
         void *p = nullptr;
@@ -98,8 +106,15 @@ void step_coefficients(int it, double dt, double re, double &a0, double &a1, dou
 // receives the z-physical fields of u and omega, c->G if null.
 void enqueue_nonlinear(cdns_ctx *c, const double2 *u, double2 *N, bool prof, int step_slot,
                        double2 *G_fp64 = nullptr);
+// The column solve of a step from U[cur], Nb[cur], bw and the stored history
+// (RHS assembly, pressure and velocity solves, zero-mode and flow corrections).
+void enqueue_solve(cdns_ctx *c, double a0, double a1, double b0, double b1, double g_v);
 // Solver state of c for wall-normal Helmholtz constant g_v (no-op if current).
 int do_setup(cdns_ctx *c, double g_v);
+// Entry points that transform or step the whole channel refuse a pencil rank.
+int require_whole(const cdns_ctx *c);
+// Sets up the pencil workspace of a rank context made by cdns_create's body.
+int pencil_init(cdns_ctx *c, int ranks, int rank);
 // One step of cdns_step: setup if g changed, then the step (graph replay for it >= 3).
 int one_step(cdns_ctx *c, int it);
 // Launch shapes of c (z line width, Chebyshev transform forms): cached or timed (tune.cu).

@@ -139,6 +139,7 @@ extern "C" {
 
 int cdns_write_restart(cdns_ctx *c, const char *path, long long step, double time, int text) {
     if (!c || !path) return fail(CDNS_ERR_ARG, "null argument");
+    if (int r = require_whole(c)) return r;
     if (!c->have_velocity) return fail(CDNS_ERR_STATE, "no velocity to write");
     if (!little_endian()) return fail(CDNS_ERR_ARG, "binary files need a little-endian host");
     DeviceGuard guard(c->device);
@@ -165,6 +166,7 @@ int cdns_write_restart(cdns_ctx *c, const char *path, long long step, double tim
 
 int cdns_read_restart(cdns_ctx *c, const char *path, long long *step, double *time) {
     if (!c || !path) return fail(CDNS_ERR_ARG, "null argument");
+    if (int r = require_whole(c)) return r;
     std::ifstream in(path, std::ios::binary);
     if (!in) return fail(CDNS_ERR_ARG, std::string("cannot open restart: ") + path);
     std::string t((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
@@ -214,6 +216,7 @@ int cdns_read_restart(cdns_ctx *c, const char *path, long long *step, double *ti
 
 int cdns_write_physical(cdns_ctx *c, const char *path, long long step, double time, int text) {
     if (!c || !path) return fail(CDNS_ERR_ARG, "null argument");
+    if (int r = require_whole(c)) return r;
     if (!little_endian()) return fail(CDNS_ERR_ARG, "binary files need a little-endian host");
     const cdns_mesh_desc &m = c->mesh;
     const size_t plane = (size_t)m.NZ * (m.NY + 1) * m.NX;

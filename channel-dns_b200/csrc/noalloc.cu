@@ -108,6 +108,7 @@ extern "C" int cdns_transform_fine_backward_noalloc(const cdns_mesh_desc *m, con
     d.nkx = m->NXS + 1; d.nkz = 2 * m->NZS + 1; d.ncy = m->NYS + 1; d.ny2 = m->NY2 + 1;
     d.ncol = d.nkx * d.nkz;
     d.fcol = d.ncol;
+    d.zc = d.NZS * d.nkx;
     d.nyh = m->NY2 / 2 + 1;
     d.Ns = (long long)d.nkz * d.ncy * d.nkx;
     FftPlan px{}, pz{};

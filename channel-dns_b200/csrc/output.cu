@@ -349,6 +349,7 @@ extern "C" {
 
 int cdns_output_reduce(cdns_ctx *c, int higher, double *plane_sums, double *diag, double *physical) {
     if (!c) return fail(CDNS_ERR_ARG, "null context");
+    if (int r = require_whole(c)) return r;
     if (!c->have_velocity) return fail(CDNS_ERR_STATE, "cdns_output_reduce before cdns_set_velocity");
     DeviceGuard guard(c->device);
     int r = ensure_output(c, physical != nullptr);
@@ -402,6 +403,7 @@ int cdns_output_reduce(cdns_ctx *c, int higher, double *plane_sums, double *diag
 
 int cdns_statistics_sample(cdns_ctx *c) {
     if (!c) return fail(CDNS_ERR_ARG, "null context");
+    if (int r = require_whole(c)) return r;
     if (!c->have_velocity) return fail(CDNS_ERR_STATE, "cdns_statistics_sample before cdns_set_velocity");
     DeviceGuard guard(c->device);
     int r = ensure_output(c, false);
@@ -418,6 +420,7 @@ int cdns_statistics_sample(cdns_ctx *c) {
 
 int cdns_statistics_read(cdns_ctx *c, long long *count, double *dp_means, double *means) {
     if (!c) return fail(CDNS_ERR_ARG, "null context");
+    if (int r = require_whole(c)) return r;
     DeviceGuard guard(c->device);
     int r = ensure_output(c, false);
     if (r) return r;
@@ -448,6 +451,7 @@ int cdns_statistics_reset(cdns_ctx *c) {
 
 int cdns_transform_coarse(cdns_ctx *c, int dir, const double *in, double *out) {
     if (!c || !in || !out) return fail(CDNS_ERR_ARG, "null argument");
+    if (int r = require_whole(c)) return r;
     DeviceGuard guard(c->device);
     int r = ensure_output(c, true);
     if (r) return r;

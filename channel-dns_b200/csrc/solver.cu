@@ -189,7 +189,7 @@ k_solve(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, SolveArgs A
     if (col < ncol) {
         const int kzi = col / nkx, kx = col - kzi * nkx;
         const double ax = t.wavx[kx], az = t.wavz[kzi];
-        const bool zero_col = kzi == d.NZS && kx == 0;
+        const bool zero_col = col == d.zc;
         const long long cm = (long long)col * ncy;   // column-major base
         bool pivot_fail = false;
         double2 pv[E], v0[E], v1[E], v2[E], dy[E];
@@ -315,7 +315,7 @@ k_solve(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, SolveArgs A
 
     // ---- influence and sigma corrections, coalesced over the block --------
     // odd-y coefficients take sigma_0 for p, u, w and sigma_1 for v; even-y the reverse
-    const int zc = d.NZS * nkx;   // the (kz, kx) = (0, 0) column
+    const int zc = d.zc;   // the (kz, kx) = (0, 0) column (-1: not on this rank)
     const bool fix_zero = !s.solve_only && zc >= col0 && zc < col0 + TC;
     bool bad = false;
     for (int i = tid; i < S; i += kThreads) {

@@ -157,7 +157,7 @@ k_setup_solve(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, Setup
         const int kzi = active ? col / nkx : 0;
         const int kx = active ? col - kzi * nkx : 0;
         const double ax = t.wavx[kx], az = t.wavz[kzi];
-        const bool zero_col = active && kzi == d.NZS && kx == 0;
+        const bool zero_col = active && col == d.zc;
         if (active)
             tau_chain(par, ny, pp.G_pre, 1.0, 0.0, zero_col, A.bcp_top, A.bcp_bot, st.wn_p[col], dyb + l,
                       pc + l, adp + l, TC, sWL, sWD, sWR);
@@ -257,7 +257,7 @@ __global__ void k_inf_normalize(Dims d, double a_v1, double2 *inf_div) {
     const int nc = d.ncol;
     const double2 i00 = I[col], i01 = I[nc + col], i10 = I[2 * nc + col], i11 = I[3 * nc + col];
     double2 den = csub(cmul(i00, i11), cmul(i01, i10));
-    const bool root = (col == d.NZS * d.nkx);
+    const bool root = (col == d.zc);
     if (root) den = (a_v1 == 0.0) ? mk(1.0, 0.0) : cdiv(mk(0.25, 0.0), i00);
     if (root) {
         I[col] = den;
@@ -286,7 +286,7 @@ __global__ void k_sigma0(Dims d, double re, const double *wn_v, const double2 *p
     const double2 pbn = p_b[on];
     sigma0[col] = mk(re + w * vbn.x, w * vbn.y);
     double2 s1 = csub(mk(re + w * vbn1.x, w * vbn1.y), cscale(re * (2.0 * n), pbn));
-    if (col == d.NZS * d.nkx) s1 = mk(1.0, 0.0);
+    if (col == d.zc) s1 = mk(1.0, 0.0);
     sigma0[d.ncol + col] = s1;
 }
 
@@ -301,7 +301,7 @@ __global__ void k_unit_response(Dims d, Tables t, PhysParams pp, double g_v, con
     double *ad = reinterpret_cast<double *>(o + ncy);
     double *WL = ad + ncy, *WD = WL + ncy, *WR = WD + ncy;
     const int par = threadIdx.x;
-    const long long zc = (long long)(d.NZS * d.nkx) * ncy;
+    const long long zc = (long long)d.zc * ncy;
     for (int y = par; y < ncy; y += 2) {
         r[y] = mk(y == 0 ? pp.Re : 0.0, 0.0);
         ad[y] = ad_v[zc + y];
@@ -359,8 +359,9 @@ void setup_solver(const Dims &d, const Tables &t, const PhysParams &pp, double g
         k_setup_solve<MODE_COUPLED><<<blocks, kThreads, sm, s>>>(d, t, pp, g_v, st, A);
     }
     k_sigma0<<<nb, 128, 0, s>>>(d, pp.Re, st.wn_v, st.p_b, st.v_b, st.sigma0);
+    // the zero mode's unit responses (correct_flow): only where that column is held
     const size_t smu = sizeof(double2) * 2 * d.ncy + sizeof(double) * 4 * d.ncy;
-    k_unit_response<<<1, 2, smu, s>>>(d, t, pp, g_v, st.ad_v, st.unit);
+    if (d.zc >= 0) k_unit_response<<<1, 2, smu, s>>>(d, t, pp, g_v, st.ad_v, st.unit);
 }
 
 }  // namespace cdns

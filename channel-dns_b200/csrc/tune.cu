@@ -150,6 +150,12 @@ namespace cdns {
 // a profiled one, whose timings would mislead the tuner -- reuses the choices.
 int tune_context(cdns_ctx *c, bool force) {
     if (c->mixed) return CDNS_OK;   // FP32 stage buffers keep the rule-based shapes
+    if (c->pen) {
+        // a pencil rank holds part of the mesh: timing it would file its
+        // shapes under the whole mesh's key, so it keeps the rule-based ones
+        apply(c, Choice{});
+        return CDNS_OK;
+    }
     const char *wfile = std::getenv("CDNS_WISDOM");
     if (wfile && *wfile) {
         std::call_once(g_env_import, [&] {
@@ -196,6 +202,7 @@ extern "C" {
 
 int cdns_tune(cdns_ctx *c) {
     if (!c) return fail(CDNS_ERR_ARG, "null context");
+    if (int r = require_whole(c)) return r;
     DeviceGuard guard(c->device);
     for (auto &g : c->graph)
         if (g) {

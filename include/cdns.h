@@ -320,6 +320,42 @@ int cdns_batch_synchronize(cdns_batch *batch);
 /* The batch's CUDA stream (a cudaStream_t): steady steps are launched on it. */
 int cdns_batch_stream(cdns_batch *batch, void **stream);
 
+/* Pencil decomposition of one channel over `ranks` ranks (one GPU each):
+ * replaces the reference's distributed path (INDEX_Serial = 0) -- Mesh's
+ * block tables (src/core/mesh.cpp:20-85) and the transposes of Transforms
+ * (src/fft/transforms.cpp:126-170, 304-404) called from Simulation::run's
+ * multi-rank branch (src/sim/simulation.cpp:191-218).
+ *
+ * Rank r holds the spectral state of the kx block [kx0, kx0 + nkx) (all kz
+ * and Chebyshev modes; cdns_set_velocity / cdns_get_velocity /
+ * cdns_get_pressure / cdns_set_velocity_bc take the reference layout of that
+ * block, [2*NZS+1][..][nkx](+[3])) and, inside a step, the fine-grid y slab
+ * [j0, j0 + nj) of the NY2 + 1 points.  Blocks follow the reference's rule:
+ * n / ranks each, one more on each of the last n % ranks ranks; ranks must
+ * not exceed NXS + 1, NY + 1 or NY2 + 1.  Rank 0 holds the zero mode.
+ *
+ * cdns_pencil_layout writes table[4 * r ..] = {kx0, nkx, j0, nj} for every
+ * rank (host only).  A step of iteration `it` is
+ *   cdns_pencil_stage(ctx, it, 0)   curl, Chebyshev synthesis, pack exchange 0
+ *   all-to-all of exchange 0         send buffer -> peers' recv buffers
+ *   cdns_pencil_stage(ctx, it, 1)   unpack, z synthesis, x stage, z analysis, pack exchange 1
+ *   all-to-all of exchange 1
+ *   cdns_pencil_stage(ctx, it, 2)   unpack, Chebyshev analysis, column solve
+ * on every rank; stages run on the context stream (cdns_get_stream) and the
+ * exchange must be ordered on it.  cdns_pencil_buffer gives each exchange's
+ * send (recv = 0) or receive (recv = 1) buffer on the device and its length
+ * in doubles; the per-peer lengths, in rank order, are cdns_pencil_counts
+ * (host only; send[q] on this rank equals recv[rank] on rank q).  Whole-channel
+ * calls (cdns_step, transforms, output, files, adjoint) refuse a pencil
+ * rank context with CDNS_ERR_STATE.  FP64 only. */
+int cdns_pencil_layout(const cdns_mesh_desc *mesh, int ranks, int *table);
+int cdns_pencil_counts(const cdns_mesh_desc *mesh, int ranks, int rank, int exchange, long long *send,
+                       long long *recv);
+int cdns_pencil_create(const cdns_mesh_desc *mesh, const cdns_params *params, int ranks, int rank, int device,
+                       cdns_ctx **out);
+int cdns_pencil_buffer(cdns_ctx *ctx, int exchange, int recv, void **ptr, long long *doubles);
+int cdns_pencil_stage(cdns_ctx *ctx, int iteration, int stage);
+
 #ifdef __cplusplus
 }
 #endif

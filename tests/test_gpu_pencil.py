@@ -1,0 +1,121 @@
+"""The pencil decomposition on one B200: every rank of a decomposition runs in
+this process (cdns.pencil.LocalPencil, exchanges by device copies), and the
+decomposed step must equal the single-context step on the same state --
+kx-block rank contexts (zero mode on rank 0 only), the y-slab stages and the
+pack/unpack kernels together.  The NCCL path (cdns.pencil.step, the call each
+GPU of a multi-GPU run makes) is run with a one-rank process group."""
+import datetime
+import os
+import socket
+
+import numpy as np
+import pytest
+
+import cdns
+from cdns import pencil
+from oracle_cases import channel_case, divergence_free_field, example_case
+from test_gpu_parity import ctx_for
+
+pytestmark = pytest.mark.gpu
+
+
+def _desc(m, p):
+    mesh = cdns.Mesh(m.NX, m.NY, m.NZ, m.NXS, m.NYS, m.NZS, m.NX2, m.NY2, m.NZ2, m.XL, m.ZL)
+    params = cdns.Params(Re=p.Re, DT=p.DT, G_pre=p.G_pre, a_pre0=p.a_pre0, b_pre0=p.b_pre0, a_V=p.a_V,
+                         b_V=p.b_V, INDEX_GRAD_PRE=p.INDEX_GRAD_PRE, THETA=p.THETA,
+                         V_Microblow0=p.V_Microblow0)
+    return mesh, params
+
+
+def rel_max(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def _reference(m, p, u0, nsteps):
+    c = ctx_for(m, p)
+    c.set_velocity(u0)
+    c.run(1, nsteps)
+    c.synchronize()
+    out = (c.get_velocity(), c.get_pressure(), c.dpdx())
+    c.close()
+    return out
+
+
+@pytest.mark.parametrize("case,ranks", [("channel32", 1), ("channel32", 2), ("channel32", 3),
+                                        ("example", 3), ("example", 5)])
+def test_local_pencil_matches_single_context(case, ranks, monkeypatch):
+    """4 steps (the two setup steps and two steady ones): velocity, pressure
+    and dp/dx of the decomposed step equal the single-context step to 1e-13
+    (32 x 33 x 32 channel at fixed dp/dx, 48^3 product grid; the 32^3 example
+    case at constant flow rate, full Nyquist spectrum, ragged blocks)."""
+    monkeypatch.setenv("CDNS_Y_TRANSFORM", "matrix")   # the form the rank contexts use
+    if case == "channel32":
+        m, p = channel_case(32)
+        u0 = np.stack(divergence_free_field(m, p, seed=2, amp=0.1, spectrum="k53", mean="loglaw"), axis=-1)
+    else:
+        m, p = example_case()
+        u0 = np.stack(divergence_free_field(m, p, seed=3, amp=0.05), axis=-1)
+    uref, pref, dref = _reference(m, p, u0, 4)
+    mesh, params = _desc(m, p)
+    lp = pencil.LocalPencil(mesh, params, ranks)
+    try:
+        lp.set_velocity(u0)
+        lp.run(1, 4)
+        u, pr, dp = lp.get_velocity(), lp.get_pressure(), lp.dpdx()
+    finally:
+        lp.close()
+    assert rel_max(u, uref) <= 1e-13
+    assert rel_max(pr, pref) <= 1e-13
+    assert np.allclose(dp, dref, rtol=1e-13, atol=1e-300)
+
+
+def test_pencil_rank_refuses_whole_channel_calls_and_misordered_stages():
+    m, p = channel_case(16)
+    mesh, params = _desc(m, p)
+    r = pencil.PencilRank(mesh, params, 2, 1)
+    try:
+        assert r.spectral_shape == (2 * m.NZS + 1, m.NYS + 1, pencil.layout(mesh, 2)[1][1])
+        r.set_velocity(np.zeros(r.spectral_shape + (3,), dtype=np.complex128))
+        with pytest.raises(cdns.CdnsError) as e:
+            r.step(1)
+        assert e.value.code == 3
+        with pytest.raises(cdns.CdnsError) as e:
+            r.stage(1, 1)          # stage 1 before stage 0
+        assert e.value.code == 3
+        with pytest.raises(ValueError):
+            r.set_velocity(np.zeros(m.spectral_shape() + (3,), dtype=np.complex128))   # whole channel
+    finally:
+        r.close()
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def test_nccl_step_one_rank(monkeypatch):
+    """cdns.pencil.step through a one-rank NCCL group: the stages on the
+    context stream, the all-to-alls ordered on it, 3 steps as the single
+    context."""
+    import torch
+    import torch.distributed as dist
+    monkeypatch.setenv("CDNS_Y_TRANSFORM", "matrix")   # the form the rank contexts use
+    m, p = channel_case(32)
+    u0 = np.stack(divergence_free_field(m, p, seed=4, amp=0.1), axis=-1)
+    uref, pref, _ = _reference(m, p, u0, 3)
+    mesh, params = _desc(m, p)
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(_free_port())
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60))
+    r = pencil.PencilRank(mesh, params, 1, 0)
+    try:
+        r.set_velocity(u0)
+        pencil.run(r, 1, 3)
+        r.synchronize()
+        u, pr = r.get_velocity(), r.get_pressure()
+    finally:
+        r.close()
+        dist.destroy_process_group()
+    assert rel_max(u, uref) <= 1e-13 and rel_max(pr, pref) <= 1e-13
