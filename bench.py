@@ -358,6 +358,55 @@ def run_adjoint(device: int, seed: int, reps: int = 3) -> dict:
     return out
 
 
+def run_pencil(ranks: int, steps: int, warmup: int, device: int, seed: int) -> dict:
+    """The workload as a `ranks`-way pencil decomposition with every rank in
+    this process on one GPU (cdns.pencil.LocalPencil): each rank's three stages
+    per step timed with CUDA events on its stream, one rank at a time, the
+    exchanges between stages done by device copies (not timed: across GPUs
+    they are NVLink all-to-alls).  Reports per-rank stage times, their maximum
+    (a rank's device time per step) and sum (the decomposition's total
+    device work against the single-context step), and the bytes each rank
+    sends to other ranks per step."""
+    import numpy as np
+    import torch
+    from cdns import pencil
+    from cdns.fields import divergence_free_field
+    mesh, params = workload_mesh()
+    u0 = np.stack(divergence_free_field(mesh, params, seed=seed, amp=0.1, spectrum="k53", mean="loglaw"),
+                  axis=-1)
+    lp = pencil.LocalPencil(mesh, params, ranks, device)
+    try:
+        lp.set_velocity(u0)
+        lp.run(1, warmup)
+        streams = [m.torch_stream() for m in lp.members]
+        ms = np.zeros((ranks, 3))
+        for it in range(warmup + 1, warmup + 1 + steps):
+            for st in range(3):
+                for r, m in enumerate(lp.members):
+                    a = torch.cuda.Event(enable_timing=True)
+                    b = torch.cuda.Event(enable_timing=True)
+                    a.record(streams[r])
+                    m.stage(it, st)
+                    b.record(streams[r])
+                    m.synchronize()
+                    ms[r, st] += a.elapsed_time(b)
+                if st < 2:
+                    lp._exchange(st)
+        ms /= steps
+        sent = [sum(8 * (sum(m.exchange_counts(e)[0]) - m.exchange_counts(e)[0][r]) for e in (0, 1))
+                for r, m in enumerate(lp.members)]
+        finite = bool(np.isfinite(lp.get_velocity()).all())
+    finally:
+        lp.close()
+    per_rank = ms.sum(axis=1)
+    return {"ranks": ranks, "steps": steps, "layout": pencil.layout(mesh, ranks),
+            "stage_ms": [[round(float(x), 5) for x in row] for row in ms],
+            "rank_max_ms": float(per_rank.max()), "rank_sum_ms": float(per_rank.sum()),
+            "bytes_to_peers_per_step": max(sent), "finite": finite,
+            "emulated": "all ranks in one process on one GPU, stages one rank at a time, "
+                        "exchanges by device copies (untimed)"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -372,6 +421,8 @@ def main():
     ap.add_argument("--ensemble-steps", type=int, default=200)
     ap.add_argument("--no-adjoint", action="store_true", help="skip the discrete-adjoint arm")
     ap.add_argument("--no-output", action="store_true", help="skip the statistics-sampling arm")
+    ap.add_argument("--pencil", type=int, default=0,
+                    help="also time a P-rank pencil decomposition of the workload on this GPU (0: skip)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -542,6 +593,13 @@ def main():
     if not args.no_adjoint:
         adjoint = run_adjoint(local, 2000 + rank)
 
+    # ---- pencil decomposition, emulated on this GPU (opt-in) ---------------
+    pencil_arm = None
+    if args.pencil > 0 and world == 1:
+        pencil_arm = run_pencil(args.pencil, min(K, 20), W, local, 1)
+        pencil_arm["single_ms"] = ms_per_step
+        pencil_arm["overhead"] = pencil_arm["rank_sum_ms"] / ms_per_step
+
     # ---- end to end through the C ABI with host buffers -------------------
     KE = args.e2e_steps or min(K, 200)
     ctx2 = cdns.Context(mesh, params, device=local)
@@ -603,6 +661,7 @@ def main():
             "ensemble": ensemble,
             "adjoint": adjoint,
             "statistics": output,
+            "pencil": pencil_arm,
             "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": KE, "finite": finite,
                     "protocol": "upload + steps 1..K one call each with dpdx readback + download"},
