@@ -91,3 +91,42 @@ def test_restart_reader_checks(tmp_path):
         with pytest.raises(cdns.CdnsError):
             c.read_restart(str(path))
         assert np.array_equal(c.get_velocity(), u)
+
+
+@pytest.mark.parametrize("text", [False, True])
+def test_saved_restart_matches_continuous_run(tmp_path, text):
+    """tests/test_simulation.cpp:169-231: an 8^3 channel (NXS = NZS = 4,
+    NYS = 6, no dealiasing, constant flow rate, DT = 1e-4) run 6 steps, against
+    3 steps, a restart file (text or binary), a fresh context that reads it
+    (the checkpoint bit for bit, step 3, time 3 DT) and 3 more steps.  A restart
+    holds no multistep history, so the continuation repeats the first-order
+    startup (src/sim/simulation.cpp:36-45): relative L2 below 1e-7."""
+    import dataclasses
+    from oracle_cases import divergence_free_field, example_case
+    m, p = example_case(NXS=4, NYS=6, NZS=4, N2=8, N=8)
+    p = dataclasses.replace(p, DT=1e-4)
+    u0 = np.stack(divergence_free_field(m, p, seed=12, amp=0.01), axis=-1)
+    cont = ctx_for(m, p)
+    cont.set_velocity(u0)
+    cont.run(1, 6)
+    cont.synchronize()
+    ucont = cont.get_velocity()
+    first = ctx_for(m, p)
+    first.set_velocity(u0)
+    first.run(1, 3)
+    first.synchronize()
+    ck = first.get_velocity()
+    path = tmp_path / ("field_S_ 0.dat" if text else "field_S_ 0.bin")
+    first.write_restart(str(path), 3, 3 * p.DT, text=text)
+    first.close()
+    res = ctx_for(m, p)
+    step, time = res.read_restart(str(path))
+    assert step == 3 and abs(time - 3 * p.DT) <= 1e-18
+    assert np.array_equal(res.get_velocity(), ck)
+    res.run(1, 3)
+    res.synchronize()
+    u = res.get_velocity()
+    assert np.isfinite(u).all()
+    assert np.sum(np.abs(ucont - u0) ** 2) > 1e-16          # an evolving field
+    err = np.sqrt(np.sum(np.abs(u - ucont) ** 2) / np.sum(np.abs(ucont) ** 2))
+    assert err < 1e-7
