@@ -764,7 +764,7 @@ int cdns_last_error(char *buf, size_t len) {
     return CDNS_OK;
 }
 
-const char *cdns_version(void) { return "cdns-b200 0.3 (sm_100a, fp64 + mixed fp32/fp64, batch, discrete adjoint)"; }
+const char *cdns_version(void) { return "cdns-b200 0.4 (sm_100a, fp64 + mixed fp32/fp64, batch, discrete adjoint, pencil ranks)"; }
 
 }  // extern "C"
 

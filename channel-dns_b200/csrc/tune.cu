@@ -41,9 +41,10 @@ std::string mesh_key(const cdns_ctx *c) {
     cudaDeviceProp prop{};
     cudaGetDeviceProperties(&prop, c->device);
     const Dims &d = c->d;
-    char buf[256];
-    std::snprintf(buf, sizeof buf, "%s/%d|%d,%d,%d|%d,%d,%d", prop.name, prop.multiProcessorCount, d.NX2, d.NY2,
-                  d.NZ2, d.NXS, d.NYS, d.NZS);
+    // the device name holds at most 256 characters; seven ints and separators follow
+    char buf[256 + 96];
+    std::snprintf(buf, sizeof buf, "%.256s/%d|%d,%d,%d|%d,%d,%d", prop.name, prop.multiProcessorCount, d.NX2,
+                  d.NY2, d.NZ2, d.NXS, d.NYS, d.NZS);
     return buf;
 }
 
