@@ -19,6 +19,10 @@ envelope at 10 % rms (synthetic, cdns/fields.py).
   cpu_baseline  the reference's own sources (oracle/_ref, built with the
           project FFTW/MPI shims) on this host's cores, bounded sample.
 
+  pencil  the workload as an 8-rank pencil decomposition (one channel over
+          several GPUs) with every rank emulated on this GPU: per-rank stage
+          times and the bytes each rank exchanges per step (--pencil P).
+
 ``--impl reference`` times the reference CPU solver alone on the same
 workload.  With torchrun (N > 1) every rank advances its own channel
 (replicas, no collective in the data path; scaling "weak").
@@ -421,7 +425,7 @@ def main():
     ap.add_argument("--ensemble-steps", type=int, default=200)
     ap.add_argument("--no-adjoint", action="store_true", help="skip the discrete-adjoint arm")
     ap.add_argument("--no-output", action="store_true", help="skip the statistics-sampling arm")
-    ap.add_argument("--pencil", type=int, default=0,
+    ap.add_argument("--pencil", type=int, default=8,
                     help="also time a P-rank pencil decomposition of the workload on this GPU (0: skip)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -596,9 +600,12 @@ def main():
     # ---- pencil decomposition, emulated on this GPU (opt-in) ---------------
     pencil_arm = None
     if args.pencil > 0 and world == 1:
-        pencil_arm = run_pencil(args.pencil, min(K, 20), W, local, 1)
-        pencil_arm["single_ms"] = ms_per_step
-        pencil_arm["overhead"] = pencil_arm["rank_sum_ms"] / ms_per_step
+        try:
+            pencil_arm = run_pencil(args.pencil, min(K, 20), W, local, 1)
+            pencil_arm["single_ms"] = ms_per_step
+            pencil_arm["overhead"] = pencil_arm["rank_sum_ms"] / ms_per_step
+        except Exception as exc:  # an auxiliary arm must not hide the main line
+            pencil_arm = {"ranks": args.pencil, "error": str(exc)[:200]}
 
     # ---- end to end through the C ABI with host buffers -------------------
     KE = args.e2e_steps or min(K, 200)
