@@ -170,6 +170,21 @@ def coarse(m, p, spectral):
     return phys, back
 
 
+def blocks(m, p, ranks: int):
+    """The reference Mesh's block tables for a `ranks`-way split: int array
+    [ranks][5] (x_begin, x_count, y2_begin, y2_count, owns_zero_x_mode), or
+    None if Mesh rejects the split."""
+    d = tempfile.mkdtemp(prefix="cdns_ref_")
+    write_config(d, m, p, 1)
+    out = os.path.join(d, "b.bin")
+    subprocess.run([RUNNER, "blocks", d, str(ranks), out], check=True, capture_output=True)
+    raw = np.frombuffer(open(out, "rb").read(), dtype="<i4").copy()
+    _rmtree(d)
+    if raw.size == 1 and raw[0] == -1:
+        return None
+    return raw.reshape(ranks, 5)
+
+
 def reduce(m, p, velocity, pressure):
     """Reference output branch on a state: physical (u, v, w, p), plane sums
     [NY+1][20], plane finite flags, (EKT, TKE, div_L2, finite)."""

@@ -31,7 +31,13 @@
 //       sigma correction (src/solver/eqsolve_pv.cpp:311-450); input is the
 //       velocity RHS [kz][y][kx][3], pressure BC [kz][2][kx], velocity BC
 //       [kz][2][kx][3]; writes pressure, velocity, u_dpdx_unit, w_dpdz_unit.
+//   ref_runner blocks <run-dir> <ranks> <out.bin>
+//       The distributed block tables of Mesh (src/core/mesh.cpp:20-85) for a
+//       <ranks>-way split (INDEX_Serial = 0): per rank, int32 x_begin,
+//       x_count, y2_begin, y2_count, owns_zero_x_mode; or a single int32 -1
+//       if Mesh rejects the split.
 #include <chrono>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
@@ -85,7 +91,7 @@ void fill(Array4D<std::complex<double>> &f, const std::complex<double> *src) {
 
 int main(int argc, char **argv) {
     if (argc < 4) {
-        std::cerr << "usage: ref_runner run|nonlinear|fine|coarse|reduce|dump|solve <run-dir> ...\n";
+        std::cerr << "usage: ref_runner run|nonlinear|fine|coarse|reduce|dump|solve|blocks <run-dir> ...\n";
         return 2;
     }
     const std::string mode = argv[1];
@@ -197,6 +203,24 @@ int main(int argc, char **argv) {
             io.write_restart(ntpit, t, velocity);
             io.write_physical(ntpit, t, snapshot);
             return 0;
+        }
+        if (mode == "blocks" && argc >= 5) {
+            const int ranks = std::atoi(argv[3]);
+            MeshParm mp = params.mesh;
+            mp.INDEX_Serial = 0;
+            std::vector<std::int32_t> table;
+            try {
+                for (int r = 0; r < ranks; ++r) {
+                    Mesh m(mp, params.parm.XL, params.parm.ZL, r, ranks);
+                    table.insert(table.end(), {m.x_begin(r), m.x_count(r), m.y2_begin(r), m.y2_count(r),
+                                               m.owns_zero_x_mode() ? 1 : 0});
+                }
+            } catch (const std::invalid_argument &) {
+                table.assign(1, -1);
+            }
+            std::ofstream out(argv[4], std::ios::binary);
+            write(out, table.data(), table.size());
+            return out ? 0 : 1;
         }
         if (mode == "solve" && argc >= 6) {
             const double g = std::atof(argv[3]);

@@ -25,9 +25,12 @@ on small seeded inputs and stores inputs and outputs as compressed npz files:
   golden_reduce.npz     the output branch on a 16x17x16 state (a divergence-free
                         field plus a non-solenoidal part): physical u, v, w,
                         p, plane sums, finite flags, EKT/TKE/div_L2.
+  golden_blocks.npz     the reference Mesh's distributed block tables (x block,
+                        fine-grid y slab, zero-mode owner) for 1..12 ranks on
+                        four meshes, and the splits it rejects.
 
 Usage: python tests/golden/make_golden.py [name ...]   (needs oracle/_ref built;
-names: step example nonlinear solve fine coarse reduce files, default all)
+names: step example nonlinear solve fine coarse reduce files blocks, default all)
 """
 import os
 import sys
@@ -93,11 +96,34 @@ def dump_files(which):
                            for k, v in files.items()})
 
 
+BLOCK_CASES = {
+    # tests/test_mesh.cpp:10-22 (32^3, NXS = NZS = 16, NYS = 30, 48^3 product grid)
+    "distributed": lambda: example_case(NXS=16, NYS=30, NZS=16, N2=48, N=32),
+    "channel32": lambda: channel_case(32),
+    "retau180": lambda: channel_case(128),
+    "narrow": lambda: example_case(NXS=1, NYS=6, NZS=2, N2=8, N=8),
+}
+
+
+def block_tables(which):
+    if "blocks" not in which:
+        return
+    out = {}
+    for tag, make in BLOCK_CASES.items():
+        m, p = make()
+        out[f"{tag}_mesh"] = mesh_dict(m, p)["mesh"]
+        for ranks in range(1, 13):
+            t = ref_io.blocks(m, p, ranks)
+            out[f"{tag}_{ranks}"] = np.array([-1], dtype=np.int32) if t is None else t
+    np.savez_compressed(os.path.join(HERE, "golden_blocks.npz"), **out)
+
+
 def main(which):
     if not ref_io.available():
         raise SystemExit("oracle/_ref is not built: run make -C oracle")
     coarse_and_reduce(which)
     dump_files(which)
+    block_tables(which)
     if "step" not in which:
         print("golden fixtures written to", HERE)
         return
@@ -151,4 +177,5 @@ def _cheb_1my2(ncy):
 
 
 if __name__ == "__main__":
-    main(set(sys.argv[1:]) or {"step", "example", "nonlinear", "solve", "fine", "coarse", "reduce", "files"})
+    main(set(sys.argv[1:]) or {"step", "example", "nonlinear", "solve", "fine", "coarse", "reduce", "files",
+                               "blocks"})

@@ -1,5 +1,6 @@
 """The pencil decomposition's host side on CPU: the block tables (the
-reference's tests/test_mesh.cpp:26-51 restated), the per-peer exchange counts,
+reference's tests/test_mesh.cpp:26-51 restated, and the reference Mesh's own
+tables as golden vectors), the per-peer exchange counts,
 and both exchanges of a step between two gloo ranks through cdns.pencil's
 exchange() -- the call the GPU ranks make over NCCL -- with the packed chunk
 order the device pack and unpack kernels use ([field][y][kz][kx], chunks in
@@ -38,6 +39,26 @@ def test_blocks_cover_every_index_once(ranks):
         sizes = [t[col] for t in lay]
         extra = n % ranks
         assert sizes == [n // ranks + (1 if r >= ranks - extra else 0) for r in range(ranks)]
+
+
+def test_layout_matches_the_reference_mesh_tables():
+    """tests/golden/golden_blocks.npz: the reference Mesh's own block tables
+    (its sources compiled in oracle/_ref) for 1..12 ranks on four meshes --
+    the kx block, the fine-grid y slab and the zero-mode owner of every rank,
+    and the splits it rejects."""
+    from golden_io import GOLDEN
+    d = np.load(os.path.join(GOLDEN, "golden_blocks.npz"))
+    for tag in ("distributed", "channel32", "retau180", "narrow"):
+        mesh = cdns.Mesh(*[int(v) for v in d[f"{tag}_mesh"]], 1.0, 1.0)
+        for ranks in range(1, 13):
+            ref = d[f"{tag}_{ranks}"]
+            if ref.size == 1 and ref[0] == -1:
+                with pytest.raises(cdns.CdnsError):
+                    pencil.layout(mesh, ranks)
+                continue
+            lay = pencil.layout(mesh, ranks)
+            assert [list(t) for t in lay] == ref[:, :4].tolist(), (tag, ranks)
+            assert [1 if t[0] == 0 else 0 for t in lay] == ref[:, 4].tolist()
 
 
 def test_rejects_empty_blocks():
