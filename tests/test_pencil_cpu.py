@@ -69,6 +69,19 @@ def test_rejects_empty_blocks():
         pencil.layout(_distributed_mesh(), 0)
 
 
+def test_host_calls_reject_bad_arguments():
+    """The host-only entry points check their arguments before any work:
+    exchange index, rank index, rank count (1..64) and empty blocks."""
+    m = _distributed_mesh()
+    for bad in [(2, 0, 2), (2, 2, 0), (2, -1, 0), (65, 0, 0), (18, 0, 0)]:
+        ranks, rank, exchange = bad
+        with pytest.raises(cdns.CdnsError) as e:
+            pencil.counts(m, ranks, rank, exchange)
+        assert e.value.code == 1, bad
+    with pytest.raises(cdns.CdnsError):
+        pencil.layout(m, 65)
+
+
 @pytest.mark.parametrize("ranks", [2, 3, 5])
 def test_exchange_counts_pair_up(ranks):
     """What rank r sends to q is what q expects from r, and each exchange moves
