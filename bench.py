@@ -362,7 +362,7 @@ def run_adjoint(device: int, seed: int, reps: int = 3) -> dict:
     return out
 
 
-def run_pencil(ranks: int, steps: int, warmup: int, device: int, seed: int) -> dict:
+def run_pencil(ranks: int, steps: int, warmup: int, device: int, seed: int, exchange: str = "copy") -> dict:
     """The workload as a `ranks`-way pencil decomposition with every rank in
     this process on one GPU (cdns.pencil.LocalPencil): each rank's three stages
     per step timed with CUDA events on its stream, one rank at a time, the
@@ -378,7 +378,7 @@ def run_pencil(ranks: int, steps: int, warmup: int, device: int, seed: int) -> d
     mesh, params = workload_mesh()
     u0 = np.stack(divergence_free_field(mesh, params, seed=seed, amp=0.1, spectrum="k53", mean="loglaw"),
                   axis=-1)
-    lp = pencil.LocalPencil(mesh, params, ranks, device)
+    lp = pencil.LocalPencil(mesh, params, ranks, device, exchange=exchange)
     try:
         lp.set_velocity(u0)
         lp.run(1, warmup)
@@ -394,7 +394,7 @@ def run_pencil(ranks: int, steps: int, warmup: int, device: int, seed: int) -> d
                     b.record(streams[r])
                     m.synchronize()
                     ms[r, st] += a.elapsed_time(b)
-                if st < 2:
+                if st < 2 and exchange == "copy":
                     lp._exchange(st)
         ms /= steps
         sent = [sum(8 * (sum(m.exchange_counts(e)[0]) - m.exchange_counts(e)[0][r]) for e in (0, 1))
@@ -403,7 +403,9 @@ def run_pencil(ranks: int, steps: int, warmup: int, device: int, seed: int) -> d
     finally:
         lp.close()
     per_rank = ms.sum(axis=1)
-    return {"ranks": ranks, "steps": steps, "layout": pencil.layout(mesh, ranks),
+    if exchange == "peer":
+        sent = [0] * ranks   # peer loads and stores instead of exchange buffers
+    return {"ranks": ranks, "steps": steps, "exchange": exchange, "layout": pencil.layout(mesh, ranks),
             "stage_ms": [[round(float(x), 5) for x in row] for row in ms],
             "rank_max_ms": float(per_rank.max()), "rank_sum_ms": float(per_rank.sum()),
             "bytes_to_peers_per_step": max(sent), "finite": finite,
@@ -604,6 +606,9 @@ def main():
             pencil_arm = run_pencil(args.pencil, min(K, 20), W, local, 1)
             pencil_arm["single_ms"] = ms_per_step
             pencil_arm["overhead"] = pencil_arm["rank_sum_ms"] / ms_per_step
+            fused = run_pencil(args.pencil, min(K, 20), W, local, 1, exchange="peer")
+            pencil_arm["fused_exchange"] = {k: fused[k] for k in ("stage_ms", "rank_max_ms", "rank_sum_ms", "finite")}
+            pencil_arm["fused_exchange"]["overhead"] = fused["rank_sum_ms"] / ms_per_step
         except Exception as exc:  # an auxiliary arm must not hide the main line
             pencil_arm = {"ranks": args.pencil, "error": str(exc)[:200]}
 

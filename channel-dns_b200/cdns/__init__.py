@@ -114,6 +114,8 @@ _SIGNATURES = {
     "cdns_pencil_buffer": [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
                            ctypes.POINTER(ctypes.c_longlong)],
     "cdns_pencil_stage": [ctypes.c_void_p, ctypes.c_int, ctypes.c_int],
+    "cdns_pencil_columns": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_longlong)],
+    "cdns_pencil_set_peers": [ctypes.c_void_p, ctypes.c_void_p],
 }
 
 

@@ -98,6 +98,23 @@ class PencilRank(Context):
         _check(lib().cdns_pencil_buffer(self._h, exchange, int(recv), ctypes.byref(p), ctypes.byref(n)))
         return torch.as_tensor(_DeviceArray(int(p.value), int(n.value)), device=f"cuda:{self.device}")
 
+    def columns(self) -> int:
+        """Device pointer of this rank's y-physical column buffer (the
+        fused exchange's peer view)."""
+        p = ctypes.c_void_p()
+        n = ctypes.c_longlong(0)
+        _check(lib().cdns_pencil_columns(self._h, ctypes.byref(p), ctypes.byref(n)))
+        return int(p.value)
+
+    def set_peers(self, columns: Optional[Sequence[int]]) -> None:
+        """Every rank's column buffer (device pointers in this process, rank
+        order) for the fused exchange; None returns to the exchange buffers."""
+        if columns is None:
+            _check(lib().cdns_pencil_set_peers(self._h, None))
+            return
+        arr = (ctypes.c_void_p * len(columns))(*[ctypes.c_void_p(int(c)) for c in columns])
+        _check(lib().cdns_pencil_set_peers(self._h, ctypes.cast(arr, ctypes.c_void_p)))
+
     def torch_stream(self):
         import torch
         return torch.cuda.ExternalStream(self.stream_ptr(), device=f"cuda:{self.device}")
@@ -133,14 +150,23 @@ def run(rank: PencilRank, first_iteration: int, nsteps: int, group=None) -> None
 
 class LocalPencil:
     """Every rank of a pencil decomposition in one process on one device.
-    Each stage runs on all ranks, then the exchange copies each peer's chunk
-    between the ranks' buffers on the device (no kernel of one rank waits on
-    another's).  The whole-channel state goes in and out in the reference
-    layout."""
+    Each stage runs on all ranks, then (exchange="copy") the exchange copies
+    each peer's chunk between the ranks' buffers on the device, or
+    (exchange="peer") the fused exchange's z transforms read and write the
+    other ranks' column buffers directly; either way no kernel of one rank
+    waits on another's, the stages are ordered by host synchronisation.  The
+    whole-channel state goes in and out in the reference layout."""
 
-    def __init__(self, mesh: Mesh, params: Params, ranks: int, device: int = 0):
+    def __init__(self, mesh: Mesh, params: Params, ranks: int, device: int = 0, exchange: str = "copy"):
+        if exchange not in ("copy", "peer"):
+            raise ValueError("exchange must be 'copy' or 'peer'")
         self.mesh = mesh
+        self.exchange = exchange
         self.members = [PencilRank(mesh, params, ranks, r, device) for r in range(ranks)]
+        if exchange == "peer":
+            cols = [m.columns() for m in self.members]
+            for m in self.members:
+                m.set_peers(cols)
 
     def close(self) -> None:
         for m in self.members:
@@ -190,7 +216,10 @@ class LocalPencil:
             for m in self.members:
                 m.stage(iteration, st)
             if st < 2:
-                self._exchange(st)
+                if self.exchange == "peer":
+                    self.synchronize()     # every rank's stage done before any reads it
+                else:
+                    self._exchange(st)
 
     def run(self, first_iteration: int, nsteps: int) -> None:
         for it in range(first_iteration, first_iteration + nsteps):

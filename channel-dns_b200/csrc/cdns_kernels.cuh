@@ -54,6 +54,24 @@ void launch_x_cross(const Dims &d, const double2 *roots, const float2 *G, float2
 void launch_z_forward(const Dims &d, const double2 *roots, const float2 *H, float2 *F, int nf, cudaStream_t s);
 void launch_x_r2c(const Dims &d, const FftPlan &P, const double2 *roots, const double *phys,
                   double2 *H, cudaStream_t s, bool coarse = false);
+// Every pencil rank's y-physical column buffer as seen from one rank: rank q
+// holds the kx block [kx0_q, kx0_q + nkx_q) in the layout [f][NY2+1][2NZS+1][nkx_q],
+// so line kx of the whole spectrum is col[kx] = &F_q[kx - kx0_q] with row stride
+// width[kx] = nkx_q.  The pointers are device pointers valid in this process.
+struct PeerCols {
+    double2 *const *col;   // [NXS+1]
+    const int *width;      // [NXS+1]
+    int ny2;               // NY2 + 1: every rank's buffer holds all y points
+    int j0;                // first y point of this rank's slab
+};
+// The z transforms of a pencil rank's y slab (ds: every kx, ny2 = the slab's
+// points) with the exchange fused in: the synthesis of the six fields reads
+// the slab's rows from every rank's columns, the analysis of the three fields
+// writes them back there.  Register forms of NZ2 only (false otherwise).
+bool launch_z_backward_peers(const Dims &ds, const double2 *roots, const PeerCols &pc, double2 *G,
+                             cudaStream_t s);
+bool launch_z_forward_peers(const Dims &ds, const double2 *roots, const double2 *H, const PeerCols &pc,
+                            cudaStream_t s);
 // Chebyshev synthesis (ana = false: spectral src0/src1 as in launch_ysynth ->
 // F) or analysis (ana = true: F in src0 -> spectral) in the FFT (DCT-I) form;
 // false if NY2 has no register split (the caller takes the matrix form).

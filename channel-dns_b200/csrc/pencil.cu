@@ -23,6 +23,7 @@
 //   exchange 0 recv / exchange 1 send: y in this slab, kx in q's block
 #include <algorithm>
 #include <new>
+#include <vector>
 
 #include "context.cuh"
 
@@ -105,6 +106,12 @@ struct PencilWork {
     PartMap block[2], slab[2];
     int next_stage = 0, iteration = 0;
     long long chunk_max[2][2] = {{0, 0}, {0, 0}};
+    // fused exchange (cdns_pencil_set_peers): per global kx, the owning rank's
+    // column pointer and row stride; the z transforms then read and write
+    // every rank's column buffer directly and the exchange buffers are idle
+    double2 **col = nullptr;
+    int *width = nullptr;
+    bool peers = false;
 };
 
 void pencil_release(PencilWork *w) { delete w; }
@@ -202,6 +209,7 @@ int pencil_init(cdns_ctx *c, int ranks, int rank) {
     for (int e = 0; e < 2; ++e)
         for (int k = 0; k < 2; ++k)
             if ((r = c->alloc(w->buf[e][k], (size_t)w->count[e][k]))) return r;
+    if ((r = c->alloc(w->col, (size_t)nkxg)) || (r = c->alloc(w->width, (size_t)nkxg))) return r;
     cudaError_t err = configure_transform_kernels(ds);
     if (err != cudaSuccess) return fail(CDNS_ERR_CUDA, cudaGetErrorString(err));
     return CDNS_OK;
@@ -252,6 +260,45 @@ int cdns_pencil_buffer(cdns_ctx *c, int exchange, int recv, void **ptr, long lon
     return CDNS_OK;
 }
 
+int cdns_pencil_columns(cdns_ctx *c, void **ptr, long long *doubles) {
+    if (!c || !ptr || !doubles) return fail(CDNS_ERR_ARG, "null argument");
+    if (!c->pen) return fail(CDNS_ERR_STATE, "not a pencil rank context");
+    *ptr = c->F;
+    *doubles = 2LL * 6 * c->d.ny2 * c->d.ncol;
+    return CDNS_OK;
+}
+
+int cdns_pencil_set_peers(cdns_ctx *c, void *const *columns) {
+    if (!c) return fail(CDNS_ERR_ARG, "null context");
+    PencilWork *w = c->pen;
+    if (!w) return fail(CDNS_ERR_STATE, "not a pencil rank context");
+    if (w->next_stage != 0) return fail(CDNS_ERR_STATE, "cdns_pencil_set_peers inside a step");
+    DeviceGuard guard(c->device);
+    if (!columns) {
+        w->peers = false;
+        return CDNS_OK;
+    }
+    const Dims ds = slab_dims(c);
+    if (!register_forms(ds)) return fail(CDNS_ERR_ARG, "the fused exchange needs NZ2 and NX2 with a register split");
+    const int nkxg = c->d.NXS + 1;
+    std::vector<double2 *> col(nkxg);
+    std::vector<int> width(nkxg);
+    for (int q = 0; q < w->ranks; ++q) {
+        if (!columns[q]) return fail(CDNS_ERR_ARG, "null peer column buffer");
+        for (int k = 0; k < w->nkx[q]; ++k) {
+            col[w->kx0[q] + k] = static_cast<double2 *>(columns[q]) + k;
+            width[w->kx0[q] + k] = w->nkx[q];
+        }
+    }
+    if (columns[w->rank] != static_cast<void *>(c->F))
+        return fail(CDNS_ERR_ARG, "this rank's entry must be its own column buffer");
+    CK(cudaMemcpyAsync(w->col, col.data(), sizeof(double2 *) * nkxg, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(w->width, width.data(), sizeof(int) * nkxg, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    w->peers = true;
+    return CDNS_OK;
+}
+
 int cdns_pencil_stage(cdns_ctx *c, int iteration, int stage) {
     if (!c) return fail(CDNS_ERR_ARG, "null context");
     PencilWork *w = c->pen;
@@ -272,16 +319,24 @@ int cdns_pencil_stage(cdns_ctx *c, int iteration, int stage) {
         if ((r = do_setup(c, g))) return r;
         launch_curl(d, c->t, c->U[k], c->om, c->bw, c->pp.Re, s);
         launch_ysynth(d, c->t, c->U[k], c->om, 3, 6, c->F, s);
-        r = part_copy(w->block[0], w->chunk_max[0][0], true, c->F, w->buf[0][0], s);
+        if (!w->peers) r = part_copy(w->block[0], w->chunk_max[0][0], true, c->F, w->buf[0][0], s);
     } else if (stage == 1) {
         const Dims ds = slab_dims(c);
-        if ((r = part_copy(w->slab[0], w->chunk_max[0][1], false, w->Fs, w->buf[0][1], s))) return r;
-        launch_z_backward(ds, c->pz, c->t.root_z, w->Fs, w->Gs, 6, s);
-        launch_x_cross(ds, c->px, c->t.root_x, w->Gs, w->Hs, s);
-        launch_z_forward(ds, c->pz, c->t.root_z, w->Hs, w->Fs, 3, s);
-        r = part_copy(w->slab[1], w->chunk_max[1][0], true, w->Fs, w->buf[1][0], s);
+        if (w->peers) {
+            const PeerCols pc{w->col, w->width, d.ny2, w->j0[w->rank]};
+            launch_z_backward_peers(ds, c->t.root_z, pc, w->Gs, s);
+            launch_x_cross(ds, c->px, c->t.root_x, w->Gs, w->Hs, s);
+            launch_z_forward_peers(ds, c->t.root_z, w->Hs, pc, s);
+        } else {
+            if ((r = part_copy(w->slab[0], w->chunk_max[0][1], false, w->Fs, w->buf[0][1], s))) return r;
+            launch_z_backward(ds, c->pz, c->t.root_z, w->Fs, w->Gs, 6, s);
+            launch_x_cross(ds, c->px, c->t.root_x, w->Gs, w->Hs, s);
+            launch_z_forward(ds, c->pz, c->t.root_z, w->Hs, w->Fs, 3, s);
+            r = part_copy(w->slab[1], w->chunk_max[1][0], true, w->Fs, w->buf[1][0], s);
+        }
     } else if (stage == 2) {
-        if ((r = part_copy(w->block[1], w->chunk_max[1][1], false, c->F, w->buf[1][1], s))) return r;
+        if (!w->peers && (r = part_copy(w->block[1], w->chunk_max[1][1], false, c->F, w->buf[1][1], s)))
+            return r;
         launch_yanalysis(d, c->t, c->F, c->Nb[k], 3, s);
         enqueue_solve(c, a0, a1, b0, b1, g);
         c->cur = 1 - k;

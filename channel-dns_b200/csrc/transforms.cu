@@ -193,6 +193,64 @@ k_z_forward_r(Dims d, const double2 *__restrict__ roots, const C *__restrict__ H
     fft2_lines<N1, N2, -1>(TL, tw, S, src, dst);
 }
 
+// The pencil rank's fused exchange: the same transforms, the spectral side
+// read from and written to every rank's column buffer (PeerCols) at the
+// slab's global y point pc.j0 + j.  Fine-grid conventions (FP64).
+struct ZExpandPeers {
+    PeerCols pc;
+    int f, jg, nkx, kx0, nkz, NZS, n;
+    __device__ __forceinline__ double2 operator()(int z, int line) const {
+        const int kx = kx0 + line;
+        if (kx >= nkx) return mk(0.0, 0.0);
+        int kz;
+        if (z <= NZS) kz = (z == n - NZS) ? -NZS : z;
+        else if (z >= n - NZS) kz = z - n;
+        else return mk(0.0, 0.0);
+        return pc.col[kx][((long long)(f * pc.ny2 + jg) * nkz + (kz + NZS)) * pc.width[kx]];
+    }
+};
+struct ZTruncPeers {
+    PeerCols pc;
+    int f, jg, nkx, kx0, nkz, NZS, n;
+    double invn;
+    __device__ __forceinline__ void operator()(int z, int line, double2 v) const {
+        const int kx = kx0 + line;
+        if (kx >= nkx) return;
+        const double2 s = cscale(invn, v);
+        double2 *p = pc.col[kx];
+        const long long row = (long long)(f * pc.ny2 + jg) * nkz;
+        const int w = pc.width[kx];
+        if (z <= NZS) p[(row + z + NZS) * w] = s;
+        if (z >= n - NZS) p[(row + z - n + NZS) * w] = s;
+    }
+};
+
+template <int N1, int N2>
+__global__ void __launch_bounds__(16 * 17)
+k_z_backward_peers(Dims d, const double2 *__restrict__ roots, PeerCols pc, double2 *__restrict__ G, int TL) {
+    extern __shared__ double2 sm_d[];
+    constexpr int n = N1 * N2;
+    double2 *S = sm_d + n;
+    const int f = blockIdx.z, j = blockIdx.y, kx0 = blockIdx.x * TL;
+    const Twiddles<double2> tw = load_twiddles<double2>(sm_d, roots, n);
+    const ZExpandPeers src{pc, f, pc.j0 + j, d.nkx, kx0, d.nkz, d.NZS, n};
+    const RowDst<double2> dst{G + ((long long)f * d.ny2 + j) * (long long)n * d.nkx, d.nkx, kx0};
+    fft2_lines<N1, N2, +1>(TL, tw, S, src, dst);
+}
+
+template <int N1, int N2>
+__global__ void __launch_bounds__(16 * 17)
+k_z_forward_peers(Dims d, const double2 *__restrict__ roots, const double2 *__restrict__ H, PeerCols pc, int TL) {
+    extern __shared__ double2 sm_d[];
+    constexpr int n = N1 * N2;
+    double2 *S = sm_d + n;
+    const int f = blockIdx.z, j = blockIdx.y, kx0 = blockIdx.x * TL;
+    const Twiddles<double2> tw = load_twiddles<double2>(sm_d, roots, n);
+    const RowSrc<double2> src{H + ((long long)f * d.ny2 + j) * (long long)n * d.nkx, d.nkx, kx0};
+    const ZTruncPeers dst{pc, f, pc.j0 + j, d.nkx, kx0, d.nkz, d.NZS, n, 1.0 / (double)n};
+    fft2_lines<N1, N2, -1>(TL, tw, S, src, dst);
+}
+
 // ---------------------------------------------------------------------------
 // Chebyshev synthesis and analysis as a DCT-I of N + 1 points, N = NY2 =
 // N1 x N2, through one length-N complex FFT per column (FP64).  For x_0..x_N,
@@ -1224,6 +1282,8 @@ template <class C> cudaError_t configure_register_forms(const Dims &d) {
         e = raise_smem(k_z_backward_r<N1, N2, C>, sm);
         if (e == cudaSuccess)
             e = raise_smem(k_z_forward_r<N1, N2, C>, sm);
+        if (e == cudaSuccess && sizeof(C) == 16) e = raise_smem(k_z_backward_peers<N1, N2>, sm);
+        if (e == cudaSuccess && sizeof(C) == 16) e = raise_smem(k_z_forward_peers<N1, N2>, sm);
     });
     return e;
 }
@@ -1296,6 +1356,28 @@ bool z_forward_r(const Dims &d, const double2 *roots, const C *H, C *F, int nf, 
         constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
         k_z_forward_r<N1, N2, C><<<grid, (N1 > N2 ? N1 : N2) * tl, smem_zfft_r(d, N1, N2, sizeof(C)), s>>>(
             d, roots, H, F, tl, coarse);
+    });
+}
+
+bool launch_z_backward_peers(const Dims &d, const double2 *roots, const PeerCols &pc, double2 *G,
+                             cudaStream_t s) {
+    const int tl = z_lines(d);
+    dim3 grid((d.nkx + tl - 1) / tl, d.ny2, 6);
+    return with_xsplit(d.NZ2, [&](auto a, auto b) {
+        constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
+        k_z_backward_peers<N1, N2><<<grid, (N1 > N2 ? N1 : N2) * tl, smem_zfft_r(d, N1, N2, sizeof(double2)), s>>>(
+            d, roots, pc, G, tl);
+    });
+}
+
+bool launch_z_forward_peers(const Dims &d, const double2 *roots, const double2 *H, const PeerCols &pc,
+                            cudaStream_t s) {
+    const int tl = z_lines(d);
+    dim3 grid((d.nkx + tl - 1) / tl, d.ny2, 3);
+    return with_xsplit(d.NZ2, [&](auto a, auto b) {
+        constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
+        k_z_forward_peers<N1, N2><<<grid, (N1 > N2 ? N1 : N2) * tl, smem_zfft_r(d, N1, N2, sizeof(double2)), s>>>(
+            d, roots, H, pc, tl);
     });
 }
 

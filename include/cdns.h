@@ -356,6 +356,22 @@ int cdns_pencil_create(const cdns_mesh_desc *mesh, const cdns_params *params, in
 int cdns_pencil_buffer(cdns_ctx *ctx, int exchange, int recv, void **ptr, long long *doubles);
 int cdns_pencil_stage(cdns_ctx *ctx, int iteration, int stage);
 
+/* Fused exchange: instead of pack -> all-to-all -> unpack, stage 1's z
+ * synthesis reads its slab's rows of y-physical columns straight from every
+ * rank's column buffer and its z analysis writes the nonlinear term back
+ * there (plain loads and stores; across GPUs, peer access over NVLink).
+ * cdns_pencil_columns gives this rank's column buffer (device pointer and
+ * length in doubles); cdns_pencil_set_peers(ctx, columns) takes every rank's,
+ * in rank order, as device pointers valid in this process (CUDA IPC or peer
+ * mappings across processes; entry `rank` must be this context's own), and
+ * NULL returns to the exchange buffers.  With peers set, a step is stage 0 on
+ * every rank, then stage 1 once all ranks finished stage 0, then stage 2 once
+ * all finished stage 1 (the caller's barrier; no kernel waits on another
+ * rank).  Needs NX2 and NZ2 with a register split (32, 48, 64, 72, 96, 128,
+ * 144, 192, 196). */
+int cdns_pencil_columns(cdns_ctx *ctx, void **ptr, long long *doubles);
+int cdns_pencil_set_peers(cdns_ctx *ctx, void *const *columns);
+
 #ifdef __cplusplus
 }
 #endif

@@ -41,13 +41,17 @@ def _reference(m, p, u0, nsteps):
     return out
 
 
-@pytest.mark.parametrize("case,ranks", [("channel32", 1), ("channel32", 2), ("channel32", 3),
-                                        ("example", 3), ("example", 5)])
-def test_local_pencil_matches_single_context(case, ranks, monkeypatch):
+@pytest.mark.parametrize("case,ranks,exchange", [("channel32", 1, "copy"), ("channel32", 2, "copy"),
+                                                 ("channel32", 3, "copy"), ("example", 3, "copy"),
+                                                 ("example", 5, "copy"), ("channel32", 1, "peer"),
+                                                 ("channel32", 3, "peer"), ("example", 5, "peer")])
+def test_local_pencil_matches_single_context(case, ranks, exchange, monkeypatch):
     """4 steps (the two setup steps and two steady ones): velocity, pressure
     and dp/dx of the decomposed step equal the single-context step to 1e-13
     (32 x 33 x 32 channel at fixed dp/dx, 48^3 product grid; the 32^3 example
-    case at constant flow rate, full Nyquist spectrum, ragged blocks)."""
+    case at constant flow rate, full Nyquist spectrum, ragged blocks), with the
+    exchange by packed buffers and with the fused exchange (z transforms on
+    the other ranks' column buffers)."""
     monkeypatch.setenv("CDNS_Y_TRANSFORM", "matrix")   # the form the rank contexts use
     if case == "channel32":
         m, p = channel_case(32)
@@ -57,7 +61,7 @@ def test_local_pencil_matches_single_context(case, ranks, monkeypatch):
         u0 = np.stack(divergence_free_field(m, p, seed=3, amp=0.05), axis=-1)
     uref, pref, dref = _reference(m, p, u0, 4)
     mesh, params = _desc(m, p)
-    lp = pencil.LocalPencil(mesh, params, ranks)
+    lp = pencil.LocalPencil(mesh, params, ranks, exchange=exchange)
     try:
         lp.set_velocity(u0)
         lp.run(1, 4)
@@ -84,6 +88,19 @@ def test_pencil_rank_refuses_whole_channel_calls_and_misordered_stages():
         assert e.value.code == 3
         with pytest.raises(ValueError):
             r.set_velocity(np.zeros(m.spectral_shape() + (3,), dtype=np.complex128))   # whole channel
+        with pytest.raises(cdns.CdnsError, match="register split"):
+            r.set_peers([r.columns(), r.columns()])   # NX2 = NZ2 = 24: no fused exchange
+    finally:
+        r.close()
+    m, p = channel_case(32)
+    mesh, params = _desc(m, p)
+    r = pencil.PencilRank(mesh, params, 2, 1)
+    try:
+        own = r.columns()
+        for bad, what in (([own, 0], "null"), ([0, own], "null"), ([own, own + 16], "own column")):
+            with pytest.raises(cdns.CdnsError, match=what) as e:
+                r.set_peers(bad)
+            assert e.value.code == 1
     finally:
         r.close()
 
