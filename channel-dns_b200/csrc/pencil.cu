@@ -324,7 +324,8 @@ int cdns_pencil_stage(cdns_ctx *c, int iteration, int stage) {
         const Dims ds = slab_dims(c);
         if (w->peers) {
             const PeerCols pc{w->col, w->width, d.ny2, w->j0[w->rank]};
-            launch_z_backward_peers(ds, c->t.root_z, pc, w->Gs, s);
+            if (!launch_z_backward_peers(ds, c->t.root_z, pc, w->Gs, s))
+                return fail(CDNS_ERR_ARG, "the fused exchange needs NZ2 with a register split");
             launch_x_cross(ds, c->px, c->t.root_x, w->Gs, w->Hs, s);
             launch_z_forward_peers(ds, c->t.root_z, w->Hs, pc, s);
         } else {
