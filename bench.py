@@ -157,9 +157,11 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def reference_arm_time(steps: int, warmup: int, threads: int):
+def reference_arm_time(steps: int, warmup: int, threads: int, reps: int = 1):
     """Steady steps/s of the reference CPU solver: T(n1 + steps) - T(n1),
-    each run from the same restart (setup and final output cancel)."""
+    each run from the same restart (setup and final output cancel); the
+    median of `reps` such pairs (tests/tools/bench_hybrid.py:52-88 takes the
+    median of 3)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import ref_io  # the reference sources built in oracle/_ref (checker / baseline only)
     import cdns
@@ -183,17 +185,21 @@ def reference_arm_time(steps: int, warmup: int, threads: int):
     p.a_V, p.b_V, p.INDEX_GRAD_PRE, p.THETA, p.V_Microblow0 = (1.0, 1.0, 1.0), (0.0, 0.0, 0.0), 1, 0.0, 0.0
     if ref_io.available():
         n1 = max(warmup, 2)
-        _, _, t1 = ref_io.run_steps(m, p, u0, n1, threads=threads)
-        _, _, t2 = ref_io.run_steps(m, p, u0, n1 + steps, threads=threads)
-        dt = max(t2 - t1, 1e-9)
-        return steps / dt, {"kind": "reference", "cores": threads,
-                            "sample": f"reference sources + project FFT shim (oracle/_ref), "
-                                      f"T({n1 + steps} steps) - T({n1} steps) from one restart, "
-                                      f"{threads} threads",
-                            # the reference's own --timing counts every step of a run, the two
-                            # setup steps (EqSolvePV::setup at iterations 1-2) included
-                            "with_setup": {"value": (n1 + steps) / max(t2, 1e-9), "unit": "steps/s",
-                                           "steps": n1 + steps}}
+        steady, whole = [], []
+        for _ in range(max(reps, 1)):
+            _, _, t1 = ref_io.run_steps(m, p, u0, n1, threads=threads)
+            _, _, t2 = ref_io.run_steps(m, p, u0, n1 + steps, threads=threads)
+            steady.append(steps / max(t2 - t1, 1e-9))
+            whole.append((n1 + steps) / max(t2, 1e-9))
+        return statistics.median(steady), {
+            "kind": "reference", "cores": threads,
+            "sample": f"reference sources + project FFT shim (oracle/_ref), "
+                      f"T({n1 + steps} steps) - T({n1} steps) from one restart, {threads} threads, "
+                      f"median of {len(steady)}",
+            "runs": [round(v, 4) for v in steady],
+            # the reference's own --timing counts every step of a run, the two
+            # setup steps (EqSolvePV::setup at iterations 1-2) included
+            "with_setup": {"value": statistics.median(whole), "unit": "steps/s", "steps": n1 + steps}}
     # the numpy restatement, single thread, one steady step
     import numpy as np
     import channel_oracle as orc
@@ -215,7 +221,7 @@ def run_reference(args, world, rank):
         return
     threads = os.cpu_count() or 1
     steps = max(1, min(args.steps, 10))
-    v, info = reference_arm_time(steps, args.warmup, threads)
+    v, info = reference_arm_time(steps, args.warmup, threads, reps=3)
     line = {"metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": args.gpus, "steps": steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
