@@ -478,8 +478,15 @@ def main():
     clocks = ClockSampler(local)
     clocks.start()
     ctx.set_velocity(host_u.numpy())
-    ctx.run(1, W)
+    # iterations 1-2 each run EqSolvePV::setup (its g changes): timed apart, not in `value`
+    s0 = torch.cuda.Event(enable_timing=True)
+    s1 = torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    ctx.run(1, 2)
+    s1.record(stream)
+    ctx.run(3, W - 2)
     ctx.synchronize()
+    setup_ms = s0.elapsed_time(s1)
     barrier()
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
@@ -688,6 +695,8 @@ def main():
                     "d2h_bytes_per_step": d2h, "steps": KE, "finite": finite,
                     "protocol": "upload + steps 1..K one call each with dpdx readback + download"},
             "clocks": clk,
+            "setup_steps": {"ms": setup_ms, "steps": 2,
+                            "what": "iterations 1-2, each with the solver setup; excluded from value"},
             "gpu_launches": len(per_launch) * K,   # one kernel per stage per step
         }
         print(json.dumps(line), flush=True)
