@@ -143,6 +143,21 @@ def step(rank: PencilRank, iteration: int, group=None) -> None:
         rank.stage(iteration, e + 1)
 
 
+def share_dpdx(rank, group=None) -> Tuple[float, float]:
+    """dp/dx and dp/dz of the last step on every rank of the group: rank 0
+    holds the zero mode and computes them, the others receive them (the
+    reference's broadcast from the zero-mode owner after correct_flow,
+    src/sim/simulation.cpp:135-139).
+    Uses `rank.rank`, `rank.device` and `rank.dpdx()` (rank 0 only); a CUDA
+    tensor over NCCL, a CPU tensor over gloo."""
+    import torch
+    import torch.distributed as dist
+    dev = torch.device(f"cuda:{rank.device}") if dist.get_backend(group) == "nccl" else torch.device("cpu")
+    t = torch.tensor(rank.dpdx() if rank.rank == 0 else (0.0, 0.0), dtype=torch.float64, device=dev)
+    dist.broadcast(t, src=dist.get_global_rank(group, 0) if group is not None else 0, group=group)
+    return float(t[0].item()), float(t[1].item())
+
+
 def run(rank: PencilRank, first_iteration: int, nsteps: int, group=None) -> None:
     for it in range(first_iteration, first_iteration + nsteps):
         step(rank, it, group)

@@ -174,23 +174,59 @@ def _worker(rank, world, port, q):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2, 3])
-def test_two_exchanges_of_a_step_over_gloo(world):
+class _RankStub:
+    """The attributes share_dpdx reads from a PencilRank."""
+
+    def __init__(self, rank):
+        self.rank, self.device = rank, 0
+
+    def dpdx(self):
+        assert self.rank == 0, "only the zero-mode owner computes dp/dx"
+        return (1.5, -0.25)
+
+
+def _dpdx_worker(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        got = pencil.share_dpdx(_RankStub(rank))
+        out = [None] * world
+        dist.all_gather_object(out, got)
+        if rank == 0:
+            q.put(out)
+    finally:
+        dist.destroy_process_group()
+
+
+def _spawn(target, world):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, world, port, q)) for r in range(world)]
+    procs = [ctx.Process(target=target, args=(r, world, port, q)) for r in range(world)]
     for p in procs:
         p.start()
     try:
-        flags = q.get(timeout=120)
+        res = q.get(timeout=120)
     finally:
         for p in procs:
             p.join(timeout=60)
             if p.is_alive():
                 p.kill()
     assert all(p.exitcode == 0 for p in procs)
-    assert flags == [(True, True)] * world
+    return res
+
+
+def test_pressure_gradient_reaches_every_rank():
+    """src/sim/simulation.cpp:135-139: the zero-mode owner's dp/dx, dp/dz
+    broadcast to the other ranks (3 gloo ranks)."""
+    assert _spawn(_dpdx_worker, 3) == [(1.5, -0.25)] * 3
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_two_exchanges_of_a_step_over_gloo(world):
+    assert _spawn(_worker, world) == [(True, True)] * world
 
 
 def _free_port() -> int:
