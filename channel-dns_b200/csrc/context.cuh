@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdlib>
 #include <string>
 #include <vector>
 
@@ -82,6 +83,13 @@ struct cdns_ctx {
     template <typename T> int alloc(T *&ptr, size_t count) {
         void *p = nullptr;
         const size_t b = sizeof(T) * (count ? count : 1);
+        // CDNS_DEVICE_BYTES_CAP=<bytes>: refuse allocations past a cap (host-side
+        // injection of an out-of-memory failure for tests)
+        if (const char *cap = std::getenv("CDNS_DEVICE_BYTES_CAP")) {
+            const unsigned long long limit = std::strtoull(cap, nullptr, 10);
+            if (limit > 0 && bytes + b > limit)
+                return cdns::fail(CDNS_ERR_NOMEM, "device allocation cap (CDNS_DEVICE_BYTES_CAP) reached");
+        }
         cudaError_t e = cudaMalloc(&p, b);
         if (e != cudaSuccess)
             return cdns::fail(CDNS_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));

@@ -259,6 +259,24 @@ def test_nonfinite_input_is_reported():
     assert e.value.code == 4
 
 
+def test_allocation_failure_is_reported_and_leaves_the_device_usable(monkeypatch):
+    """An out-of-memory failure injected on the host (a device-bytes cap below
+    what a context needs): cdns_create returns CDNS_ERR_NOMEM and frees what it
+    had taken; with the cap lifted the next context steps normally."""
+    m, p = channel_case(16)
+    monkeypatch.setenv("CDNS_DEVICE_BYTES_CAP", str(64 * 1024))
+    with pytest.raises(cdns.CdnsError) as e:
+        ctx_for(m, p)
+    assert e.value.code == 6
+    monkeypatch.delenv("CDNS_DEVICE_BYTES_CAP")
+    c = ctx_for(m, p)
+    c.set_velocity(np.stack(divergence_free_field(m, p, seed=1, amp=0.05, kmax=3), axis=-1))
+    c.run(1, 3)
+    c.synchronize()
+    assert np.isfinite(c.get_velocity()).all()
+    c.close()
+
+
 def test_bad_mesh_is_rejected():
     m, p = channel_case(16)
     with pytest.raises(cdns.CdnsError) as e:
