@@ -116,6 +116,8 @@ _SIGNATURES = {
     "cdns_pencil_stage": [ctypes.c_void_p, ctypes.c_int, ctypes.c_int],
     "cdns_pencil_columns": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_longlong)],
     "cdns_pencil_set_peers": [ctypes.c_void_p, ctypes.c_void_p],
+    "cdns_pencil_ipc_handle": [ctypes.c_void_p, ctypes.c_void_p],
+    "cdns_pencil_open_peer": [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)],
 }
 
 

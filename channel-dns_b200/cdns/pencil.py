@@ -115,6 +115,22 @@ class PencilRank(Context):
         arr = (ctypes.c_void_p * len(columns))(*[ctypes.c_void_p(int(c)) for c in columns])
         _check(lib().cdns_pencil_set_peers(self._h, ctypes.cast(arr, ctypes.c_void_p)))
 
+    def ipc_handle(self) -> bytes:
+        """CUDA IPC handle of this rank's column buffer (to send to the other
+        ranks of a multi-process decomposition)."""
+        buf = ctypes.create_string_buffer(64)
+        _check(lib().cdns_pencil_ipc_handle(self._h, ctypes.cast(buf, ctypes.c_void_p)))
+        return buf.raw
+
+    def open_peer(self, handle: bytes) -> int:
+        """Map a peer rank's column buffer into this process; its device pointer."""
+        if len(handle) != 64:
+            raise ValueError("a CUDA IPC handle has 64 bytes")
+        buf = ctypes.create_string_buffer(bytes(handle), 64)
+        p = ctypes.c_void_p()
+        _check(lib().cdns_pencil_open_peer(self._h, ctypes.cast(buf, ctypes.c_void_p), ctypes.byref(p)))
+        return int(p.value)
+
     def torch_stream(self):
         import torch
         return torch.cuda.ExternalStream(self.stream_ptr(), device=f"cuda:{self.device}")
@@ -156,6 +172,36 @@ def share_dpdx(rank, group=None) -> Tuple[float, float]:
     t = torch.tensor(rank.dpdx() if rank.rank == 0 else (0.0, 0.0), dtype=torch.float64, device=dev)
     dist.broadcast(t, src=dist.get_global_rank(group, 0) if group is not None else 0, group=group)
     return float(t[0].item()), float(t[1].item())
+
+
+def map_peers(rank, group=None) -> List[int]:
+    """Set up the fused exchange of a multi-process decomposition (one rank
+    per process and GPU): gather every rank's IPC handle over the group, map
+    the peers' column buffers into this process and hand the pointers, in rank
+    order, to the rank context.  Uses `rank.rank`, `rank.columns()`,
+    `rank.ipc_handle()`, `rank.open_peer()` and `rank.set_peers()`."""
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    handles = [None] * world
+    dist.all_gather_object(handles, rank.ipc_handle(), group=group)
+    cols = [rank.columns() if q == rank.rank else rank.open_peer(handles[q]) for q in range(world)]
+    rank.set_peers(cols)
+    return cols
+
+
+def step_fused(rank, iteration: int, group=None) -> None:
+    """One time step with the fused exchange across processes: each stage on
+    the rank's stream, then the stream drained and a barrier over the group,
+    so that no rank reads a peer's column buffer before the peer wrote it
+    (stage 0 -> 1), nor its own before every peer wrote its rows there
+    (stage 1 -> 2).
+    Uses `rank.stage()` and `rank.synchronize()`."""
+    import torch.distributed as dist
+    for st in range(3):
+        rank.stage(iteration, st)
+        if st < 2:
+            rank.synchronize()
+            dist.barrier(group=group)
 
 
 def run(rank: PencilRank, first_iteration: int, nsteps: int, group=None) -> None:

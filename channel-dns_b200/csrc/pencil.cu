@@ -22,6 +22,7 @@
 //   exchange 0 send / exchange 1 recv: y in q's slab,  kx in this rank's block
 //   exchange 0 recv / exchange 1 send: y in this slab, kx in q's block
 #include <algorithm>
+#include <cstring>
 #include <new>
 #include <vector>
 
@@ -112,9 +113,14 @@ struct PencilWork {
     double2 **col = nullptr;
     int *width = nullptr;
     bool peers = false;
+    std::vector<void *> opened;   // peers' column buffers mapped from CUDA IPC handles
 };
 
-void pencil_release(PencilWork *w) { delete w; }
+void pencil_release(PencilWork *w) {
+    if (!w) return;
+    for (void *p : w->opened) cudaIpcCloseMemHandle(p);
+    delete w;
+}
 
 namespace {
 
@@ -265,6 +271,30 @@ int cdns_pencil_columns(cdns_ctx *c, void **ptr, long long *doubles) {
     if (!c->pen) return fail(CDNS_ERR_STATE, "not a pencil rank context");
     *ptr = c->F;
     *doubles = 2LL * 6 * c->d.ny2 * c->d.ncol;
+    return CDNS_OK;
+}
+
+int cdns_pencil_ipc_handle(cdns_ctx *c, void *handle) {
+    if (!c || !handle) return fail(CDNS_ERR_ARG, "null argument");
+    if (!c->pen) return fail(CDNS_ERR_STATE, "not a pencil rank context");
+    static_assert(sizeof(cudaIpcMemHandle_t) == CDNS_IPC_HANDLE_BYTES, "IPC handle size");
+    DeviceGuard guard(c->device);
+    cudaIpcMemHandle_t h;
+    CK(cudaIpcGetMemHandle(&h, c->F));
+    std::memcpy(handle, &h, sizeof h);
+    return CDNS_OK;
+}
+
+int cdns_pencil_open_peer(cdns_ctx *c, const void *handle, void **ptr) {
+    if (!c || !handle || !ptr) return fail(CDNS_ERR_ARG, "null argument");
+    if (!c->pen) return fail(CDNS_ERR_STATE, "not a pencil rank context");
+    DeviceGuard guard(c->device);
+    cudaIpcMemHandle_t h;
+    std::memcpy(&h, handle, sizeof h);
+    void *p = nullptr;
+    CK(cudaIpcOpenMemHandle(&p, h, cudaIpcMemLazyEnablePeerAccess));
+    c->pen->opened.push_back(p);
+    *ptr = p;
     return CDNS_OK;
 }
 

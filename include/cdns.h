@@ -56,7 +56,9 @@ typedef enum {
 typedef enum { CDNS_PRECISION_FP64 = 0, CDNS_PRECISION_MIXED = 1 } cdns_precision;
 
 /* Mesh, mirrors MeshParm (src/core/params.hpp:6-11) + XL/ZL
- * (src/core/mesh.hpp:9-37).  Single rank: INDEX_Serial = 1. */
+ * (src/core/mesh.hpp:9-37).  cdns_create holds the whole channel
+ * (INDEX_Serial = 1); cdns_pencil_create one rank of a decomposition
+ * (INDEX_Serial = 0). */
 typedef struct {
     int NX, NY, NZ;
     int NXS, NYS, NZS;
@@ -371,6 +373,14 @@ int cdns_pencil_stage(cdns_ctx *ctx, int iteration, int stage);
  * 144, 192, 196). */
 int cdns_pencil_columns(cdns_ctx *ctx, void **ptr, long long *doubles);
 int cdns_pencil_set_peers(cdns_ctx *ctx, void *const *columns);
+/* Across processes: cdns_pencil_ipc_handle writes the CUDA IPC handle of this
+ * rank's column buffer (CDNS_IPC_HANDLE_BYTES bytes, to be sent to the other
+ * ranks); cdns_pencil_open_peer maps a peer's handle into this process and
+ * returns the device pointer for cdns_pencil_set_peers (unmapped when the
+ * context is destroyed). */
+#define CDNS_IPC_HANDLE_BYTES 64
+int cdns_pencil_ipc_handle(cdns_ctx *ctx, void *handle);
+int cdns_pencil_open_peer(cdns_ctx *ctx, const void *handle, void **ptr);
 
 #ifdef __cplusplus
 }

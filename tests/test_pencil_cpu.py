@@ -224,6 +224,70 @@ def test_pressure_gradient_reaches_every_rank():
     assert _spawn(_dpdx_worker, 3) == [(1.5, -0.25)] * 3
 
 
+class _FusedStub:
+    """A rank as map_peers and step_fused see it: fake device pointers and
+    handles, and stages that log their start and end (the first stage of
+    rank 0 is slow, so an ordering mistake shows)."""
+
+    def __init__(self, rank):
+        self.rank, self.peers, self.log = rank, None, []
+
+    def columns(self):
+        return 1000 + self.rank
+
+    def ipc_handle(self):
+        return bytes([self.rank]) * 64
+
+    def open_peer(self, handle):
+        assert len(handle) == 64 and handle[0] != self.rank
+        return 5000 + handle[0]
+
+    def set_peers(self, cols):
+        self.peers = list(cols)
+
+    def stage(self, it, st):
+        import time
+        t0 = time.monotonic()
+        if self.rank == 0 and st == 0:
+            time.sleep(0.3)
+        self.log.append((it, st, t0, time.monotonic()))
+
+    def synchronize(self):
+        pass
+
+
+def _fused_worker(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        r = _FusedStub(rank)
+        pencil.map_peers(r)
+        pencil.step_fused(r, 5)
+        out = [None] * world
+        dist.all_gather_object(out, (r.peers, r.log))
+        if rank == 0:
+            q.put(out)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_fused_exchange_host_sequence():
+    """Across processes: every rank maps its peers' column buffers from the
+    gathered IPC handles (its own buffer at its own index), and a step's stage
+    1 starts on no rank before stage 0 ended on all, nor stage 2 before stage 1
+    (3 gloo ranks, stub device calls)."""
+    out = _spawn(_fused_worker, 3)
+    for r, (peers, log) in enumerate(out):
+        assert peers == [1000 + q if q == r else 5000 + q for q in range(3)]
+        assert [(it, st) for it, st, _, _ in log] == [(5, 0), (5, 1), (5, 2)]
+    for st in (0, 1):
+        end = max(log[st][3] for _, log in out)
+        start = min(log[st + 1][2] for _, log in out)
+        assert end <= start, st
+
+
 @pytest.mark.parametrize("world", [2, 3])
 def test_two_exchanges_of_a_step_over_gloo(world):
     assert _spawn(_worker, world) == [(True, True)] * world
