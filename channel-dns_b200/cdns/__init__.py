@@ -72,6 +72,7 @@ _SIGNATURES = {
     "cdns_statistics_read": [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong), ctypes.c_void_p, ctypes.c_void_p],
     "cdns_statistics_reset": [ctypes.c_void_p],
     "cdns_set_velocity_device": [ctypes.c_void_p, ctypes.c_void_p],
+    "cdns_update_velocity": [ctypes.c_void_p, ctypes.c_void_p],
     "cdns_get_velocity_device": [ctypes.c_void_p, ctypes.c_void_p],
     "cdns_step": [ctypes.c_void_p, ctypes.c_int],
     "cdns_run": [ctypes.c_void_p, ctypes.c_int, ctypes.c_int],
@@ -304,6 +305,17 @@ def _input(a, shape, dtype, name: str) -> np.ndarray:
     return a
 
 
+def _output(out, shape, name: str) -> np.ndarray:
+    """A fresh complex128 array of `shape`, or `out` after checking that the C
+    call may write `shape` values into it."""
+    if out is None:
+        return np.empty(shape, dtype=np.complex128)
+    if out.dtype != np.complex128 or out.shape != tuple(shape) or not out.flags.c_contiguous \
+            or not out.flags.writeable:
+        raise ValueError(f"{name} output must be a writeable C-contiguous complex128 array of shape {tuple(shape)}")
+    return out
+
+
 # cdns_precision (include/cdns.h)
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
@@ -357,13 +369,21 @@ class Context:
         u = _input(u, self.spectral_shape + (3,), np.complex128, "velocity")
         _check(lib().cdns_set_velocity(self._h, _ptr(u)))
 
-    def get_velocity(self) -> np.ndarray:
-        out = np.empty(self.spectral_shape + (3,), dtype=np.complex128)
+    def update_velocity(self, u: np.ndarray) -> None:
+        """Replace the current velocity, keeping the multistep history (the
+        next step stays second order), as a disturbance injection does."""
+        u = _input(u, self.spectral_shape + (3,), np.complex128, "velocity")
+        _check(lib().cdns_update_velocity(self._h, _ptr(u)))
+
+    def get_velocity(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """The velocity [nkz][ncy][nkx][3]; into ``out`` (e.g. a pinned
+        buffer) when given, which must be C-contiguous complex128 of that shape."""
+        out = _output(out, self.spectral_shape + (3,), "velocity")
         _check(lib().cdns_get_velocity(self._h, _ptr(out)))
         return out
 
-    def get_pressure(self) -> np.ndarray:
-        out = np.empty(self.spectral_shape, dtype=np.complex128)
+    def get_pressure(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        out = _output(out, self.spectral_shape, "pressure")
         _check(lib().cdns_get_pressure(self._h, _ptr(out)))
         return out
 

@@ -34,7 +34,9 @@ def build(ref_root: str = "/root/reference") -> bool:
 
 
 def write_config(run_dir: str, m, p, nsteps: int, index_cont: int = 1, ndumfrq: int | None = None,
-                 nprnfrq: int | None = None, fmt: str = "binary") -> None:
+                 nprnfrq: int | None = None, fmt: str = "binary", nstat: int | None = None,
+                 physical_interval: int = 0, statistics_interval: int | None = None,
+                 ncount_disturb: int = 0, ndisturbfrq: int = 1, eps_disturb: float = 0.0) -> None:
     def f(x):
         return repr(float(x))
 
@@ -72,16 +74,16 @@ NSTEPS = {nsteps}
 NDUMFRQ = {ndumfrq or big}
 NPRNFRQ = {nprnfrq or big}
 DT = {f(p.DT)}
-NCOUNT_disturb = 0
-NDISTURBFRQ = 1
-EPS_disturb = 0.0
+NCOUNT_disturb = {ncount_disturb}
+NDISTURBFRQ = {ndisturbfrq}
+EPS_disturb = {f(eps_disturb)}
 V_Microblow0 = {f(p.V_Microblow0)}
-Nstat = {big}
+Nstat = {big if nstat is None else nstat}
 
 [output]
 format = "{fmt}"
-physical_interval = 0
-statistics_interval = {big}
+physical_interval = {physical_interval}
+statistics_interval = {big if statistics_interval is None else statistics_interval}
 """
     with open(os.path.join(run_dir, "config.toml"), "w") as fh:
         fh.write(text)
@@ -99,14 +101,23 @@ def write_restart(run_dir: str, m, velocity, ntpit: int = 0, time: float = 0.0) 
         fh.write(np.ascontiguousarray(a).astype("<c16").tobytes())
 
 
-def run_steps(m, p, velocity, nsteps: int, threads: int = 1, workdir: str | None = None):
-    """Run the reference step loop from a restart; returns (u list, pressure, wall_s)."""
+def run_steps(m, p, velocity, nsteps: int, threads: int = 1, workdir: str | None = None,
+              nstat: int | None = None):
+    """Run the reference step loop from a restart; returns (u list, pressure,
+    wall_s), and with ``nstat`` (Simulation::run samples statistics at every
+    step ntpit > nstat, src/sim/simulation.cpp:225-250) a fourth item: the
+    Statistics running means at full precision, a dict with "count",
+    "dp_means" (dpdx, dpdz) and "means" [20][NY+1] in Statistics::write's
+    order (u v w, p, uu vv ww uv vw wu, pp, pu pv pw, u^3 v^3 w^3, u^4 v^4 w^4)."""
     own = workdir is None
     d = workdir or tempfile.mkdtemp(prefix="cdns_ref_")
-    write_config(d, m, p, nsteps)
+    write_config(d, m, p, nsteps, nstat=nstat)
     write_restart(d, m, velocity)
     out = os.path.join(d, "out.bin")
-    r = subprocess.run([RUNNER, "run", d, out, str(threads)], capture_output=True, text=True)
+    cmd = [RUNNER, "run", d, out, str(threads)]
+    if nstat is not None:
+        cmd.append(os.path.join(d, "stats.bin"))
+    r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"ref_runner run failed: {r.stderr}\n{r.stdout}")
     wall = None
@@ -119,9 +130,17 @@ def run_steps(m, p, velocity, nsteps: int, threads: int = 1, workdir: str | None
     data = np.frombuffer(raw[16:], dtype="<c16")
     vel = data[: 3 * n].reshape(m.nkz, m.ncy, m.nkx, 3)
     pres = data[3 * n: 4 * n].reshape(m.nkz, m.ncy, m.nkx).copy()
+    stats = None
+    if nstat is not None:
+        sraw = open(os.path.join(d, "stats.bin"), "rb").read()
+        count, = struct.unpack("<q", sraw[:8])
+        vals = np.frombuffer(sraw[8:], dtype="<f8")
+        stats = {"count": int(count), "dp_means": (float(vals[0]), float(vals[1])),
+                 "means": vals[2:].reshape(20, m.NY + 1).copy()}
     if own:
         _rmtree(d)
-    return [vel[..., k].copy() for k in range(3)], pres, wall
+    u = [vel[..., k].copy() for k in range(3)]
+    return (u, pres, wall) if nstat is None else (u, pres, wall, stats)
 
 
 def nonlinear(m, p, velocity):

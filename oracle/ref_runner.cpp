@@ -2,11 +2,16 @@
 // (compiled from the reference tree with the FFTW/MPI shims in ref_shim/).
 // Test infrastructure only: it produces golden vectors and the CPU baseline.
 //
-//   ref_runner run <run-dir> <out.bin> [threads]
+//   ref_runner run <run-dir> <out.bin> [threads] [stats.bin]
 //       Params::load -> Mesh -> Transforms -> Simulation::initialize/run
 //       (src/main.cpp:173-225 path), then writes nt, time, the spectral
 //       velocity [kz][y][kx][3] and pressure [kz][y][kx] (complex<double>).
 //       Prints the step-loop wall time (steady_clock, as src/main.cpp:224-233).
+//       With stats.bin, also writes the run's Statistics running means at
+//       full precision (the values Statistics::write prints with 8 decimals,
+//       src/sim/statistics.cpp:117-139, :163-205): int64 count, dpdx mean,
+//       dpdz mean, then per y plane-array of NY+1 doubles in the order
+//       u v w, p, uu vv ww uv vw wu, pp, pu pv pw, u^3 v^3 w^3, u^4 v^4 w^4.
 //   ref_runner nonlinear <run-dir> <velocity.bin> <out.bin>
 //       TimeStepper::nonlinear_term (src/solver/timestepper.cpp:11-17):
 //       writes N [kz][y][kx][3] and the pressure wall BC [kz][2][kx].
@@ -67,6 +72,35 @@ struct EqSolvePVTestAccess {
     }
 };
 
+// Read access to the running means that Simulation keeps in its Statistics
+// member (src/sim/simulation.hpp:66, src/sim/statistics.hpp:34-40), which the
+// reference only prints rounded to 8 decimals.  Names used in an explicit
+// instantiation are exempt from access checking ([temp.explicit]), so each
+// Member<Tag, &Class::member_> instantiation defines a friend get(Tag) that
+// returns the member pointer.
+namespace member_access {
+template <typename Tag, typename Tag::type Ptr> struct Member {
+    friend typename Tag::type get(Tag) { return Ptr; }
+};
+struct SimStatistics { using type = Statistics Simulation::*; friend type get(SimStatistics); };
+struct StatsVector { using type = std::vector<double> Statistics::*; };
+struct VelocityMean : StatsVector { friend type get(VelocityMean); };
+struct PressureMean : StatsVector { friend type get(PressureMean); };
+struct VelocitySecond : StatsVector { friend type get(VelocitySecond); };
+struct PressureVelocity : StatsVector { friend type get(PressureVelocity); };
+struct PressureSecond : StatsVector { friend type get(PressureSecond); };
+struct VelocityThird : StatsVector { friend type get(VelocityThird); };
+struct VelocityFourth : StatsVector { friend type get(VelocityFourth); };
+template struct Member<SimStatistics, &Simulation::statistics_>;
+template struct Member<VelocityMean, &Statistics::velocity_mean_>;
+template struct Member<PressureMean, &Statistics::pressure_mean_>;
+template struct Member<VelocitySecond, &Statistics::velocity_second_>;
+template struct Member<PressureVelocity, &Statistics::pressure_velocity_>;
+template struct Member<PressureSecond, &Statistics::pressure_second_>;
+template struct Member<VelocityThird, &Statistics::velocity_third_>;
+template struct Member<VelocityFourth, &Statistics::velocity_fourth_>;
+}  // namespace member_access
+
 namespace {
 template <typename T> void read_all(const std::string &path, std::vector<T> &out) {
     std::ifstream in(path, std::ios::binary);
@@ -120,6 +154,21 @@ int main(int argc, char **argv) {
             write(out, &t, 1);
             write(out, sim.velocity().data(), sim.velocity().size());
             write(out, sim.pressure().data(), sim.pressure().size());
+            if (argc > 5) {
+                namespace ma = member_access;
+                const Statistics &st = sim.*get(ma::SimStatistics{});
+                std::ofstream so(argv[5], std::ios::binary);
+                const std::int64_t count = st.count();
+                const double dp[2] = {st.dpdx_mean(), st.dpdz_mean()};
+                write(so, &count, 1);
+                write(so, dp, 2);
+                for (const auto &v : {st.*get(ma::VelocityMean{}), st.*get(ma::PressureMean{}),
+                                      st.*get(ma::VelocitySecond{}), st.*get(ma::PressureSecond{}),
+                                      st.*get(ma::PressureVelocity{}), st.*get(ma::VelocityThird{}),
+                                      st.*get(ma::VelocityFourth{})})
+                    write(so, v.data(), v.size());
+                if (!so) return 1;
+            }
             return out ? 0 : 1;
         }
         if (mode == "nonlinear" && argc >= 5) {

@@ -28,9 +28,13 @@ on small seeded inputs and stores inputs and outputs as compressed npz files:
   golden_blocks.npz     the reference Mesh's distributed block tables (x block,
                         fine-grid y slab, zero-mode owner) for 1..12 ranks on
                         four meshes, and the splits it rejects.
+  golden_stats.npz      16x17x16 channel (log-law mean plus a k^-5/3
+                        perturbation), 6 steps with Nstat = 2: the final
+                        velocity and pressure and the Statistics running means
+                        of the 4 sampled steps at full precision.
 
 Usage: python tests/golden/make_golden.py [name ...]   (needs oracle/_ref built;
-names: step example nonlinear solve fine coarse reduce files blocks, default all)
+names: step example nonlinear solve fine coarse reduce files blocks stats, default all)
 """
 import os
 import sys
@@ -118,12 +122,26 @@ def block_tables(which):
     np.savez_compressed(os.path.join(HERE, "golden_blocks.npz"), **out)
 
 
+def statistics_run(which):
+    """golden_stats.npz: Simulation::run sampling Statistics at every step
+    after Nstat (src/sim/simulation.cpp:225-250, src/sim/statistics.cpp:117-139)."""
+    if "stats" not in which:
+        return
+    m, p = channel_case(16)
+    u0 = divergence_free_field(m, p, seed=81, amp=0.1, spectrum="k53", mean="loglaw")
+    ru, rp, _, st = ref_io.run_steps(m, p, u0, 6, nstat=2)
+    np.savez_compressed(os.path.join(HERE, "golden_stats.npz"), **mesh_dict(m, p), nsteps=6, nstat=2,
+                        u0=np.stack(u0), u=np.stack(ru), p=rp, count=st["count"],
+                        dp_means=np.array(st["dp_means"]), means=st["means"])
+
+
 def main(which):
     if not ref_io.available():
         raise SystemExit("oracle/_ref is not built: run make -C oracle")
     coarse_and_reduce(which)
     dump_files(which)
     block_tables(which)
+    statistics_run(which)
     if "step" not in which:
         print("golden fixtures written to", HERE)
         return
@@ -178,4 +196,4 @@ def _cheb_1my2(ncy):
 
 if __name__ == "__main__":
     main(set(sys.argv[1:]) or {"step", "example", "nonlinear", "solve", "fine", "coarse", "reduce", "files",
-                               "blocks"})
+                               "blocks", "stats"})

@@ -100,3 +100,38 @@ def test_oracle_output_reduction_matches_reference():
     v = d["values"]
     assert abs(ekt - v[0]) <= 1e-14 * v[0] and abs(tke - v[1]) <= 1e-13 * v[1]
     assert v[2] > 0.1 and abs(div - v[2]) <= 1e-12 * v[2] and v[3] == 1.0
+
+
+def statistics_scale(m, u_list, p):
+    """Per moment, the largest plane magnitude of the sums of absolute values
+    of its terms over the sampled states: the round-off scale of a mean that
+    cancels (the plane mean of v, the means at the no-slip walls)."""
+    vp, pp = orc.to_physical(m, u_list, p)
+    return plane_sum_scale(vp, pp).max(axis=0) / float(m.NX * m.NZ)
+
+
+def test_oracle_statistics_run_matches_reference():
+    """Simulation::run sampling Statistics after Nstat (src/sim/simulation.cpp:225-250,
+    src/sim/statistics.cpp:117-139): the running means of the reference's own
+    run, read at full precision, against the oracle's step loop and
+    Statistics restatement (4 samples after 6 steps of a 16x17x16 channel)."""
+    m, p, d = load("golden_stats.npz")
+    sim = orc.Simulation(m, p, list(d["u0"]))
+    st = orc.Statistics(m)
+    scale = np.zeros(20)
+    with np.errstate(all="ignore"):
+        for it in range(1, int(d["nsteps"]) + 1):
+            sim.step()
+            if it > int(d["nstat"]):
+                vp, pp = orc.to_physical(m, sim.u, sim.pressure)
+                st.accumulate(orc.plane_moments(vp, pp), sim.dpdx, sim.dpdz)
+                scale = np.maximum(scale, statistics_scale(m, sim.u, sim.pressure))
+    for k in range(3):
+        assert orc.rel_l2(sim.u[k], d["u"][k]) <= 1e-12
+    assert st.count == int(d["count"]) == 4
+    assert np.allclose(st.dp, d["dp_means"], rtol=0, atol=1e-14)
+    # The states themselves agree to ~1e-12 (numpy's FFTs against the shim's),
+    # so the means agree to that level of their round-off scale (measured
+    # 2.1e-12 at most, in the pressure-velocity moments).
+    slots = np.array(orc.STAT_SOURCE)   # plane moment behind each mean slot
+    assert np.all(np.abs(st.means - d["means"]) <= 1e-11 * scale[slots][:, None])
