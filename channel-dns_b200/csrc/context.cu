@@ -446,6 +446,19 @@ int cdns_set_velocity(cdns_ctx *c, const double *v) {
     return CDNS_OK;
 }
 
+int cdns_update_velocity(cdns_ctx *c, const double *v) {
+    if (!c || !v) return fail(CDNS_ERR_ARG, "null argument");
+    if (int r = require_whole(c)) return r;
+    if (!c->have_velocity) return fail(CDNS_ERR_STATE, "cdns_update_velocity before cdns_set_velocity");
+    DeviceGuard guard(c->device);
+    CK(cudaMemcpyAsync(c->aux, v, sizeof(double2) * 3 * c->d.Ns, cudaMemcpyHostToDevice, c->stream));
+    // the current slot only: u_prev, N_prev and B_prev of the multistep history stay
+    launch_deinterleave(reinterpret_cast<const double2 *>(c->aux), c->U[c->cur], c->d.Ns, 3, c->stream);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->stream));
+    return CDNS_OK;
+}
+
 int cdns_get_velocity_device(cdns_ctx *c, double *v) {
     if (!c || !v) return fail(CDNS_ERR_ARG, "null argument");
     if (!c->have_velocity) return fail(CDNS_ERR_STATE, "no velocity set");

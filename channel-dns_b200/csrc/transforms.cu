@@ -674,6 +674,189 @@ k_x_cross_r(Dims d, const double2 *__restrict__ roots, const C *__restrict__ G, 
 }
 
 // ---------------------------------------------------------------------------
+// K3, half-warp form for NX2 = N1 x N2 (N1, N2 <= 16).  A half-warp (16
+// lanes) owns a pair of rows (A, B) of the flattened row index R = j NZ2 + z
+// from the spectral gather to the spectral store, so it synchronises with
+// __syncwarp only (the twiddle table is the block's one barrier).  Per row:
+//   three inverse lines (u + i v), (w + i om_x), (om_y + i om_z): lanes n2
+//     gather Z[n2 + N2 n1] and do the N1-point DFT, twiddle, exchange through
+//     the half-warp's scratch, lanes k1 do the N2-point DFT -> the line at
+//     x = k1 + N1 k2 in lane k1's registers; the first two lines are kept
+//     lane-private in shared memory (no exchange: lane k1 reads back what it
+//     wrote) for
+//   the products N = u x omega at the same x points, in registers; then
+//   the forward line (N0 + i N1) of the row: lane a = k1 holds x = a + N1 b,
+//     so the N2-point DFT over b runs on its registers, twiddle, exchange,
+//     lanes q1 do the N1-point DFT -> P[q1 + N2 q2]; Hermitian unpack with
+//     the partner lane (N2 - q1) by shuffle, modes q <= NXS -> HBM.
+// N2 of row A waits lane-private in shared memory; with row B's it forms the
+// third forward line N2(A) + i N2(B).  Rows past the end (an odd row count)
+// are neither read nor written.
+// ---------------------------------------------------------------------------
+constexpr int kXHWarps = 2;   // warps per block of the half-warp form
+__host__ __device__ constexpr int xh_scratch(int n1, int n2) {
+    return n1 * (n2 + 1) > n2 * (n1 + 1) ? n1 * (n2 + 1) : n2 * (n1 + 1);
+}
+// bytes of one half-warp's shared memory: scratch, two stashed lines, N2 of row A
+__host__ __device__ constexpr int xh_bytes(int n1, int n2, int elem) {
+    return elem * (xh_scratch(n1, n2) + 2 * n1 * n2) + (elem / 2) * n1 * n2;
+}
+
+template <int N1, int N2, class C, bool MEAN>
+__global__ void __launch_bounds__(32 * kXHWarps)
+k_x_cross_h(Dims d, const double2 *__restrict__ roots, const C *__restrict__ G, C *__restrict__ H,
+            const double *__restrict__ mean) {
+    using T = typename CReal<C>::T;
+    constexpr int n = N1 * N2;
+    constexpr int NV = N1 > N2 ? N1 : N2;
+    constexpr int SP1 = N2 + 1, SP2 = N1 + 1;   // padded scratch rows (inverse, forward)
+    extern __shared__ double2 sm_d[];
+    const Twiddles<C> tw = load_twiddles<C>(sm_d, roots, n);
+    const int hw = threadIdx.x >> 4, sub = threadIdx.x & 15;
+    char *mine = reinterpret_cast<char *>(sm_d + n) + hw * xh_bytes(N1, N2, (int)sizeof(C));
+    C *S = reinterpret_cast<C *>(mine);                        // exchange scratch
+    C *P = S + xh_scratch(N1, N2);                             // stashed lines [2][N2][N1]
+    T *Q = reinterpret_cast<T *>(P + 2 * n);                   // N2 of row A [N2][N1]
+    const long long rows = (long long)d.ny2 * d.NZ2;
+    const long long rA = 2 * ((long long)blockIdx.x * (2 * kXHWarps) + hw);
+    const int nkx = d.nkx, nxs = d.NXS;
+    const long long fstride = rows * nkx;
+    const int nyq = (n % 2 == 0) ? n / 2 : -1;
+    const int lane = threadIdx.x & 31;
+    const int partner = (lane & 16) + (sub < N2 ? (N2 - sub) % N2 : sub);
+    // FP32: no 1/NX2 here (not exact in FP32); the FP64 y analysis applies 1/(NX2 NZ2)
+    const T invn = (T)(sizeof(C) == 8 ? 1.0 : 1.0 / (double)n);
+    __syncthreads();   // twiddles complete; no block-wide barrier below
+    C v[NV];
+
+    // forward FFT of the line in v (lane a < N1: v[b] = p[a + N1 b]), unpack
+    // of the two real spectra, stores of modes q <= NXS: outA to dstA, outB to dstB
+    auto forward_store = [&](C *dstA, C *dstB, bool okA, bool okB) {
+        if (sub < N1) {
+            C(&w)[N2] = reinterpret_cast<C(&)[N2]>(v);
+            dft_reg<N2, -1>(w, tw, N1);
+#pragma unroll
+            for (int q1 = 0; q1 < N2; ++q1)
+                S[q1 * SP2 + sub] = (q1 == 0 || sub == 0) ? w[q1] : tw.template mul<-1>(w[q1], sub * q1);
+        }
+        __syncwarp();
+        if (sub < N2) {
+#pragma unroll
+            for (int a = 0; a < N1; ++a) v[a] = S[sub * SP2 + a];
+            C(&w)[N1] = reinterpret_cast<C(&)[N1]>(v);
+            dft_reg<N1, -1>(w, tw, N2);
+        }
+#pragma unroll
+        for (int q2 = 0; q2 < N1; ++q2) {
+            C pm;
+            pm.x = __shfl_sync(0xffffffffu, v[N1 - 1 - q2].x, partner);
+            pm.y = __shfl_sync(0xffffffffu, v[N1 - 1 - q2].y, partner);
+            const int q = sub + N2 * q2;
+            if (sub >= N2 || q > nxs) continue;
+            if (sub == 0) pm = v[(N1 - q2) % N1];
+            const C p0 = v[q2];
+            if (okA) dstA[q] = cscale(invn, mkc<C>(T(0.5) * (p0.x + pm.x), T(0.5) * (p0.y - pm.y)));
+            if (okB) dstB[q] = cscale(invn, mkc<C>(T(0.5) * (p0.y + pm.y), T(-0.5) * (p0.x - pm.x)));
+        }
+        __syncwarp();   // scratch free for the next exchange
+    };
+
+#pragma unroll 1
+    for (int rr = 0; rr < 2; ++rr) {
+        const long long row = rA + rr;
+        const bool live = row < rows;
+        // ---- three inverse lines ------------------------------------------
+#pragma unroll 1
+        for (int line = 0; line < 3; ++line) {
+            if (sub < N2) {
+                const C *rowA = G + (2 * line) * fstride + row * nkx;
+                const C *rowB = rowA + fstride;
+#pragma unroll
+                for (int n1 = 0; n1 < N1; ++n1) {
+                    const int m = sub + N2 * n1;
+                    C x = mkc<C>(0.0, 0.0);
+                    if (live) {
+                        if (m <= nxs) {
+                            C A = rowA[m], B = rowB[m];
+                            if (m == 0 || m == nyq) {
+                                A.y = 0.0;
+                                B.y = 0.0;
+                            }
+                            x = mkc<C>(A.x - B.y, A.y + B.x);
+                        } else if (m >= n - nxs && m != nyq) {
+                            const C A = rowA[n - m], B = rowB[n - m];
+                            x = mkc<C>(A.x + B.y, B.x - A.y);
+                        }
+                    }
+                    v[n1] = x;
+                }
+                C(&w)[N1] = reinterpret_cast<C(&)[N1]>(v);
+                dft_reg<N1, +1>(w, tw, N2);
+#pragma unroll
+                for (int k1 = 0; k1 < N1; ++k1)
+                    S[k1 * SP1 + sub] = (k1 == 0 || sub == 0) ? w[k1] : tw.template mul<+1>(w[k1], sub * k1);
+            }
+            __syncwarp();
+            if (sub < N1) {
+#pragma unroll
+                for (int n2 = 0; n2 < N2; ++n2) v[n2] = S[sub * SP1 + n2];
+                C(&w)[N2] = reinterpret_cast<C(&)[N2]>(v);
+                dft_reg<N2, +1>(w, tw, N1);
+                if (line < 2) {
+#pragma unroll
+                    for (int k2 = 0; k2 < N2; ++k2) P[(line * N2 + k2) * N1 + sub] = w[k2];
+                }
+            }
+            __syncwarp();
+        }
+        // ---- products u x omega at x = sub + N1 k2 -------------------------
+        if (sub < N1) {
+            T mu = 0, mv = 0, mw = 0, mox = 0, moy = 0, moz = 0;
+            if constexpr (MEAN) {
+                const int ny2 = d.ny2;
+                const int j = live ? (int)(row / d.NZ2) : 0;
+                mu = (T)mean[j];
+                mv = (T)mean[ny2 + j];
+                mw = (T)mean[2 * ny2 + j];
+                mox = (T)mean[3 * ny2 + j];
+                moy = (T)mean[4 * ny2 + j];
+                moz = (T)mean[5 * ny2 + j];
+            }
+#pragma unroll
+            for (int k2 = 0; k2 < N2; ++k2) {
+                const C p0 = P[k2 * N1 + sub];
+                const C p1 = P[(N2 + k2) * N1 + sub];
+                const T uu = p0.x, vv = p0.y, ww = p1.x, ox = p1.y, oy = v[k2].x, oz = v[k2].y;
+                T n0 = vv * oz - ww * oy;
+                T n1v = ww * ox - uu * oz;
+                T n2v = uu * oy - vv * ox;
+                if constexpr (MEAN) {
+                    // fluctuations about the FP64 mean profiles: + M x om' + u' x M_om
+                    // (M x M_om is added to the mean mode in FP64 after the analysis)
+                    n0 += (mv * oz - mw * oy) + (vv * moz - ww * moy);
+                    n1v += (mw * ox - mu * oz) + (ww * mox - uu * moz);
+                    n2v += (mu * oy - mv * ox) + (uu * moy - vv * mox);
+                }
+                v[k2] = mkc<C>(n0, n1v);
+                if (rr == 0) {
+                    Q[k2 * N1 + sub] = n2v;
+                } else {
+                    P[k2 * N1 + sub] = mkc<C>(Q[k2 * N1 + sub], n2v);   // third line N2(A) + i N2(B)
+                }
+            }
+        }
+        // ---- forward line (N0 + i N1) of this row -------------------------
+        forward_store(H + row * nkx, H + fstride + row * nkx, live, live);
+    }
+    // ---- third forward line N2(A) + i N2(B) -------------------------------
+    if (sub < N1) {
+#pragma unroll
+        for (int b = 0; b < N2; ++b) v[b] = P[b * N1 + sub];
+    }
+    forward_store(H + 2 * fstride + rA * nkx, H + 2 * fstride + (rA + 1) * nkx, rA < rows, rA + 1 < rows);
+}
+
+// ---------------------------------------------------------------------------
 // Transpose of K3 in the register form (NX2 = N1 x N2, FP64): k_x_adjoint's
 // algebra with the layout of k_x_cross_r.  16 lanes per line, RW rows per
 // block; five inverse lines per row, (u, v), (w, om_x), (om_y, om_z),
@@ -1261,6 +1444,9 @@ size_t smem_xadjoint_r(int n1, int n2) {
     const size_t s1 = L * n1 * (n2 + 1), s2 = L * n1 * n2;
     return sizeof(double2) * (n1 * n2 + (s1 > s2 ? s1 : s2));
 }
+size_t smem_xcross_h(int n1, int n2, size_t elem) {
+    return sizeof(double2) * n1 * n2 + (size_t)(2 * kXHWarps) * xh_bytes(n1, n2, (int)elem);
+}
 size_t smem_xcross_r(int n1, int n2, size_t elem) {
     const size_t L = 3 * kRWr;
     const size_t s1 = L * n1 * (n2 + 1), s2 = L * n1 * n2;
@@ -1272,6 +1458,8 @@ template <class C> cudaError_t configure_register_forms(const Dims &d) {
     with_xsplit(d.NX2, [&](auto a, auto b) {
         constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
         e = raise_smem(k_x_cross_r<N1, N2, C, sizeof(C) == 8>, smem_xcross_r(N1, N2, sizeof(C)));
+        if (e == cudaSuccess)
+            e = raise_smem(k_x_cross_h<N1, N2, C, sizeof(C) == 8>, smem_xcross_h(N1, N2, sizeof(C)));
         if (e == cudaSuccess && sizeof(C) == 16) e = raise_smem(k_x_adjoint_r<N1, N2>, smem_xadjoint_r(N1, N2));
         if (e == cudaSuccess && sizeof(C) == 16) e = raise_smem(k_x_moments_r<N1, N2>, smem_xmoments_r(N1, N2));
     });
@@ -1339,6 +1527,15 @@ bool z_backward_r(const Dims &d, const double2 *roots, const C *F, C *G, int nf,
 }
 template <class C, bool MEAN>
 bool x_cross_r(const Dims &d, const double2 *roots, const C *G, C *H, const double *mean, cudaStream_t s) {
+    if (d.xrw == 1) {   // half-warp form: 4 kXHWarps rows per block
+        const long long rows = (long long)d.ny2 * d.NZ2;
+        const int per = 4 * kXHWarps;
+        return with_xsplit(d.NX2, [&](auto a, auto b) {
+            constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
+            k_x_cross_h<N1, N2, C, MEAN><<<(unsigned)((rows + per - 1) / per), 32 * kXHWarps,
+                                           smem_xcross_h(N1, N2, sizeof(C)), s>>>(d, roots, G, H, mean);
+        });
+    }
     const int rw = (d.xrw == 2 || d.xrw == 4) ? d.xrw : kRWr;   // even, at most kRWr
     return with_xsplit(d.NX2, [&](auto a, auto b) {
         constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;

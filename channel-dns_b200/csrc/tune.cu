@@ -6,7 +6,8 @@
 // CUDA events on its stream,
 //   - the kx lines per block of the z transforms (8..17): the z synthesis of
 //     the six nonlinear-term fields plus the z analysis of three, and
-//   - the rows per block (2 or 4) of the register-form x stage,
+//   - the form of the register-form x stage: 2 or 4 rows per block, or a
+//     half-warp per row pair,
 //   - the Chebyshev synthesis (six fields) and analysis (three fields) in the
 //     matrix form (FP64 MMA products) and in the FFT form (DCT-I through one
 //     length-NY2 FFT per column; meshes whose NY2 has a register split),
@@ -94,10 +95,11 @@ int measure(cdns_ctx *c, Choice &out) {
     out.ztl = best_tl;
     Dims d = base;
     d.ztl = best_tl;
-    // x stage: 2 or 4 rows per block (smaller blocks couple fewer warps at each barrier)
+    // x stage: 2 or 4 rows per block (smaller blocks couple fewer warps at each
+    // barrier) or the half-warp form (1: a half-warp per row pair, no block barrier)
     {
         float best_x = 1e30f;
-        for (int rw : {4, 2}) {
+        for (int rw : {4, 2, 1}) {
             Dims dx = d;
             dx.xrw = rw;
             float ms;
@@ -125,6 +127,16 @@ int measure(cdns_ctx *c, Choice &out) {
     return CDNS_OK;
 }
 
+// CDNS_X_STAGE=rows4|rows2|halfwarp fixes the form of the register-form x
+// stage (comparisons, tests); FP32 contexts honour it too.
+void apply_x_stage_env(cdns_ctx *c) {
+    if (const char *e = std::getenv("CDNS_X_STAGE")) {
+        if (std::strcmp(e, "rows4") == 0) c->d.xrw = 4;
+        else if (std::strcmp(e, "rows2") == 0) c->d.xrw = 2;
+        else if (std::strcmp(e, "halfwarp") == 0) c->d.xrw = 1;
+    }
+}
+
 void apply(cdns_ctx *c, const Choice &ch) {
     c->d.ztl = ch.ztl;
     c->d.xrw = ch.xrw;
@@ -134,6 +146,7 @@ void apply(cdns_ctx *c, const Choice &ch) {
         if (std::strcmp(e, "matrix") == 0) c->t.yform = 0;
         else if (std::strcmp(e, "fft") == 0) c->t.yform = 3;
     }
+    apply_x_stage_env(c);
 }
 
 }  // namespace
@@ -150,7 +163,10 @@ namespace cdns {
 // exports the cache to it after every new measurement, so that a later run --
 // a profiled one, whose timings would mislead the tuner -- reuses the choices.
 int tune_context(cdns_ctx *c, bool force) {
-    if (c->mixed) return CDNS_OK;   // FP32 stage buffers keep the rule-based shapes
+    if (c->mixed) {   // FP32 stage buffers keep the rule-based shapes
+        apply_x_stage_env(c);
+        return CDNS_OK;
+    }
     if (c->pen) {
         // a pencil rank holds part of the mesh: timing it would file its
         // shapes under the whole mesh's key, so it keeps the rule-based ones
@@ -271,7 +287,7 @@ int cdns_wisdom_import(const char *path) {
                             &ch.yform, &ch.xrw);
         if (n == 2) ch.xrw = 0;   // entries written before the x-stage choice existed
         if (n < 2 || ch.ztl < 0 || ch.ztl > 17 || (ch.ztl != 0 && ch.ztl < 8) || ch.yform < 0 || ch.yform > 3 ||
-            (ch.xrw != 0 && ch.xrw != 2 && ch.xrw != 4))
+            (ch.xrw != 0 && ch.xrw != 1 && ch.xrw != 2 && ch.xrw != 4))
             return fail(CDNS_ERR_ARG, "malformed wisdom entry");
         got[key] = ch;
         pos = end;

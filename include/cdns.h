@@ -100,6 +100,13 @@ int cdns_get_pressure(cdns_ctx *ctx, double *pressure);
 int cdns_set_pressure(cdns_ctx *ctx, const double *pressure);
 int cdns_set_velocity_bc(cdns_ctx *ctx, const double *bc);
 int cdns_set_velocity_device(cdns_ctx *ctx, const double *velocity_dev);
+/* Replace the current velocity and keep the multistep history (the previous
+ * velocity, nonlinear term and pressure wall data), as the reference's
+ * disturbance injection changes velocity_ between two steps of a run
+ * (Simulation::apply_disturbance, src/sim/simulation.cpp:96-106, called from
+ * Simulation::run :255-256); the next step stays second order.  Whole-channel
+ * contexts that already hold a velocity. */
+int cdns_update_velocity(cdns_ctx *ctx, const double *velocity);
 int cdns_get_velocity_device(cdns_ctx *ctx, double *velocity_dev);
 
 /* One time step of Simulation::run (src/sim/simulation.cpp:174-185,

@@ -25,7 +25,7 @@ def available() -> bool:
     return os.access(RUNNER, os.X_OK)
 
 
-def build(ref_root: str = "/root/reference") -> bool:
+def build(ref_root: str) -> bool:
     """Compile the reference sources with the shims (needs the reference tree)."""
     if not os.path.isdir(os.path.join(ref_root, "src")):
         return available()
