@@ -1,19 +1,18 @@
 """Python host side of the B200 channel-dns time step (ctypes over the C ABI).
 
 The product is ``libcdns_cuda.so`` (``include/cdns.h``); this module mirrors
-the reference driver's view of the hot path -- Params/Mesh from a run
-directory's ``config.toml`` (src/core/params.cpp:130-228), a context that
-owns the device state, ``step``/``run`` of Simulation::run
-(src/sim/simulation.cpp:173-185) and the state hand-over in the reference's
-spectral layout.  There is no CPU fallback: every call goes to the CUDA
+the reference driver's view of the hot path -- the Mesh and Params values the
+driver hands over (src/core/params.hpp:6-35; reading config.toml stays the
+driver's), a context that owns the device state, ``step``/``run`` of
+Simulation::run (src/sim/simulation.cpp:173-185) and the state hand-over in
+the reference's spectral layout.  There is no CPU fallback: every call goes to the CUDA
 library, and importing without the built library raises.
 """
 from __future__ import annotations
 
 import ctypes
-import math
 import os
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 from typing import Optional, Sequence, Tuple
 
 import numpy as np
@@ -119,6 +118,7 @@ _SIGNATURES = {
     "cdns_pencil_set_peers": [ctypes.c_void_p, ctypes.c_void_p],
     "cdns_pencil_ipc_handle": [ctypes.c_void_p, ctypes.c_void_p],
     "cdns_pencil_open_peer": [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)],
+    "cdns_pencil_close_peers": [ctypes.c_void_p],
 }
 
 
@@ -193,92 +193,6 @@ class Params:
         return ParamsDesc(self.Re, self.G_pre, self.a_pre0, self.b_pre0, (ctypes.c_double * 3)(*self.a_V),
                           (ctypes.c_double * 3)(*self.b_V), self.INDEX_GRAD_PRE, self.THETA, self.DT,
                           self.V_Microblow0)
-
-
-# Keys of config.toml per table (src/core/params.cpp:130-228); the integer ones.
-_CONFIG_KEYS = {
-    "mesh": ("NX", "NY", "NZ", "INDEX_disturb_Z", "NXS", "NYS", "NZS", "NX2", "NY2", "NZ2", "INDEX_Serial"),
-    "parm": ("INDEX_GRAD_PRE", "INDEX_UNSTEADY_BC", "XL", "ZL", "THETA", "Re", "G_pre", "a_pre0", "b_pre0",
-             "a_V", "b_V"),
-    "control": ("INDEX_CONT", "NSTEPS", "NDUMFRQ", "NPRNFRQ", "NCOUNT_disturb", "NDISTURBFRQ", "Nstat",
-                "EPS_init", "DT", "EPS_disturb", "V_Microblow0"),
-    "output": ("format", "physical_interval", "statistics_interval"),
-}
-_CONFIG_INTS = set(_CONFIG_KEYS["mesh"]) | {"INDEX_GRAD_PRE", "INDEX_UNSTEADY_BC", "INDEX_CONT", "NSTEPS", "NDUMFRQ",
-                                            "NPRNFRQ", "NCOUNT_disturb", "NDISTURBFRQ", "Nstat"}
-
-
-def load_config(run_dir: str) -> Tuple[Mesh, Params, dict]:
-    """Read ``<run_dir>/config.toml`` as Params::load does
-    (src/core/params.cpp:130-228): case-insensitive keys, the tables [mesh],
-    [parm], [control] and an optional [output]; an unknown table or key, a
-    missing key, a non-integer where an integer is required, a non-finite
-    number or an a_V / b_V that is not three numbers raises ValueError.
-    Returns (mesh, params, control); control holds the [control] values
-    (lower-case keys), plus "index_serial" (0: run the channel as pencil
-    ranks, cdns.pencil) and "output_format"."""
-    import tomllib
-    with open(os.path.join(run_dir, "config.toml"), "rb") as fh:
-        raw = tomllib.load(fh)
-    t = {}
-    for name, table in raw.items():
-        if name.lower() not in _CONFIG_KEYS:
-            raise ValueError(f"unknown TOML table: {name}")
-        t[name.lower()] = {k.lower(): v for k, v in table.items()} if isinstance(table, dict) else table
-    for name in ("mesh", "parm", "control", "output"):
-        if name not in t:
-            if name == "output":
-                continue
-            raise ValueError(f"missing TOML table: {name}")
-        known = {k.lower() for k in _CONFIG_KEYS[name]}
-        for key in t[name]:
-            if key not in known:
-                raise ValueError(f"unknown TOML key: {name}.{key}")
-
-    def get(name, key):
-        v = t[name].get(key.lower())
-        if key in _CONFIG_INTS:
-            if not isinstance(v, int) or isinstance(v, bool) or not -2 ** 31 <= v < 2 ** 31:
-                raise ValueError(f"integer required: {name}.{key}")
-            return v
-        if isinstance(v, bool) or not isinstance(v, (int, float)) or not math.isfinite(v):
-            raise ValueError(f"finite number required: {name}.{key}")
-        return float(v)
-
-    def triple(key):
-        a = t["parm"].get(key.lower())
-        if not isinstance(a, list) or len(a) != 3:
-            raise ValueError(f"parm.{key} requires three numbers")
-        if any(isinstance(v, bool) or not isinstance(v, (int, float)) or not math.isfinite(v) for v in a):
-            raise ValueError(f"invalid parm.{key} element")
-        return tuple(float(v) for v in a)
-
-    me = {k: get("mesh", k) for k in _CONFIG_KEYS["mesh"]}
-    pa = {k: get("parm", k) for k in _CONFIG_KEYS["parm"] if k not in ("a_V", "b_V")}
-    co = {k.lower(): get("control", k) for k in _CONFIG_KEYS["control"]}
-    fmt = "ascii"
-    if "output" in t:
-        out = t["output"]
-        fmt = out.get("format")
-        if not isinstance(fmt, str):
-            raise ValueError("output.format requires a string")
-        fmt = fmt.lower()
-        if fmt not in ("ascii", "binary", "both"):
-            raise ValueError("output.format must be ascii, binary, or both")
-        for key, low in (("physical_interval", 0), ("statistics_interval", 1)):
-            if key in out:
-                v = out[key]
-                if not isinstance(v, int) or isinstance(v, bool) or v < low:
-                    raise ValueError(f"output.{key} must be {'non-negative' if low == 0 else 'positive'}")
-                co[key] = v
-    co["index_serial"] = me["INDEX_Serial"]
-    co["output_format"] = fmt
-    mesh = Mesh(me["NX"], me["NY"], me["NZ"], me["NXS"], me["NYS"], me["NZS"], me["NX2"], me["NY2"], me["NZ2"],
-                pa["XL"], pa["ZL"])
-    params = Params(Re=pa["Re"], DT=co["dt"], G_pre=pa["G_pre"], a_pre0=pa["a_pre0"], b_pre0=pa["b_pre0"],
-                    a_V=triple("a_V"), b_V=triple("b_V"), INDEX_GRAD_PRE=pa["INDEX_GRAD_PRE"],
-                    THETA=pa["THETA"], V_Microblow0=co["v_microblow0"])
-    return mesh, params, co
 
 
 def step_coefficients(iteration: int, dt: float, reynolds: float):

@@ -131,6 +131,11 @@ class PencilRank(Context):
         _check(lib().cdns_pencil_open_peer(self._h, ctypes.cast(buf, ctypes.c_void_p), ctypes.byref(p)))
         return int(p.value)
 
+    def close_peers(self) -> None:
+        """Unmap the peers' column buffers this process opened (every rank,
+        then a barrier, before any rank closes its context)."""
+        _check(lib().cdns_pencil_close_peers(self._h))
+
     def torch_stream(self):
         import torch
         return torch.cuda.ExternalStream(self.stream_ptr(), device=f"cuda:{self.device}")
@@ -187,6 +192,16 @@ def map_peers(rank, group=None) -> List[int]:
     cols = [rank.columns() if q == rank.rank else rank.open_peer(handles[q]) for q in range(world)]
     rank.set_peers(cols)
     return cols
+
+
+def unmap_peers(rank, group=None) -> None:
+    """End the fused exchange of a multi-process decomposition: every rank
+    unmaps the peers' buffers, then all meet at a barrier, so that no rank
+    frees its column buffer while another still maps it.  Call it on every
+    rank before closing the rank contexts.  Uses `rank.close_peers()`."""
+    import torch.distributed as dist
+    rank.close_peers()
+    dist.barrier(group=group)
 
 
 def step_fused(rank, iteration: int, group=None) -> None:

@@ -26,6 +26,18 @@ __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 std::atomic<unsigned char *> g_scratch_addr[kMaxDevices];
+// The mesh whose tables the array of each device holds and for which the
+// kernels' shared-memory limits were raised (guarded by g_setup_mutex).
+struct TableMesh {
+    bool valid = false;
+    cdns_mesh_desc mesh{};
+};
+TableMesh g_table_mesh[kMaxDevices];
+
+bool same_mesh(const cdns_mesh_desc &a, const cdns_mesh_desc &b) {
+    return a.NX == b.NX && a.NY == b.NY && a.NZ == b.NZ && a.NXS == b.NXS && a.NYS == b.NYS && a.NZS == b.NZS &&
+           a.NX2 == b.NX2 && a.NY2 == b.NY2 && a.NZ2 == b.NZ2 && a.XL == b.XL && a.ZL == b.ZL;
+}
 
 size_t align256(size_t b) { return (b + 255) / 256 * 256; }
 
@@ -114,7 +126,9 @@ extern "C" int cdns_transform_fine_backward_noalloc(const cdns_mesh_desc *m, con
     FftPlan px{}, pz{};
     if (!factor(d.NX2, px) || !factor(d.NZ2, pz))
         return record_error(CDNS_ERR_ARG, "NX2/NZ2 must factor into primes <= 13");
-    if ((size_t)16 * d.NZ2 * 33 > 220 * 1024 || (size_t)16 * d.NX2 * 9 > 220 * 1024)
+    // the limits cdns_create applies: configure_transform_kernels raises the
+    // shared memory of every transform kernel for this mesh
+    if ((size_t)16 * d.NZ2 * 35 > 220 * 1024 || (size_t)16 * d.NX2 * 25 > 220 * 1024)
         return record_error(CDNS_ERR_ARG, "mesh exceeds the shared-memory tiling limits");
     // scratch layout: tables, then the two stage buffers
     const size_t b_wavx = align256(sizeof(double) * d.nkx);
@@ -138,8 +152,23 @@ extern "C" int cdns_transform_fine_backward_noalloc(const cdns_mesh_desc *m, con
     unsigned char *base = nullptr;
     int r = scratch_on_current_device(&base);
     if (r) return r;
-    cudaError_t e = configure_transform_kernels(d);
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return record_error(CDNS_ERR_CUDA, cudaGetErrorString(e));
+    // tables and kernel limits once per device and mesh: a call with the mesh
+    // of the previous call on this device only launches the transform
+    bool fresh;
+    {
+        std::lock_guard<std::mutex> lock(g_setup_mutex);
+        fresh = !g_table_mesh[dev].valid || !same_mesh(g_table_mesh[dev].mesh, *m);
+        if (fresh) {
+            g_table_mesh[dev].valid = false;
+            e = configure_transform_kernels(d);
+            if (e != cudaSuccess) return record_error(CDNS_ERR_CUDA, cudaGetErrorString(e));
+            g_table_mesh[dev].mesh = *m;
+            g_table_mesh[dev].valid = true;
+        }
+    }
     unsigned char *p = base;
     double *wavx = reinterpret_cast<double *>(p); p += b_wavx;
     double *wavz = reinterpret_cast<double *>(p); p += b_wavz;
@@ -152,9 +181,17 @@ extern "C" int cdns_transform_fine_backward_noalloc(const cdns_mesh_desc *m, con
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const double pi = std::acos(-1.0);
     const int nt = std::max(std::max(d.nkx, d.nkz), std::max(2 * d.NY2, std::max(d.NX2, d.NZ2)));
-    k_noalloc_tables<<<(nt + 127) / 128, 128, 0, s>>>(d, 2.0 * pi / m->XL, 2.0 * pi / m->ZL, wavx,
-                                                       wavz, cosy, root_x, root_z);
-    launch_cheb_tables(d, cosy, csyn, nullptr, s);
+    if (fresh) {
+        k_noalloc_tables<<<(nt + 127) / 128, 128, 0, s>>>(d, 2.0 * pi / m->XL, 2.0 * pi / m->ZL, wavx,
+                                                           wavz, cosy, root_x, root_z);
+        launch_cheb_tables(d, cosy, csyn, nullptr, s);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            std::lock_guard<std::mutex> lock(g_setup_mutex);
+            g_table_mesh[dev].valid = false;
+            return record_error(CDNS_ERR_CUDA, cudaGetErrorString(e));
+        }
+    }
     Tables t{};
     t.csyn = csyn;
     t.wavx = wavx;

@@ -285,6 +285,18 @@ int cdns_pencil_ipc_handle(cdns_ctx *c, void *handle) {
     return CDNS_OK;
 }
 
+int cdns_pencil_close_peers(cdns_ctx *c) {
+    if (!c) return fail(CDNS_ERR_ARG, "null context");
+    if (!c->pen) return fail(CDNS_ERR_STATE, "not a pencil rank context");
+    if (c->pen->next_stage != 0) return fail(CDNS_ERR_STATE, "cdns_pencil_close_peers inside a step");
+    DeviceGuard guard(c->device);
+    CK(cudaStreamSynchronize(c->stream));   // no stage of this rank still reads a peer's buffer
+    c->pen->peers = false;
+    for (void *p : c->pen->opened) CK(cudaIpcCloseMemHandle(p));
+    c->pen->opened.clear();
+    return CDNS_OK;
+}
+
 int cdns_pencil_open_peer(cdns_ctx *c, const void *handle, void **ptr) {
     if (!c || !handle || !ptr) return fail(CDNS_ERR_ARG, "null argument");
     if (!c->pen) return fail(CDNS_ERR_STATE, "not a pencil rank context");
@@ -295,6 +307,45 @@ int cdns_pencil_open_peer(cdns_ctx *c, const void *handle, void **ptr) {
     CK(cudaIpcOpenMemHandle(&p, h, cudaIpcMemLazyEnablePeerAccess));
     c->pen->opened.push_back(p);
     *ptr = p;
+    return CDNS_OK;
+}
+
+// A peer's column buffer must be device memory that this context's device
+// can reach (its own, or a peer device with access enabled here, which this
+// call enables), and it must hold `bytes` from `p` on (checked with the
+// driver's address-range query where the driver offers it).  Anything else
+// is refused before a kernel could fault on it.
+static int check_peer_columns(cdns_ctx *c, const void *p, unsigned long long bytes) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess || a.type != cudaMemoryTypeDevice) {
+        cudaGetLastError();
+        return fail(CDNS_ERR_ARG, "peer column buffer is not device memory");
+    }
+    if (a.device != c->device) {
+        int can = 0;
+        CK(cudaDeviceCanAccessPeer(&can, c->device, a.device));
+        if (!can) return fail(CDNS_ERR_ARG, "peer column buffer is on a device this device cannot access");
+        const cudaError_t e = cudaDeviceEnablePeerAccess(a.device, 0);
+        if (e == cudaErrorPeerAccessAlreadyEnabled) cudaGetLastError();
+        else if (e != cudaSuccess) return fail(CDNS_ERR_CUDA, cudaGetErrorString(e));
+    }
+    using RangeFn = int (*)(unsigned long long *, size_t *, unsigned long long);
+    static RangeFn range = [] {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            fn = nullptr;
+        cudaGetLastError();
+        return reinterpret_cast<RangeFn>(fn);
+    }();
+    if (range) {
+        unsigned long long base = 0;
+        size_t size = 0;
+        if (range(&base, &size, reinterpret_cast<unsigned long long>(p)) == 0 &&
+            reinterpret_cast<unsigned long long>(p) + bytes > base + size)
+            return fail(CDNS_ERR_ARG, "peer column buffer is smaller than the rank's columns");
+    }
     return CDNS_OK;
 }
 
@@ -313,15 +364,17 @@ int cdns_pencil_set_peers(cdns_ctx *c, void *const *columns) {
     const int nkxg = c->d.NXS + 1;
     std::vector<double2 *> col(nkxg);
     std::vector<int> width(nkxg);
-    for (int q = 0; q < w->ranks; ++q) {
+    for (int q = 0; q < w->ranks; ++q)
         if (!columns[q]) return fail(CDNS_ERR_ARG, "null peer column buffer");
+    if (columns[w->rank] != static_cast<void *>(c->F))
+        return fail(CDNS_ERR_ARG, "this rank's entry must be its own column buffer");
+    for (int q = 0; q < w->ranks; ++q) {
+        if (int r = check_peer_columns(c, columns[q], 16ull * 6 * c->d.ny2 * c->d.nkz * w->nkx[q])) return r;
         for (int k = 0; k < w->nkx[q]; ++k) {
             col[w->kx0[q] + k] = static_cast<double2 *>(columns[q]) + k;
             width[w->kx0[q] + k] = w->nkx[q];
         }
     }
-    if (columns[w->rank] != static_cast<void *>(c->F))
-        return fail(CDNS_ERR_ARG, "this rank's entry must be its own column buffer");
     CK(cudaMemcpyAsync(w->col, col.data(), sizeof(double2 *) * nkxg, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(w->width, width.data(), sizeof(int) * nkxg, cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));

@@ -148,11 +148,17 @@ int cdns_transform_fine(cdns_ctx *ctx, int direction, const double *in, double *
  * stream) and the call returns without waiting.  No context is needed.
  * Intermediate buffers and tables live in one 32 MiB array in device memory
  * that the library holds on every GPU that loads it (product grids up to
- * about 96^3); larger meshes are rejected with CDNS_ERR_ARG.  The first call
- * on each device looks up that array's address, so make it before any
- * stream capture.  All calls share the array: calls that overlap on the GPU
- * (different streams, threads or devices' streams running at once on one
- * device) race and must be serialised by the caller. */
+ * about 96^3); larger meshes are rejected with CDNS_ERR_ARG.  The array's
+ * memory is committed when the library's device code is loaded on a device:
+ * at the first call there with lazy module loading (the CUDA default), at
+ * library load with eager loading; calls allocate nothing after that.  The
+ * first call on each device looks up that array's address, and the first
+ * call with a mesh (after a call with another mesh) computes that mesh's
+ * tables into the array and raises the kernels' shared-memory limits; make
+ * such calls before any stream capture.  Later calls with the same mesh only
+ * queue the three transform kernels.  All calls share the array: calls that
+ * overlap on the GPU (different streams, threads or devices' streams running
+ * at once on one device) race and must be serialised by the caller. */
 int cdns_transform_fine_backward_noalloc(const cdns_mesh_desc *mesh, const double *spectral,
                                          double *physical, void *stream);
 
@@ -388,6 +394,12 @@ int cdns_pencil_set_peers(cdns_ctx *ctx, void *const *columns);
 #define CDNS_IPC_HANDLE_BYTES 64
 int cdns_pencil_ipc_handle(cdns_ctx *ctx, void *handle);
 int cdns_pencil_open_peer(cdns_ctx *ctx, const void *handle, void **ptr);
+/* Unmap every peer buffer this context opened and return it to the exchange
+ * buffers (after waiting for its stream).  Across processes, every rank calls
+ * it and then meets the others at a barrier before any rank destroys its
+ * context, so that no rank frees a buffer another rank still maps (the
+ * teardown order the CUDA IPC API asks for; MpiContext has none to mirror). */
+int cdns_pencil_close_peers(cdns_ctx *ctx);
 
 #ifdef __cplusplus
 }

@@ -13,7 +13,7 @@ import pytest
 
 import cdns
 from cdns import pencil
-from oracle_cases import channel_case, divergence_free_field, example_case
+from oracle_cases import channel_case, divergence_free_field, example_case, orc
 from test_gpu_parity import ctx_for
 
 pytestmark = pytest.mark.gpu
@@ -29,6 +29,19 @@ def _desc(m, p):
 
 def rel_max(a, b):
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+_ORACLE = {}
+
+
+def _oracle(case, m, p, u0, nsteps):
+    """The oracle's step loop from the same state (cached per case)."""
+    if case not in _ORACLE:
+        sim = orc.Simulation(m, p, [u0[..., k] for k in range(3)])
+        with np.errstate(all="ignore"):
+            sim.run(nsteps)
+        _ORACLE[case] = sim.u
+    return _ORACLE[case]
 
 
 def _reference(m, p, u0, nsteps):
@@ -47,7 +60,8 @@ def _reference(m, p, u0, nsteps):
                                                  ("channel32", 3, "peer"), ("example", 5, "peer")])
 def test_local_pencil_matches_single_context(case, ranks, exchange, monkeypatch):
     """4 steps (the two setup steps and two steady ones): velocity, pressure
-    and dp/dx of the decomposed step equal the single-context step to 1e-13
+    and dp/dx of the decomposed step equal the single-context step to 1e-13,
+    and the velocity the oracle's step loop to 1e-10
     (32 x 33 x 32 channel at fixed dp/dx, 48^3 product grid; the 32^3 example
     case at constant flow rate, full Nyquist spectrum, ragged blocks), with the
     exchange by packed buffers and with the fused exchange (z transforms on
@@ -71,6 +85,10 @@ def test_local_pencil_matches_single_context(case, ranks, exchange, monkeypatch)
     assert rel_max(u, uref) <= 1e-13
     assert rel_max(pr, pref) <= 1e-13
     assert np.allclose(dp, dref, rtol=1e-13, atol=1e-300)
+    # and against the oracle directly (the time-step tolerance)
+    uo = _oracle(case, m, p, u0, 4)
+    for k in range(3):
+        assert orc.rel_l2(u[..., k], uo[k]) <= 1e-10
 
 
 def test_pencil_rank_refuses_whole_channel_calls_and_misordered_stages():
@@ -97,7 +115,12 @@ def test_pencil_rank_refuses_whole_channel_calls_and_misordered_stages():
     r = pencil.PencilRank(mesh, params, 2, 1)
     try:
         own = r.columns()
-        for bad, what in (([own, 0], "null"), ([0, own], "null"), ([own, own + 16], "own column")):
+        own_bytes = 16 * 6 * (m.NY2 + 1) * (2 * m.NZS + 1) * pencil.layout(mesh, 2)[1][1]
+        host = np.zeros(16)
+        # near the end of the own buffer: a rank-0 block from there overruns the allocation
+        tail = own + own_bytes - 16
+        for bad, what in (([own, 0], "null"), ([0, own], "null"), ([own, own + 16], "own column"),
+                          ([host.ctypes.data, own], "not device memory"), ([tail, own], "smaller")):
             with pytest.raises(cdns.CdnsError, match=what) as e:
                 r.set_peers(bad)
             assert e.value.code == 1
