@@ -104,6 +104,24 @@ template <class K> inline cudaError_t raise_smem(K *kernel, size_t bytes) {
     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
+// Asynchronous global -> shared copies (cp.async, sm_80 and later): 16 bytes
+// cached in L2 only, or 8 bytes; src_bytes below the size fills the rest
+// with zeros (0: zeros only, the source is not read).
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, int src_bytes) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src, int src_bytes) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // Error bits recorded on the device and read by the host after a step.
 enum : unsigned { ERR_NONFINITE = 1u, ERR_PIVOT = 2u };
 

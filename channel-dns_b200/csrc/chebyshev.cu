@@ -28,17 +28,6 @@ constexpr int kSynRows = 16;   // synthesis rows (j) per warp
 constexpr int kAnaRows = 16;   // analysis rows (k of one parity) per warp
 constexpr int kMaxGroups = 8;  // row groups per block (two warps each); more go to grid.z
 
-// 16-byte asynchronous global -> shared copy; src_bytes = 0 writes zeros.
-__device__ __forceinline__ void cp_async16(void *dst, const void *src, int src_bytes) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(src), "r"(src_bytes)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N> __device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
 int syn_groups(const Dims &d) { return (d.nyh + kSynRows - 1) / kSynRows; }
 int ana_groups(const Dims &d) { return ((d.ncy + 1) / 2 + kAnaRows - 1) / kAnaRows; }
 

@@ -79,3 +79,29 @@ def test_batch_reports_member_error():
     batch.run(1, 4)
     with pytest.raises(cdns.CdnsError, match="member 1"):
         batch.synchronize()
+
+
+@pytest.mark.parametrize("n", [32, 48, 64, 96])
+def test_batch_member_against_oracle(n):
+    """One member of each ensemble grid size against the oracle's step loop
+    directly (src/sim/simulation.cpp:142-218): a batch of that member beside a
+    member of another size, 4 steps (the two setup steps and two graph-replayed
+    steady ones), relative L2 <= 1e-10 per velocity component."""
+    from oracle_cases import orc
+    other = 32 if n != 32 else 48
+    members = [(n, 100.0 + n), (other, 160.0)]
+    mp = [mesh_params(a, b) for a, b in members]
+    u0 = fields(members)
+    batch = cdns.Batch([x[2] for x in mp], [x[3] for x in mp])
+    for ctx, u in zip(batch.members, u0):
+        ctx.set_velocity(u)
+    batch.run(1, 4)
+    batch.synchronize()
+    got = batch.members[0].get_velocity()
+    batch.close()
+    m, p = mp[0][0], mp[0][1]
+    sim = orc.Simulation(m, p, [u0[0][..., k] for k in range(3)])
+    with np.errstate(all="ignore"):
+        sim.run(4)
+    for k in range(3):
+        assert orc.rel_l2(got[..., k], sim.u[k]) <= 1e-10

@@ -3,7 +3,10 @@ FP64 curl, Chebyshev accumulation, tau solves, corrections and mean flow.
 Compared against the FP64 path of the same library (itself pinned to the
 reference at 1e-10): the nonlinear term to FP32 round-off, time steps to
 relative L2 <= 1e-6 per velocity component at 48^3, and the Re_tau180 bound
-of the precision form: velocity field relative L2 <= 1e-6 after 1000 steps."""
+of the precision form after 1000 steps: velocity field relative L2 <= 1e-6,
+the errors of the mean profile and Reynolds stresses reported and bounded,
+and the per-component bound as a strict expected failure at the measured
+floor of FP32 FFT arithmetic."""
 import numpy as np
 import pytest
 
@@ -74,24 +77,75 @@ def test_mixed_steps_48():
         assert rel_l2(v32[..., k], v64[..., k]) <= 1e-6
 
 
-def test_mixed_retau180_1000_steps():
-    """The precision form's bound after 1000 Re_tau180 steps: relative L2 of the
-    velocity field <= 1e-6 against the FP64 path, every component's error below
-    1e-6 of the field norm, and a finite, divergence-free field.  (The
-    per-component relative errors of v and w, whose norms are 10-30x smaller
-    than u's, are a few 1e-6: FP32 FFT arithmetic leaves about 5e-7 relative
-    error in each evaluation of u x omega.)"""
+def run_sampled(ctx, u0, nsteps):
+    """nsteps steps from u0 with a statistics sample after every step
+    (Simulation::run with Nstat = 0); returns (velocity, running means)."""
+    ctx.set_velocity(np.stack(u0, axis=-1))
+    ctx.statistics_reset()
+    for it in range(1, nsteps + 1):
+        ctx.step(it)
+        ctx.statistics_sample()
+    ctx.synchronize()
+    return ctx.get_velocity(), ctx.statistics_read()[2]
+
+
+def statistics_errors(means32, means64):
+    """Relative L2 errors over y of the mean profile U and of the Reynolds
+    stresses <u_i u_j> - <u_i><u_j> (uu, vv, ww, uv), from the running means
+    in Statistics::write's order (u v w, p, uu vv ww uv vw wu, ...)."""
+    def stresses(mn):
+        u, v, w = mn[0], mn[1], mn[2]
+        return {"uu": mn[4] - u * u, "vv": mn[5] - v * v, "ww": mn[6] - w * w, "uv": mn[7] - u * v}
+    out = {"U": rel_l2(means32[0], means64[0])}
+    r32, r64 = stresses(means32), stresses(means64)
+    for k in r64:
+        out[k] = rel_l2(r32[k], r64[k])
+    return out
+
+
+@pytest.fixture(scope="module")
+def retau180_1000():
     m, p = retau180_case()
     u0 = divergence_free_field(m, p, seed=1, amp=0.1, spectrum="k53", mean="loglaw")
-    v64 = run(ctx_for(m, p), u0, 1000)
-    v32 = run(mixed_ctx_for(m, p), u0, 1000)
+    v64, s64 = run_sampled(ctx_for(m, p), u0, 1000)
+    v32, s32 = run_sampled(mixed_ctx_for(m, p), u0, 1000)
+    return m, p, v64, s64, v32, s32
+
+
+def test_mixed_retau180_1000_steps(retau180_1000):
+    """The precision form after 1000 Re_tau180 steps against the FP64 path:
+    relative L2 of the whole velocity field <= 1e-6, every component's error
+    below 1e-6 of the field norm, the mean profile and the Reynolds stresses
+    (running means of a statistics sample after every step) within 1e-6
+    relative L2 over y, and a finite, divergence-free field."""
+    m, p, v64, s64, v32, s32 = retau180_1000
     assert rel_l2(v32, v64) <= 1e-6
     norm = np.linalg.norm(v64)
     for k in range(3):
         assert np.linalg.norm(v32[..., k] - v64[..., k]) <= 1e-6 * norm
+    errs = statistics_errors(s32, s64)
+    print("mixed vs fp64 after 1000 steps:", {k: f"{v:.2e}" for k, v in errs.items()},
+          "per component", [f"{rel_l2(v32[..., k], v64[..., k]):.2e}" for k in range(3)])
+    assert all(v <= 1e-6 for v in errs.values())   # measured: U 4.8e-10, stresses 1.7e-8 to 2.1e-7
     cst = orc.make_constants(m, p.Re)
     div = orc.divergence(cst, [v32[..., k] for k in range(3)])
     assert np.abs(div).max() <= 1e-12 * max(1.0, np.abs(v32).max())
+
+
+@pytest.mark.xfail(strict=True, reason="floor of FP32 FFT arithmetic: per-component relative L2 after 1000 "
+                                       "steps measured u 1.3e-7, v 2.7e-6, w 3.8e-6")
+def test_mixed_retau180_1000_steps_per_component(retau180_1000):
+    """The precision form's stated bound taken per velocity component:
+    relative L2 of each of u, v, w <= 1e-6 after 1000 steps.  v and w, whose
+    norms are 10-30x smaller than u's, do not meet it: FP32 FFT arithmetic
+    leaves 3e-7 to 5e-7 relative error in each evaluation of u x omega (in
+    its x and z components), and the difference to the FP64 path grows about
+    linearly with the steps.  Moving the mean-flow terms M x omega' and
+    u' x M_omega of the product into FP64 lowers only the y component's error,
+    so the floor is that of the fluctuation products' FP32 transforms."""
+    _, _, v64, _, v32, _ = retau180_1000
+    for k in range(3):
+        assert rel_l2(v32[..., k], v64[..., k]) <= 1e-6
 
 
 @pytest.mark.parametrize("key", sorted(ODD_RADIX_MESHES))
