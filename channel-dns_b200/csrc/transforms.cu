@@ -10,6 +10,8 @@
 // The Chebyshev (y) synthesis and analysis live in chebyshev.cu; this file
 // holds the Fourier directions (src/fft/transforms.cpp:615-741): the analysis
 // keeps x1/NX2 before the z FFT and x1/NZ2 after it.
+#include <algorithm>
+#include <cstdlib>
 #include <type_traits>
 
 #include "cdns_kernels.cuh"
@@ -265,9 +267,19 @@ k_z_forward_peers(Dims d, const double2 *__restrict__ roots, const double2 *__re
 //   analysis  (ANA = true):  x_j = F_j;  S_0 = Y_0 / N, S_k = 2 Y_k / N
 //             (the scalings 1/(2 NY2) and 1/NY2 with the DCT-I's doubled
 //             interior sum), k <= NYS.
-// Block = one (field, kz) plane x TL kx lines; loads and stores run along kx.
-// Shared memory: twiddles [N], x then the FFT exchange then the outputs
-// [(N+1)][TL], Z [N][TL], Y_1 [TL].  16 threads per line in the scan phases.
+// Block = one (field, kz) plane x TL kx lines (TL a compile-time width), 16 TL
+// threads: thread t owns line l = t mod TL and row group r = t / TL (rows
+// r, r + 16, ...), so that in every phase consecutive threads touch
+// consecutive lines -- coalesced global rows along kx and conflict-free
+// shared rows [n][l].  Phases (barriers between):
+//   load x_n (n = 0..N) and each thread's partial of Y_1's sum over its rows;
+//   Z = DFT_N(y) (fft2_lines; the exchange aliases x, read before its barrier);
+//   even outputs from Z pairs, and each thread's chunk of the odd outputs'
+//   prefix sum (16 consecutive-k chunks per line);
+//   the carry of the earlier chunks (a fixed-order sum of their totals) and
+//   the odd outputs; stores along kx.
+// Shared memory: twiddles [N], x / exchange / outputs [(N+1)][TL], Z [N][TL],
+// partials [16][TL] (Y_1's, then the chunk totals), Y_1 [TL].
 // ---------------------------------------------------------------------------
 struct YdctSrc {
     const double2 *X;
@@ -285,113 +297,100 @@ struct YdctDst {
     __device__ __forceinline__ void operator()(int k, int l, double2 v) const { Z[k * TL + l] = v; }
 };
 
-template <int N1, int N2, bool ANA>
-__global__ void __launch_bounds__(16 * 17)
+constexpr int kYdctRows = 16;   // row groups of the DCT kernel (16 TL threads)
+__host__ __device__ constexpr size_t ydct_slots(int n, int tl) {
+    return (size_t)n + (size_t)(n + 1) * tl + (size_t)n * tl + (size_t)kYdctRows * tl + tl;
+}
+
+template <int N1, int N2, bool ANA, int TL>
+__global__ void __launch_bounds__(16 * TL)
 k_ydct_r(Dims d, const double2 *__restrict__ roots, const double *__restrict__ cosy, const double2 *src0,
-         const double2 *src1, int nsplit, double2 *__restrict__ out, int TL) {
+         const double2 *src1, int nsplit, double2 *__restrict__ out) {
     constexpr int N = N1 * N2;
+    constexpr int R = kYdctRows;
+    constexpr int M = N / 2 - 1;                // odd outputs beyond Y_1: k = 1..M
+    constexpr int CH = (N / 2 + R) / R;         // k = 0..N/2 in R chunks of CH
     extern __shared__ double2 sm_d[];
     double2 *X = sm_d + N;
     double2 *Z = X + (N + 1) * TL;
-    double2 *Y1 = Z + N * TL;
+    double2 *P = Z + N * TL;
+    double2 *Y1 = P + R * TL;
     const int f = blockIdx.z, kzi = blockIdx.y, kx0 = blockIdx.x * TL;
-    const int t = threadIdx.x, nt = blockDim.x;
-    const int nkx = d.nkx, ncy = d.ncy;
+    const int t = threadIdx.x;
+    const int l = t % TL, r = t / TL;
+    const int nkx = d.nkx, ncy = d.ncy, kx = kx0 + l;
+    const bool lok = kx < nkx;
     const Twiddles<double2> tw = load_twiddles<double2>(sm_d, roots, N);
-    // ---- x_n, n = 0..N ------------------------------------------------------
+    // ---- x_n, n = 0..N, and partials of Y_1 = sum_{n=1}^{N-1} x_n cos(pi n / N)
+    double2 y1 = mk(0.0, 0.0);
     if (!ANA) {
         const double2 *S = (f < nsplit ? src0 + (long long)f * d.Ns : src1 + (long long)(f - nsplit) * d.Ns) +
-                           (long long)kzi * ncy * nkx;
-        for (int i = t; i < (N + 1) * TL; i += nt) {
-            const int n = i / TL, l = i - (i / TL) * TL, kx = kx0 + l;
-            double2 v = (n < ncy && kx < nkx) ? S[(long long)n * nkx + kx] : mk(0.0, 0.0);
-            X[i] = n == 0 ? cadd(v, v) : v;
+                           (long long)kzi * ncy * nkx + kx;
+        for (int n = r; n <= N; n += R) {
+            double2 v = (n < ncy && lok) ? S[(long long)n * nkx] : mk(0.0, 0.0);
+            if (n == 0) v = cadd(v, v);
+            X[n * TL + l] = v;
+            if (n >= 1 && n < N) y1 = cadd(y1, cscale(cosy[n], v));
         }
     } else {
-        const double2 *F = src0 + (long long)f * d.ny2 * d.fcol + (long long)kzi * nkx;
-        for (int i = t; i < (N + 1) * TL; i += nt) {
-            const int n = i / TL, l = i - (i / TL) * TL, kx = kx0 + l;
-            X[i] = kx < nkx ? F[(long long)n * d.fcol + kx] : mk(0.0, 0.0);
+        const double2 *F = src0 + (long long)f * d.ny2 * d.fcol + (long long)kzi * nkx + kx;
+        for (int n = r; n <= N; n += R) {
+            const double2 v = lok ? F[(long long)n * d.fcol] : mk(0.0, 0.0);
+            X[n * TL + l] = v;
+            if (n >= 1 && n < N) y1 = cadd(y1, cscale(cosy[n], v));
         }
     }
+    P[r * TL + l] = y1;
     __syncthreads();
-    const int l = t >> 4, sub = t & 15;
-    // ---- Y_1 per line (16 threads) -------------------------------------------
-    {
-        double2 acc = mk(0.0, 0.0);
-        if (l < TL) {
-            for (int n = 1 + sub; n < N; n += 16) acc = cadd(acc, cscale(cosy[n], X[n * TL + l]));
-            if (sub == 0) acc = cadd(acc, cscale(0.5, csub(X[l], X[N * TL + l])));
-        }
+    if (r == 0) {
+        double2 acc = cscale(0.5, csub(X[l], X[N * TL + l]));
 #pragma unroll
-        for (int m = 8; m > 0; m >>= 1) {
-            acc.x += __shfl_xor_sync(0xffffffffu, acc.x, m, 16);
-            acc.y += __shfl_xor_sync(0xffffffffu, acc.y, m, 16);
-        }
-        if (l < TL && sub == 0) Y1[l] = acc;
+        for (int q = 0; q < R; ++q) acc = cadd(acc, P[q * TL + l]);
+        Y1[l] = acc;
     }
     // ---- Z = DFT_N(y) (the exchange buffer aliases X: read before its barrier)
     fft2_lines<N1, N2, -1>(TL, tw, X, YdctSrc{X, cosy, TL, N}, YdctDst{Z, TL});
     __syncthreads();
-    // ---- outputs into X: even from Z pairs, odd by a prefix scan -----------
-    constexpr int M = N / 2 - 1;            // odd outputs beyond Y_1: k = 1..M
-    constexpr int CH = (M + 15) / 16;       // chunk of k per thread
-    if (l < TL) {
-        for (int k = sub; k <= N / 2; k += 16) {
+    // ---- even outputs X_2k = (Z_k + Z_{N-k}) / 2; chunk sums of i (Z_q - Z_{N-q}) / 2
+    double2 part[CH];
+    double2 run = mk(0.0, 0.0);
+#pragma unroll
+    for (int c = 0; c < CH; ++c) {
+        const int k = r * CH + c;
+        if (k <= N / 2) {
             const double2 zk = Z[k * TL + l], zm = Z[((N - k) % N) * TL + l];
             X[(2 * k) * TL + l] = cscale(0.5, cadd(zk, zm));
+            if (k >= 1 && k <= M) {
+                const double2 dz = csub(zk, zm);
+                run = cadd(run, mk(-0.5 * dz.y, 0.5 * dz.x));
+            }
         }
+        part[c] = run;
     }
+    P[r * TL + l] = run;
+    __syncthreads();
+    // ---- odd outputs X_{2k+1} = Y_1 + sum_{q=1..k} i (Z_q - Z_{N-q}) / 2 -------
     {
-        double2 part[CH];
-        double2 run = mk(0.0, 0.0);
+        double2 carry = mk(0.0, 0.0);
+        for (int q = 0; q < r; ++q) carry = cadd(carry, P[q * TL + l]);
+        const double2 y = Y1[l];
+        if (r == 0) X[1 * TL + l] = y;
 #pragma unroll
         for (int c = 0; c < CH; ++c) {
-            const int k = 1 + sub * CH + c;
-            if (l < TL && k <= M) {
-                const double2 dz = csub(Z[k * TL + l], Z[(N - k) * TL + l]);
-                run = cadd(run, mk(-0.5 * dz.y, 0.5 * dz.x));   // i (Z_k - Z_{N-k}) / 2
-            }
-            part[c] = run;
-        }
-        // exclusive scan of the chunk totals over the 16 lanes of the line
-        double2 ex = run;
-#pragma unroll
-        for (int m = 1; m < 16; m <<= 1) {
-            const double ux = __shfl_up_sync(0xffffffffu, ex.x, m, 16);
-            const double uy = __shfl_up_sync(0xffffffffu, ex.y, m, 16);
-            if (sub >= m) {
-                ex.x += ux;
-                ex.y += uy;
-            }
-        }
-        double2 carry = mk(__shfl_up_sync(0xffffffffu, ex.x, 1, 16), __shfl_up_sync(0xffffffffu, ex.y, 1, 16));
-        if (sub == 0) carry = mk(0.0, 0.0);
-        if (l < TL) {
-            const double2 y1 = Y1[l];
-            if (sub == 0) X[1 * TL + l] = y1;
-#pragma unroll
-            for (int c = 0; c < CH; ++c) {
-                const int k = 1 + sub * CH + c;
-                if (k <= M) X[(2 * k + 1) * TL + l] = cadd(y1, cadd(carry, part[c]));
-            }
+            const int k = r * CH + c;
+            if (k >= 1 && k <= M) X[(2 * k + 1) * TL + l] = cadd(y, cadd(carry, part[c]));
         }
     }
     __syncthreads();
     // ---- store along kx ------------------------------------------------------
+    if (!lok) return;
     if (!ANA) {
-        double2 *Fo = out + (long long)f * d.ny2 * d.fcol + (long long)kzi * nkx;
-        for (int i = t; i < (N + 1) * TL; i += nt) {
-            const int j = i / TL, ll = i - (i / TL) * TL, kx = kx0 + ll;
-            if (kx < nkx) Fo[(long long)j * d.fcol + kx] = X[i];
-        }
+        double2 *Fo = out + (long long)f * d.ny2 * d.fcol + (long long)kzi * nkx + kx;
+        for (int j = r; j <= N; j += R) Fo[(long long)j * d.fcol] = X[j * TL + l];
     } else {
-        double2 *So = out + (long long)f * d.Ns + (long long)kzi * ncy * nkx;
+        double2 *So = out + (long long)f * d.Ns + (long long)kzi * ncy * nkx + kx;
         const double s0 = 1.0 / (double)N, sk = 2.0 / (double)N;
-        for (int i = t; i < ncy * TL; i += nt) {
-            const int k = i / TL, ll = i - (i / TL) * TL, kx = kx0 + ll;
-            if (kx < nkx) So[(long long)k * nkx + kx] = cscale(k == 0 ? s0 : sk, X[i]);
-        }
+        for (int k = r; k < ncy; k += R) So[(long long)k * nkx] = cscale(k == 0 ? s0 : sk, X[k * TL + l]);
     }
 }
 
@@ -1394,9 +1393,37 @@ int z_lines(const Dims &d) {
     return best;
 }
 
-size_t smem_ydct(const Dims &d, int n) {
-    return sizeof(double2) * ((size_t)n + (size_t)(2 * n + 2) * z_lines(d));
+// kx lines per block of the DCT kernels: of {8, 11, 13, 16}, the width that
+// keeps the most threads per SM on real lines -- blocks per SM by shared
+// memory (228 KB, 1 KB reserved per block) x 16 TL threads x nkx / (nkx
+// padded to TL) -- the wider one on a tie; CDNS_YDCT_LINES fixes it.
+int ydct_lines(const Dims &d) {
+    const char *e = std::getenv("CDNS_YDCT_LINES");
+    const int forced = e ? std::atoi(e) : 0;
+    if (forced == 8 || forced == 11 || forced == 13 || forced == 16) return forced;
+    int best = 16;
+    double best_useful = -1.0;
+    for (int tl : {16, 13, 11, 8}) {
+        const size_t bytes = sizeof(double2) * ydct_slots(d.NY2, tl) + 1024;
+        const int blocks = (int)std::min<size_t>((228u * 1024u) / bytes, 2048 / (16 * tl));
+        const int padded = ((d.nkx + tl - 1) / tl) * tl;
+        const double useful = (double)blocks * 16 * tl * d.nkx / padded;
+        if (useful > best_useful) {
+            best_useful = useful;
+            best = tl;
+        }
+    }
+    return best;
 }
+template <typename Fn> void with_ydct_lines(int tl, Fn &&fn) {
+    switch (tl) {
+    case 8: fn(std::integral_constant<int, 8>{}); break;
+    case 11: fn(std::integral_constant<int, 11>{}); break;
+    case 13: fn(std::integral_constant<int, 13>{}); break;
+    default: fn(std::integral_constant<int, 16>{}); break;
+    }
+}
+size_t smem_ydct(int n, int tl) { return sizeof(double2) * ydct_slots(n, tl); }
 // Dims with the widest line tile, for raising the kernels' shared-memory limits
 Dims widest_lines(Dims d) {
     d.ztl = kMaxZLines;
@@ -1480,9 +1507,12 @@ cudaError_t configure_ydct(const Dims &d) {
     cudaError_t e = cudaSuccess;
     with_xsplit(d.NY2, [&](auto a, auto b) {
         constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
-        const int sm = (int)smem_ydct(widest_lines(d), N1 * N2);
-        e = raise_smem(k_ydct_r<N1, N2, true>, sm);
-        if (e == cudaSuccess) e = raise_smem(k_ydct_r<N1, N2, false>, sm);
+        with_ydct_lines(ydct_lines(d), [&](auto w) {
+            constexpr int TL = decltype(w)::value;
+            const int sm = (int)smem_ydct(N1 * N2, TL);
+            e = raise_smem(k_ydct_r<N1, N2, true, TL>, sm);
+            if (e == cudaSuccess) e = raise_smem(k_ydct_r<N1, N2, false, TL>, sm);
+        });
     });
     return e;
 }
@@ -1632,15 +1662,18 @@ bool ydct_available(const Dims &d, const Tables &t) {
 bool launch_ydct(const Dims &d, const Tables &t, const double2 *src0, const double2 *src1, int nsplit, int nf,
                  double2 *out, bool ana, cudaStream_t s) {
     if (!ydct_available(d, t)) return false;
-    const int tl = z_lines(d);
+    const int tl = ydct_lines(d);
     dim3 grid((d.nkx + tl - 1) / tl, d.nkz, nf);
     return with_xsplit(d.NY2, [&](auto a, auto b) {
         constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
-        const size_t sm = smem_ydct(d, N1 * N2);
-        if (ana)
-            k_ydct_r<N1, N2, true><<<grid, 16 * tl, sm, s>>>(d, t.root_y, t.cosy, src0, src1, nsplit, out, tl);
-        else
-            k_ydct_r<N1, N2, false><<<grid, 16 * tl, sm, s>>>(d, t.root_y, t.cosy, src0, src1, nsplit, out, tl);
+        with_ydct_lines(tl, [&](auto w) {
+            constexpr int TL = decltype(w)::value;
+            const size_t sm = smem_ydct(N1 * N2, TL);
+            if (ana)
+                k_ydct_r<N1, N2, true, TL><<<grid, 16 * TL, sm, s>>>(d, t.root_y, t.cosy, src0, src1, nsplit, out);
+            else
+                k_ydct_r<N1, N2, false, TL><<<grid, 16 * TL, sm, s>>>(d, t.root_y, t.cosy, src0, src1, nsplit, out);
+        });
     });
 }
 

@@ -22,7 +22,7 @@ def test_tuning_is_valid_and_cached(tmp_path):
     t = a.tuning()
     assert 8 <= t["z_lines"] <= 17
     assert t["y_synthesis"] in ("fft", "matrix") and t["y_analysis"] in ("fft", "matrix")
-    assert t["x_rows"] in (2, 4)
+    assert t["x_rows"] in (1, 2, 4)
     assert ctx_for(m, p).tuning() == t        # the process cache
     path = tmp_path / "wisdom.json"
     cdns.wisdom_export(str(path))
@@ -70,3 +70,27 @@ def test_fft_form_matches_matrix_form(n, monkeypatch):
         c.synchronize()
         out[form] = c.get_velocity()
     assert orc.rel_l2(out["fft"], out["matrix"]) <= 1e-12
+
+
+@pytest.mark.parametrize("lines", [8, 11, 13, 16])
+@pytest.mark.parametrize("ny2", [48, 192])
+def test_fft_form_line_widths(lines, ny2, monkeypatch):
+    """The DCT-I kernels at every compiled kx-line width (CDNS_YDCT_LINES), with
+    NY2 = 48 (6 x 8) and the Re_tau180 y grid NY2 = 192 (12 x 16): fine
+    transforms and the nonlinear term against the oracle."""
+    monkeypatch.setenv("CDNS_Y_TRANSFORM", "fft")
+    monkeypatch.setenv("CDNS_YDCT_LINES", str(lines))
+    nys = 30 if ny2 == 48 else 126
+    m = orc.Mesh(32, nys + 2, 16, 16, nys, 8, 48, ny2, 24, 4 * np.pi, 2 * np.pi)
+    _, p = channel_case(16)
+    c = ctx_for(m, p)
+    assert c.tuning()["y_synthesis"] == "fft"
+    U = band_spectrum(m, 6)
+    phys = c.transform_fine("B", U)
+    assert rel_max(phys, orc.fine_backward(m, U)) <= 1e-12
+    assert rel_max(c.transform_fine("F", phys), orc.fine_forward(m, phys)) <= 1e-12
+    u = divergence_free_field(m, p, seed=8, amp=0.1, spectrum="k53", mean="loglaw")
+    N, _ = c.nonlinear(np.stack(u, axis=-1))
+    Nr, _, _ = orc.nonlinear_term(m, orc.make_constants(m, p.Re), u)
+    for k in range(3):
+        assert rel_max(N[..., k], Nr[k]) <= 1e-12
