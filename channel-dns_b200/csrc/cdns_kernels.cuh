@@ -78,6 +78,13 @@ bool launch_z_forward_peers(const Dims &ds, const double2 *roots, const double2 
 bool ydct_available(const Dims &d, const Tables &t);
 bool launch_ydct(const Dims &d, const Tables &t, const double2 *src0, const double2 *src1, int nsplit, int nf,
                  double2 *out, bool ana, cudaStream_t s);
+// The same for FP32 stage buffers: the synthesis keeps the (kz, kx) = (0, 0)
+// column in FP64 (mean[f][j]) and writes zeros there; the analysis applies
+// the 1 / (NX2 NZ2) the FP32 z and x analyses leave out.
+bool launch_ydct_synthesis_fp32(const Dims &d, const Tables &t, const double2 *src0, const double2 *src1,
+                                int nsplit, int nf, float2 *F, double *mean, cudaStream_t s);
+bool launch_ydct_analysis_fp32(const Dims &d, const Tables &t, const float2 *F, double2 *S, int nf,
+                               cudaStream_t s);
 // Output reduction, x stage on the coarse grid (Dims of the coarse grid):
 // c2r of G[nf] (u, v, w, p and, if nf = 5, div), per-point moments summed per
 // block into partial[NY+1][moment_blocks][22]; phys (may be null) receives u, v, w, p.

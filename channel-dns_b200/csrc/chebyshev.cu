@@ -558,6 +558,7 @@ void launch_ysynth(const Dims &d, const Tables &t, const double2 *src0, const do
 }
 void launch_ysynth(const Dims &d, const Tables &t, const double2 *src0, const double2 *src1, int nsplit,
                    int nf, float2 *F, double *mean, cudaStream_t s) {
+    if ((t.yform & 1) && launch_ydct_synthesis_fp32(d, t, src0, src1, nsplit, nf, F, mean, s)) return;
     ysynth(d, t, src0, src1, nsplit, nf, F, mean, s);
 }
 
@@ -581,6 +582,7 @@ void launch_yanalysis(const Dims &d, const Tables &t, const double2 *F, double2 
     yanalysis(d, t, F, S, nf, s);
 }
 void launch_yanalysis(const Dims &d, const Tables &t, const float2 *F, double2 *S, int nf, cudaStream_t s) {
+    if ((t.yform & 2) && launch_ydct_analysis_fp32(d, t, F, S, nf, s)) return;
     yanalysis(d, t, F, S, nf, s);
 }
 

@@ -302,10 +302,25 @@ __host__ __device__ constexpr size_t ydct_slots(int n, int tl) {
     return (size_t)n + (size_t)(n + 1) * tl + (size_t)n * tl + (size_t)kYdctRows * tl + tl;
 }
 
-template <int N1, int N2, bool ANA, int TL>
+// Operands of the DCT kernels; CT is the stage buffer's complex type (double2,
+// or float2 for the mixed form's FP32 stages).  Synthesis: spectral
+// spec0 / spec1 (fields f < nsplit / the rest) -> F; with `mean` (FP32 stages)
+// the (kz, kx) = (0, 0) column goes to mean[f][j] in FP64 and zeros to F.
+// Analysis: F -> spectral S, scaled by an extra sxz (1 / (NX2 NZ2) for FP32
+// stages, whose z and x analyses leave it out).
+template <class CT> struct YdctArgs {
+    const double2 *spec0, *spec1;
+    int nsplit;
+    const CT *Fin;
+    CT *Fout;
+    double2 *S;
+    double *mean;
+    double sxz;
+};
+
+template <int N1, int N2, bool ANA, int TL, class CT>
 __global__ void __launch_bounds__(16 * TL)
-k_ydct_r(Dims d, const double2 *__restrict__ roots, const double *__restrict__ cosy, const double2 *src0,
-         const double2 *src1, int nsplit, double2 *__restrict__ out) {
+k_ydct_r(Dims d, const double2 *__restrict__ roots, const double *__restrict__ cosy, YdctArgs<CT> A) {
     constexpr int N = N1 * N2;
     constexpr int R = kYdctRows;
     constexpr int M = N / 2 - 1;                // odd outputs beyond Y_1: k = 1..M
@@ -324,7 +339,7 @@ k_ydct_r(Dims d, const double2 *__restrict__ roots, const double *__restrict__ c
     // ---- x_n, n = 0..N, and partials of Y_1 = sum_{n=1}^{N-1} x_n cos(pi n / N)
     double2 y1 = mk(0.0, 0.0);
     if (!ANA) {
-        const double2 *S = (f < nsplit ? src0 + (long long)f * d.Ns : src1 + (long long)(f - nsplit) * d.Ns) +
+        const double2 *S = (f < A.nsplit ? A.spec0 + (long long)f * d.Ns : A.spec1 + (long long)(f - A.nsplit) * d.Ns) +
                            (long long)kzi * ncy * nkx + kx;
         for (int n = r; n <= N; n += R) {
             double2 v = (n < ncy && lok) ? S[(long long)n * nkx] : mk(0.0, 0.0);
@@ -333,9 +348,9 @@ k_ydct_r(Dims d, const double2 *__restrict__ roots, const double *__restrict__ c
             if (n >= 1 && n < N) y1 = cadd(y1, cscale(cosy[n], v));
         }
     } else {
-        const double2 *F = src0 + (long long)f * d.ny2 * d.fcol + (long long)kzi * nkx + kx;
+        const CT *F = A.Fin + (long long)f * d.ny2 * d.fcol + (long long)kzi * nkx + kx;
         for (int n = r; n <= N; n += R) {
-            const double2 v = lok ? F[(long long)n * d.fcol] : mk(0.0, 0.0);
+            const double2 v = lok ? cto<double2>(F[(long long)n * d.fcol]) : mk(0.0, 0.0);
             X[n * TL + l] = v;
             if (n >= 1 && n < N) y1 = cadd(y1, cscale(cosy[n], v));
         }
@@ -385,11 +400,20 @@ k_ydct_r(Dims d, const double2 *__restrict__ roots, const double *__restrict__ c
     // ---- store along kx ------------------------------------------------------
     if (!lok) return;
     if (!ANA) {
-        double2 *Fo = out + (long long)f * d.ny2 * d.fcol + (long long)kzi * nkx + kx;
-        for (int j = r; j <= N; j += R) Fo[(long long)j * d.fcol] = X[j * TL + l];
+        CT *Fo = A.Fout + (long long)f * d.ny2 * d.fcol + (long long)kzi * nkx + kx;
+        if (A.mean && kzi == d.NZS && kx == 0) {
+            // mean profile (kz, kx) = (0, 0): kept in FP64, out of the FP32 stages
+            // (its imaginary part is round-off of a real profile)
+            for (int j = r; j <= N; j += R) {
+                A.mean[f * d.ny2 + j] = X[j * TL + l].x;
+                Fo[(long long)j * d.fcol] = mkc<CT>(0.0, 0.0);
+            }
+        } else {
+            for (int j = r; j <= N; j += R) Fo[(long long)j * d.fcol] = cto<CT>(X[j * TL + l]);
+        }
     } else {
-        double2 *So = out + (long long)f * d.Ns + (long long)kzi * ncy * nkx + kx;
-        const double s0 = 1.0 / (double)N, sk = 2.0 / (double)N;
+        double2 *So = A.S + (long long)f * d.Ns + (long long)kzi * ncy * nkx + kx;
+        const double s0 = A.sxz / (double)N, sk = 2.0 * A.sxz / (double)N;
         for (int k = r; k < ncy; k += R) So[(long long)k * nkx] = cscale(k == 0 ? s0 : sk, X[k * TL + l]);
     }
 }
@@ -1510,8 +1534,10 @@ cudaError_t configure_ydct(const Dims &d) {
         with_ydct_lines(ydct_lines(d), [&](auto w) {
             constexpr int TL = decltype(w)::value;
             const int sm = (int)smem_ydct(N1 * N2, TL);
-            e = raise_smem(k_ydct_r<N1, N2, true, TL>, sm);
-            if (e == cudaSuccess) e = raise_smem(k_ydct_r<N1, N2, false, TL>, sm);
+            e = raise_smem(k_ydct_r<N1, N2, true, TL, double2>, sm);
+            if (e == cudaSuccess) e = raise_smem(k_ydct_r<N1, N2, false, TL, double2>, sm);
+            if (e == cudaSuccess) e = raise_smem(k_ydct_r<N1, N2, true, TL, float2>, sm);
+            if (e == cudaSuccess) e = raise_smem(k_ydct_r<N1, N2, false, TL, float2>, sm);
         });
     });
     return e;
@@ -1659,8 +1685,8 @@ bool ydct_available(const Dims &d, const Tables &t) {
     return t.root_y && d.NY2 % 2 == 0 && with_xsplit(d.NY2, [](auto, auto) {});
 }
 
-bool launch_ydct(const Dims &d, const Tables &t, const double2 *src0, const double2 *src1, int nsplit, int nf,
-                 double2 *out, bool ana, cudaStream_t s) {
+template <class CT>
+bool ydct(const Dims &d, const Tables &t, int nf, bool ana, const YdctArgs<CT> &A, cudaStream_t s) {
     if (!ydct_available(d, t)) return false;
     const int tl = ydct_lines(d);
     dim3 grid((d.nkx + tl - 1) / tl, d.nkz, nf);
@@ -1670,11 +1696,44 @@ bool launch_ydct(const Dims &d, const Tables &t, const double2 *src0, const doub
             constexpr int TL = decltype(w)::value;
             const size_t sm = smem_ydct(N1 * N2, TL);
             if (ana)
-                k_ydct_r<N1, N2, true, TL><<<grid, 16 * TL, sm, s>>>(d, t.root_y, t.cosy, src0, src1, nsplit, out);
+                k_ydct_r<N1, N2, true, TL, CT><<<grid, 16 * TL, sm, s>>>(d, t.root_y, t.cosy, A);
             else
-                k_ydct_r<N1, N2, false, TL><<<grid, 16 * TL, sm, s>>>(d, t.root_y, t.cosy, src0, src1, nsplit, out);
+                k_ydct_r<N1, N2, false, TL, CT><<<grid, 16 * TL, sm, s>>>(d, t.root_y, t.cosy, A);
         });
     });
+}
+bool launch_ydct(const Dims &d, const Tables &t, const double2 *src0, const double2 *src1, int nsplit, int nf,
+                 double2 *out, bool ana, cudaStream_t s) {
+    YdctArgs<double2> A{};
+    if (ana) {
+        A.Fin = src0;
+        A.S = out;
+    } else {
+        A.spec0 = src0;
+        A.spec1 = src1;
+        A.nsplit = nsplit;
+        A.Fout = out;
+    }
+    A.sxz = 1.0;
+    return ydct(d, t, nf, ana, A, s);
+}
+bool launch_ydct_synthesis_fp32(const Dims &d, const Tables &t, const double2 *src0, const double2 *src1,
+                                int nsplit, int nf, float2 *F, double *mean, cudaStream_t s) {
+    YdctArgs<float2> A{};
+    A.spec0 = src0;
+    A.spec1 = src1;
+    A.nsplit = nsplit;
+    A.Fout = F;
+    A.mean = mean;
+    return ydct(d, t, nf, false, A, s);
+}
+bool launch_ydct_analysis_fp32(const Dims &d, const Tables &t, const float2 *F, double2 *S, int nf,
+                               cudaStream_t s) {
+    YdctArgs<float2> A{};
+    A.Fin = F;
+    A.S = S;
+    A.sxz = 1.0 / ((double)d.NX2 * (double)d.NZ2);
+    return ydct(d, t, nf, true, A, s);
 }
 
 int moment_blocks(const Dims &d) { return (d.NZ2 + kRWm - 1) / kRWm; }

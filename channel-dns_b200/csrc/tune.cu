@@ -3,7 +3,8 @@
 // src/fft/wisdom.cpp:11-32).
 //
 // For each mesh, the first FP64 context times on its own device buffers, with
-// CUDA events on its stream,
+// CUDA events on its stream (a mixed-precision context times only the two
+// Chebyshev forms, on its FP32 buffers, under a key of its own),
 //   - the kx lines per block of the z transforms (8..17): the z synthesis of
 //     the six nonlinear-term fields plus the z analysis of three, and
 //   - the form of the register-form x stage: 2 or 4 rows per block, or a
@@ -44,8 +45,8 @@ std::string mesh_key(const cdns_ctx *c) {
     const Dims &d = c->d;
     // the device name holds at most 256 characters; seven ints and separators follow
     char buf[256 + 96];
-    std::snprintf(buf, sizeof buf, "%.256s/%d|%d,%d,%d|%d,%d,%d", prop.name, prop.multiProcessorCount, d.NX2,
-                  d.NY2, d.NZ2, d.NXS, d.NYS, d.NZS);
+    std::snprintf(buf, sizeof buf, "%.256s/%d|%d,%d,%d|%d,%d,%d%s", prop.name, prop.multiProcessorCount, d.NX2,
+                  d.NY2, d.NZ2, d.NXS, d.NYS, d.NZS, c->mixed ? "|fp32" : "");
     return buf;
 }
 
@@ -71,7 +72,30 @@ template <typename Fn> int time_min(cdns_ctx *c, int reps, Fn fn, float &best) {
     return CDNS_OK;
 }
 
+// FP32 stage buffers (mixed form): only the Chebyshev forms are timed, on
+// the context's FP32 buffers; the z and x shapes keep their rules.
+int measure_fp32(cdns_ctx *c, Choice &out) {
+    const Dims d = c->d;
+    cudaStream_t s = c->stream;
+    const int reps = 3;
+    out = Choice{};
+    if (!ydct_available(d, c->t)) return CDNS_OK;
+    float2 *F = reinterpret_cast<float2 *>(c->F);
+    Tables t = c->t;
+    float m_syn, f_syn, m_ana, f_ana;
+    int r = 0;
+    t.yform = 0;
+    if ((r = time_min(c, reps, [&] { launch_ysynth(d, t, c->U[0], c->om, 3, 6, F, c->mean, s); }, m_syn))) return r;
+    if ((r = time_min(c, reps, [&] { launch_yanalysis(d, t, F, c->aux, 3, s); }, m_ana))) return r;
+    t.yform = 3;
+    if ((r = time_min(c, reps, [&] { launch_ysynth(d, t, c->U[0], c->om, 3, 6, F, c->mean, s); }, f_syn))) return r;
+    if ((r = time_min(c, reps, [&] { launch_yanalysis(d, t, F, c->aux, 3, s); }, f_ana))) return r;
+    out.yform = (f_syn < m_syn ? 1 : 0) | (f_ana < m_ana ? 2 : 0);
+    return CDNS_OK;
+}
+
 int measure(cdns_ctx *c, Choice &out) {
+    if (c->mixed) return measure_fp32(c, out);
     const Dims base = c->d;
     cudaStream_t s = c->stream;
     const int reps = 3;
@@ -163,10 +187,6 @@ namespace cdns {
 // exports the cache to it after every new measurement, so that a later run --
 // a profiled one, whose timings would mislead the tuner -- reuses the choices.
 int tune_context(cdns_ctx *c, bool force) {
-    if (c->mixed) {   // FP32 stage buffers keep the rule-based shapes
-        apply_x_stage_env(c);
-        return CDNS_OK;
-    }
     if (c->pen) {
         // a pencil rank holds part of the mesh: timing it would file its
         // shapes under the whole mesh's key, so it keeps the rule-based ones

@@ -153,3 +153,22 @@ def test_mixed_rejects_meshes_without_register_form(key):
     m, p = odd_radix_case(key)
     with pytest.raises(cdns.CdnsError, match="mixed precision"):
         mixed_ctx_for(m, p)
+
+
+@pytest.mark.parametrize("form", ["matrix", "fft"])
+def test_mixed_chebyshev_forms(form, monkeypatch):
+    """Both forms of the Chebyshev transforms on the FP32 stage buffers (the
+    FFT form writes FP32 rows and keeps the mean profiles in FP64; its analysis
+    widens FP32 input and applies 1/(NX2 NZ2)): the mixed nonlinear term
+    against the FP64 one, at the bound of test_mixed_nonlinear_term_48."""
+    m, p = channel_case(32)
+    u = np.stack(divergence_free_field(m, p, seed=0, amp=0.05, kmax=4), axis=-1)
+    N64, B64 = ctx_for(m, p).nonlinear(u)
+    monkeypatch.setenv("CDNS_Y_TRANSFORM", form)
+    c32 = mixed_ctx_for(m, p)
+    assert c32.tuning()["y_synthesis"] == form and c32.tuning()["y_analysis"] == form
+    N32, B32 = c32.nonlinear(u)
+    for k in range(3):
+        assert rel_l2(N32[..., k], N64[..., k]) <= 1e-5
+    scale = max(np.abs(B64).max(), np.abs(N64[..., 1]).max() * (m.NYS + 1))
+    assert np.abs(B32 - B64).max() <= 1e-5 * scale
