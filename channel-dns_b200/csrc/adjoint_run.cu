@@ -220,12 +220,16 @@ void nonlinear_adjoint(cdns_ctx *c, const double2 *G6, const double2 *lN, const 
     Tables ta = c->t;
     ta.csyn = w->csyn_t;   // includes 1/(NX2 NZ2): the transposed x and z analysis scalings
     ta.yform = 0;          // the transposed tables run in the matrix form
-    launch_ysynth(d, ta, lN, nullptr, 3, 3, w->AF, s);
+    // the transposed analysis has the synthesis' structure and the transposed
+    // synthesis the analysis': each takes the FFT form where the forward does
+    if (!((c->t.yform & 2) && launch_ydct_adjoint_analysis(d, c->t, lN, 3, w->AF, s)))
+        launch_ysynth(d, ta, lN, nullptr, 3, 3, w->AF, s);
     launch_z_backward(d, c->pz, c->t.root_z, w->AF, w->AG, 3, s);
     launch_x_adjoint(d, c->px, c->t.root_x, G6, w->AG, s);
     // transposed z synthesis = NZ2 x the (1/NZ2-scaled) forward z transform
     launch_z_forward(d, c->pz, c->t.root_z, w->AG, w->AF, 6, s);
-    launch_yanalysis_scaled(d, w->cana_t, w->AF, w->l6, 6, (double)d.NZ2, s);
+    if (!((c->t.yform & 1) && launch_ydct_adjoint_synthesis(d, c->t, w->AF, 6, w->l6, (double)d.NZ2, s)))
+        launch_yanalysis_scaled(d, w->cana_t, w->AF, w->l6, 6, (double)d.NZ2, s);
     launch_curl_adjoint(d, c->t, w->l6, lbw, lu, c->pp.Re, s);
 }
 

@@ -85,6 +85,12 @@ bool launch_ydct_synthesis_fp32(const Dims &d, const Tables &t, const double2 *s
                                 int nsplit, int nf, float2 *F, double *mean, cudaStream_t s);
 bool launch_ydct_analysis_fp32(const Dims &d, const Tables &t, const float2 *F, double2 *S, int nf,
                                cudaStream_t s);
+// Transposes of the analysis and of the synthesis (discrete adjoint) in the
+// FFT form: the products of k_cheb_tables_adjoint's csyn_t and cana_t tables.
+bool launch_ydct_adjoint_analysis(const Dims &d, const Tables &t, const double2 *lS, int nf, double2 *F,
+                                  cudaStream_t s);
+bool launch_ydct_adjoint_synthesis(const Dims &d, const Tables &t, const double2 *F, int nf, double2 *S,
+                                   double scale, cudaStream_t s);
 // Output reduction, x stage on the coarse grid (Dims of the coarse grid):
 // c2r of G[nf] (u, v, w, p and, if nf = 5, div), per-point moments summed per
 // block into partial[NY+1][moment_blocks][22]; phys (may be null) receives u, v, w, p.

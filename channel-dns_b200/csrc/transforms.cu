@@ -304,18 +304,23 @@ __host__ __device__ constexpr size_t ydct_slots(int n, int tl) {
 
 // Operands of the DCT kernels; CT is the stage buffer's complex type (double2,
 // or float2 for the mixed form's FP32 stages).  Synthesis: spectral
-// spec0 / spec1 (fields f < nsplit / the rest) -> F; with `mean` (FP32 stages)
-// the (kz, kx) = (0, 0) column goes to mean[f][j] in FP64 and zeros to F.
-// Analysis: F -> spectral S, scaled by an extra sxz (1 / (NX2 NZ2) for FP32
-// stages, whose z and x analyses leave it out).
+// spec0 / spec1 (fields f < nsplit / the rest), coefficient k weighted by
+// in0 (k = 0) or in1, -> F, row j weighted by outE (j = 0, N) or outI; with
+// `mean` (FP32 stages) the (kz, kx) = (0, 0) column goes to mean[f][j] in FP64
+// and zeros to F.  Analysis: F, row j weighted by inE (j = 0, N) or inI, ->
+// spectral S, coefficient k scaled by s0 (k = 0) or sk.  The forward
+// transforms take unit weights and s0 = 1/N, sk = 2/N (times 1 / (NX2 NZ2) for
+// FP32 stages, whose z and x analyses leave it out); the discrete adjoint's
+// transposed stages take other weights (launch_ydct_adjoint_*).
 template <class CT> struct YdctArgs {
-    const double2 *spec0, *spec1;
-    int nsplit;
-    const CT *Fin;
-    CT *Fout;
-    double2 *S;
-    double *mean;
-    double sxz;
+    const double2 *spec0 = nullptr, *spec1 = nullptr;
+    int nsplit = 0;
+    const CT *Fin = nullptr;
+    CT *Fout = nullptr;
+    double2 *S = nullptr;
+    double *mean = nullptr;
+    double in0 = 1.0, in1 = 1.0, outE = 1.0, outI = 1.0;   // synthesis weights
+    double inE = 1.0, inI = 1.0, s0 = 0.0, sk = 0.0;       // analysis weights and scales
 };
 
 template <int N1, int N2, bool ANA, int TL, class CT>
@@ -342,7 +347,7 @@ k_ydct_r(Dims d, const double2 *__restrict__ roots, const double *__restrict__ c
         const double2 *S = (f < A.nsplit ? A.spec0 + (long long)f * d.Ns : A.spec1 + (long long)(f - A.nsplit) * d.Ns) +
                            (long long)kzi * ncy * nkx + kx;
         for (int n = r; n <= N; n += R) {
-            double2 v = (n < ncy && lok) ? S[(long long)n * nkx] : mk(0.0, 0.0);
+            double2 v = (n < ncy && lok) ? cscale(n == 0 ? A.in0 : A.in1, S[(long long)n * nkx]) : mk(0.0, 0.0);
             if (n == 0) v = cadd(v, v);
             X[n * TL + l] = v;
             if (n >= 1 && n < N) y1 = cadd(y1, cscale(cosy[n], v));
@@ -350,7 +355,8 @@ k_ydct_r(Dims d, const double2 *__restrict__ roots, const double *__restrict__ c
     } else {
         const CT *F = A.Fin + (long long)f * d.ny2 * d.fcol + (long long)kzi * nkx + kx;
         for (int n = r; n <= N; n += R) {
-            const double2 v = lok ? cto<double2>(F[(long long)n * d.fcol]) : mk(0.0, 0.0);
+            const double2 v =
+                lok ? cscale(n == 0 || n == N ? A.inE : A.inI, cto<double2>(F[(long long)n * d.fcol])) : mk(0.0, 0.0);
             X[n * TL + l] = v;
             if (n >= 1 && n < N) y1 = cadd(y1, cscale(cosy[n], v));
         }
@@ -409,12 +415,12 @@ k_ydct_r(Dims d, const double2 *__restrict__ roots, const double *__restrict__ c
                 Fo[(long long)j * d.fcol] = mkc<CT>(0.0, 0.0);
             }
         } else {
-            for (int j = r; j <= N; j += R) Fo[(long long)j * d.fcol] = cto<CT>(X[j * TL + l]);
+            for (int j = r; j <= N; j += R)
+                Fo[(long long)j * d.fcol] = cto<CT>(cscale(j == 0 || j == N ? A.outE : A.outI, X[j * TL + l]));
         }
     } else {
         double2 *So = A.S + (long long)f * d.Ns + (long long)kzi * ncy * nkx + kx;
-        const double s0 = A.sxz / (double)N, sk = 2.0 * A.sxz / (double)N;
-        for (int k = r; k < ncy; k += R) So[(long long)k * nkx] = cscale(k == 0 ? s0 : sk, X[k * TL + l]);
+        for (int k = r; k < ncy; k += R) So[(long long)k * nkx] = cscale(k == 0 ? A.s0 : A.sk, X[k * TL + l]);
     }
 }
 
@@ -1704,22 +1710,49 @@ bool ydct(const Dims &d, const Tables &t, int nf, bool ana, const YdctArgs<CT> &
 }
 bool launch_ydct(const Dims &d, const Tables &t, const double2 *src0, const double2 *src1, int nsplit, int nf,
                  double2 *out, bool ana, cudaStream_t s) {
-    YdctArgs<double2> A{};
+    YdctArgs<double2> A;
     if (ana) {
         A.Fin = src0;
         A.S = out;
+        A.s0 = 1.0 / (double)d.NY2;
+        A.sk = 2.0 / (double)d.NY2;
     } else {
         A.spec0 = src0;
         A.spec1 = src1;
         A.nsplit = nsplit;
         A.Fout = out;
     }
-    A.sxz = 1.0;
     return ydct(d, t, nf, ana, A, s);
+}
+bool launch_ydct_adjoint_analysis(const Dims &d, const Tables &t, const double2 *lS, int nf, double2 *F,
+                                  cudaStream_t s) {
+    // F_j = v_j xs sum_k s_k lS_k cos(pi j k / N): s_0 = 1/(2N), s_k = 1/N;
+    // v_0 = v_N = 1, v_j = 2; xs = 1/(NX2 NZ2), the transposed x and z scalings
+    const double N = (double)d.NY2, xs = 1.0 / ((double)d.NX2 * (double)d.NZ2);
+    YdctArgs<double2> A;
+    A.spec0 = lS;
+    A.nsplit = nf;
+    A.Fout = F;
+    A.in0 = 1.0 / (2.0 * N);
+    A.in1 = 1.0 / N;
+    A.outE = xs;
+    A.outI = 2.0 * xs;
+    return ydct(d, t, nf, false, A, s);
+}
+bool launch_ydct_adjoint_synthesis(const Dims &d, const Tables &t, const double2 *F, int nf, double2 *S,
+                                   double scale, cudaStream_t s) {
+    // S_k = scale sum_{j=0..N} F_j cos(pi j k / N): the DCT-I with its end rows doubled
+    YdctArgs<double2> A;
+    A.Fin = F;
+    A.S = S;
+    A.inE = 2.0;
+    A.s0 = scale;
+    A.sk = scale;
+    return ydct(d, t, nf, true, A, s);
 }
 bool launch_ydct_synthesis_fp32(const Dims &d, const Tables &t, const double2 *src0, const double2 *src1,
                                 int nsplit, int nf, float2 *F, double *mean, cudaStream_t s) {
-    YdctArgs<float2> A{};
+    YdctArgs<float2> A;
     A.spec0 = src0;
     A.spec1 = src1;
     A.nsplit = nsplit;
@@ -1729,10 +1762,12 @@ bool launch_ydct_synthesis_fp32(const Dims &d, const Tables &t, const double2 *s
 }
 bool launch_ydct_analysis_fp32(const Dims &d, const Tables &t, const float2 *F, double2 *S, int nf,
                                cudaStream_t s) {
-    YdctArgs<float2> A{};
+    YdctArgs<float2> A;
     A.Fin = F;
     A.S = S;
-    A.sxz = 1.0 / ((double)d.NX2 * (double)d.NZ2);
+    const double sxz = 1.0 / ((double)d.NX2 * (double)d.NZ2);
+    A.s0 = sxz / (double)d.NY2;
+    A.sk = 2.0 * sxz / (double)d.NY2;
     return ydct(d, t, nf, true, A, s);
 }
 

@@ -59,10 +59,15 @@ def test_solve_adjoint_dot_product(n):
         assert abs(lhs - rhs_) <= 1e-12 * scale, (it, lhs, rhs_, scale)
 
 
+@pytest.mark.parametrize("form", ["matrix", "fft"])
 @pytest.mark.parametrize("n", [32, 48])
-def test_nonlinear_adjoint_dot_product(n):
+def test_nonlinear_adjoint_dot_product(n, form, monkeypatch):
+    """<lN, N(u+d) - N(u-d)> = 2 <N'(u)^T lN, d> (u x omega is quadratic), with
+    the Chebyshev stages and their transposes in the matrix or the FFT form."""
+    monkeypatch.setenv("CDNS_Y_TRANSFORM", form)
     m, p = channel_case(n)
     ctx = ctx_for(m, p)
+    assert ctx.tuning()["y_synthesis"] == form
     nkz, ncy, nkx = m.spectral_shape()
     u = np.stack(divergence_free_field(m, p, seed=5, amp=0.1, kmax=6), axis=-1)
     d = np.stack([band_spectrum(m, seed=20 + c, amp=0.05) for c in range(3)], axis=-1)
@@ -121,11 +126,13 @@ def mean_profile(m, rng, scale=0.3):
     return d
 
 
-def test_adjoint_vjp_small_channel():
+@pytest.mark.parametrize("form", ["matrix", "fft"])
+def test_adjoint_vjp_small_channel(form, monkeypatch):
     """Vector-Jacobian product of 6 steps of a 32^3 channel (projection
     objective Re <w, u^6>, checkpoints every 4 steps: a partial last
     interval): initial-field fluctuations, mean profile, blowing/suction
-    modes and uniform blowing."""
+    modes and uniform blowing; Chebyshev stages in either form."""
+    monkeypatch.setenv("CDNS_Y_TRANSFORM", form)
     m, p = channel_case(32)
     u0 = np.stack(divergence_free_field(m, p, seed=1, amp=0.1, spectrum="k53", mean="loglaw"), axis=-1)
     bc0 = wall_control(m, seed=2, amp=1e-3)
