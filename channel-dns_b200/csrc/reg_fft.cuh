@@ -13,6 +13,8 @@ namespace cdns {
 
 // N = A x B with A, B in {1, 2, 3, 4, 5, 7}.
 template <int N> struct RegSplit;
+template <> struct RegSplit<2> { static constexpr int A = 2, B = 1; };
+template <> struct RegSplit<3> { static constexpr int A = 3, B = 1; };
 template <> struct RegSplit<4> { static constexpr int A = 4, B = 1; };
 template <> struct RegSplit<6> { static constexpr int A = 2, B = 3; };
 template <> struct RegSplit<7> { static constexpr int A = 7, B = 1; };

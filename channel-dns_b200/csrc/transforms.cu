@@ -533,7 +533,14 @@ k_x_cross(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 *_
 // S and P share one buffer; every phase reads into registers before a
 // barrier and writes after it.
 // ---------------------------------------------------------------------------
-template <int N1, int N2, class C, bool MEAN>
+// SPLIT (N1, N2 even): the forward phases 3 and 4 give each of the 1.5 RW
+// forward lines two slots (one warp, lanes h = 0, 1 of a pair sub, sub + 16):
+// each N-point DFT step is split by decimation in time into its even (h = 0)
+// and odd (h = 1) samples, N/2-point DFTs on each lane, the odd half twiddled
+// by W_N^k, and the butterfly X_k = E_k + W^k O_k, X_{k+N/2} = E_k - W^k O_k
+// exchanged by __shfl_xor(16): lane h then holds outputs k + h N/2.  So all
+// 3 RW slots work in every phase (without SPLIT, half of them idle in 3, 4).
+template <int N1, int N2, class C, bool MEAN, bool SPLIT = false>
 __global__ void __launch_bounds__(16 * 3 * 4)
 k_x_cross_r(Dims d, const double2 *__restrict__ roots, const C *__restrict__ G, C *__restrict__ H, int RW,
             const double *__restrict__ mean) {
@@ -615,89 +622,199 @@ k_x_cross_r(Dims d, const double2 *__restrict__ roots, const C *__restrict__ G, 
         moy = (T)mean[4 * ny2 + j];
         moz = (T)mean[5 * ny2 + j];
     }
-    // out lines per row pair (r, r+1): (N0 + i N1)(r), (N0 + i N1)(r+1), N2(r) + i N2(r+1)
-    const bool act3 = slot < L2 && sub < N2;
-    if (act3) {
-        const int pr = slot / 3, kind = slot - (slot / 3) * 3;
+    if constexpr (SPLIT) {
+        static_assert(N1 % 2 == 0 && N2 % 2 == 0, "lane-pair split needs even factors");
+        constexpr int H1 = N1 / 2, H2 = N2 / 2;
+        const int ol = slot >> 1, h = slot & 1;   // forward line, half (lanes sub and sub + 16)
+        const int pr = ol / 3, kind = ol - (ol / 3) * 3;
+        // ---- phase 3: products at x = sub + N2 (2m + h), N1/2-point DFTs --------
+        const bool act3 = ol < L2 && sub < N2;
+        if (act3) {
 #pragma unroll
-        for (int n1 = 0; n1 < N1; ++n1) {
-            const int x = sub + N2 * n1;
-            auto prod = [&](int r, T &n0, T &n1v, T &n2v) {
-                const C p0 = buf[(3 * r) * n + x];
-                const C p1 = buf[(3 * r + 1) * n + x];
-                const C p2 = buf[(3 * r + 2) * n + x];
-                const T uu = p0.x, vv = p0.y, ww = p1.x, ox = p1.y, oy = p2.x, oz = p2.y;
-                n0 = vv * oz - ww * oy;
-                n1v = ww * ox - uu * oz;
-                n2v = uu * oy - vv * ox;
-                if constexpr (MEAN) {
-                    // fluctuations about the FP64 mean profiles: + M x om' + u' x M_om
-                    // (M x M_om is added to the mean mode in FP64 after the analysis)
-                    n0 += (mv * oz - mw * oy) + (vv * moz - ww * moy);
-                    n1v += (mw * ox - mu * oz) + (ww * mox - uu * moz);
-                    n2v += (mu * oy - mv * ox) + (uu * moy - vv * mox);
+            for (int m = 0; m < H1; ++m) {
+                const int x = sub + N2 * (2 * m + h);
+                auto prod = [&](int r, T &n0, T &n1v, T &n2v) {
+                    const C p0 = buf[(3 * r) * n + x];
+                    const C p1 = buf[(3 * r + 1) * n + x];
+                    const C p2 = buf[(3 * r + 2) * n + x];
+                    const T uu = p0.x, vv = p0.y, ww = p1.x, ox = p1.y, oy = p2.x, oz = p2.y;
+                    n0 = vv * oz - ww * oy;
+                    n1v = ww * ox - uu * oz;
+                    n2v = uu * oy - vv * ox;
+                    if constexpr (MEAN) {
+                        n0 += (mv * oz - mw * oy) + (vv * moz - ww * moy);
+                        n1v += (mw * ox - mu * oz) + (ww * mox - uu * moz);
+                        n2v += (mu * oy - mv * ox) + (uu * moy - vv * mox);
+                    }
+                };
+                T a0, a1, a2, b0, b1, b2;
+                if (kind < 2) {
+                    prod(2 * pr + kind, a0, a1, a2);
+                    v[m] = mkc<C>(a0, a1);
+                } else {
+                    prod(2 * pr, a0, a1, a2);
+                    prod(2 * pr + 1, b0, b1, b2);
+                    v[m] = mkc<C>(a2, b2);
                 }
-            };
-            T a0, a1, a2, b0, b1, b2;
+            }
+        }
+        __syncthreads();
+        if (act3) {
+            C(&w)[H1] = reinterpret_cast<C(&)[H1]>(v);
+            dft_reg<H1, -1>(w, tw, 2 * N2);
+            if (h) {
+#pragma unroll
+                for (int k = 1; k < H1; ++k) w[k] = tw.template mul<-1>(w[k], k * N2);   // W_N1^k
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < H1; ++k) {
+            C q;
+            q.x = __shfl_xor_sync(0xffffffffu, v[k].x, 16);
+            q.y = __shfl_xor_sync(0xffffffffu, v[k].y, 16);
+            if (!act3) continue;
+            const C xk = h ? csub(q, v[k]) : cadd(v[k], q);
+            const int k1 = k + h * H1;
+            buf[(ol * N1 + k1) * SP + sub] = (k1 == 0 || sub == 0) ? xk : tw.template mul<-1>(xk, sub * k1);
+        }
+        __syncthreads();
+        // ---- phase 4: N2/2-point DFTs over n2 = 2m + h, unpack, modes k <= NXS ---
+        const bool act4 = ol < L2 && sub < N1;
+        if (act4) {
+#pragma unroll
+            for (int m = 0; m < H2; ++m) v[m] = buf[(ol * N1 + sub) * SP + 2 * m + h];
+            C(&w)[H2] = reinterpret_cast<C(&)[H2]>(v);
+            dft_reg<H2, -1>(w, tw, 2 * N1);
+            if (h) {
+#pragma unroll
+                for (int k = 1; k < H2; ++k) w[k] = tw.template mul<-1>(w[k], k * N1);   // W_N2^k
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < H2; ++k) {
+            C q;
+            q.x = __shfl_xor_sync(0xffffffffu, v[k].x, 16);
+            q.y = __shfl_xor_sync(0xffffffffu, v[k].y, 16);
+            v[k] = h ? csub(q, v[k]) : cadd(v[k], q);   // P[sub + N1 (h H2 + k)]
+        }
+        // partner of q = k1 + N1 k2 (k2 = h H2 + c) is n - q: for k1 > 0 lane
+        // (1 - h, N1 - k1), c' = H2 - 1 - c; for k1 = 0 lane (1 - h, 0), c' = H2 - c
+        // (c = 0: the lane itself)
+        const int base = 16 * (1 - h);
+        const int pA = base + (sub < N1 ? (N1 - sub) % N1 : sub);
+        const T invn = (T)(sizeof(C) == 8 ? 1.0 : 1.0 / (double)n);
+#pragma unroll
+        for (int c = 0; c < H2; ++c) {
+            C pa, pb;
+            pa.x = __shfl_sync(0xffffffffu, v[H2 - 1 - c].x, pA);
+            pa.y = __shfl_sync(0xffffffffu, v[H2 - 1 - c].y, pA);
+            pb.x = __shfl_sync(0xffffffffu, v[(H2 - c) % H2].x, base);
+            pb.y = __shfl_sync(0xffffffffu, v[(H2 - c) % H2].y, base);
+            const int k = sub + N1 * (h * H2 + c);
+            if (!act4 || k > nxs) continue;
+            const C pm = sub > 0 ? pa : (c == 0 ? v[0] : pb);
+            const C p0 = v[c];
+            const C outA = cscale(invn, mkc<C>(T(0.5) * (p0.x + pm.x), T(0.5) * (p0.y - pm.y)));
+            const C outB = cscale(invn, mkc<C>(T(0.5) * (p0.y + pm.y), T(-0.5) * (p0.x - pm.x)));
             if (kind < 2) {
-                prod(2 * pr + kind, a0, a1, a2);
-                v[n1] = mkc<C>(a0, a1);
+                const int z = z0 + 2 * pr + kind;
+                if (z < d.NZ2) {
+                    C *hp = H + ((long long)j * d.NZ2 + z) * nkx + k;
+                    hp[0] = outA;            // N0
+                    hp[fstride] = outB;      // N1
+                }
             } else {
-                prod(2 * pr, a0, a1, a2);
-                prod(2 * pr + 1, b0, b1, b2);
-                v[n1] = mkc<C>(a2, b2);
+                const int z = z0 + 2 * pr;
+                C *hp = H + 2 * fstride + ((long long)j * d.NZ2 + z) * nkx + k;
+                if (z < d.NZ2) hp[0] = outA;                 // N2 of row r
+                if (z + 1 < d.NZ2) hp[nkx] = outB;           // N2 of row r+1
             }
         }
-    }
-    __syncthreads();
-    if (act3) {
-        C(&w)[N1] = reinterpret_cast<C(&)[N1]>(v);
-        dft_reg<N1, -1>(w, tw, N2);
-#pragma unroll
-        for (int k1 = 0; k1 < N1; ++k1) {
-            const C t = (k1 == 0 || sub == 0) ? w[k1] : tw.template mul<-1>(w[k1], sub * k1);
-            buf[(slot * N1 + k1) * SP + sub] = t;
-        }
-    }
-    __syncthreads();
-    // ---- phase 4: N2-point DFTs, unpack, modes k <= NXS -------------------
-    const bool act4 = slot < L2 && sub < N1;
-    if (act4) {
-#pragma unroll
-        for (int n2 = 0; n2 < N2; ++n2) v[n2] = buf[(slot * N1 + sub) * SP + n2];
-        C(&w)[N2] = reinterpret_cast<C(&)[N2]>(v);
-        dft_reg<N2, -1>(w, tw, N1);
-    }
-    // partner of frequency k1 + N1 k2 is n - k = k1' + N1 k2' with
-    // k1' = (N1 - k1) mod N1, k2' = N2 - 1 - k2 (k1 > 0) or (N2 - k2) mod N2 (k1 = 0)
-    const int lane = threadIdx.x & 31;
-    const int partner = (lane & 16) + (sub < N1 ? (N1 - sub) % N1 : sub);
-    const int pr = slot / 3, kind = slot - (slot / 3) * 3;
-    // FP32: no 1/NX2 here (not exact in FP32); the FP64 y analysis applies 1/(NX2 NZ2)
-    const T invn = (T)(sizeof(C) == 8 ? 1.0 : 1.0 / (double)n);
-#pragma unroll
-    for (int k2 = 0; k2 < N2; ++k2) {
-        C pm;
-        pm.x = __shfl_sync(0xffffffffu, v[N2 - 1 - k2].x, partner);
-        pm.y = __shfl_sync(0xffffffffu, v[N2 - 1 - k2].y, partner);
-        const int k = sub + N1 * k2;
-        if (!act4 || k > nxs) continue;
-        if (sub == 0) pm = v[(N2 - k2) % N2];
-        const C p0 = v[k2];
-        const C outA = cscale(invn, mkc<C>(T(0.5) * (p0.x + pm.x), T(0.5) * (p0.y - pm.y)));
-        const C outB = cscale(invn, mkc<C>(T(0.5) * (p0.y + pm.y), T(-0.5) * (p0.x - pm.x)));
-        if (kind < 2) {
-            const int z = z0 + 2 * pr + kind;
-            if (z < d.NZ2) {
-                C *h = H + ((long long)j * d.NZ2 + z) * nkx + k;
-                h[0] = outA;            // N0
-                h[fstride] = outB;      // N1
+    } else {
+        // out lines per row pair (r, r+1): (N0 + i N1)(r), (N0 + i N1)(r+1), N2(r) + i N2(r+1)
+        const bool act3 = slot < L2 && sub < N2;
+        if (act3) {
+            const int pr = slot / 3, kind = slot - (slot / 3) * 3;
+    #pragma unroll
+            for (int n1 = 0; n1 < N1; ++n1) {
+                const int x = sub + N2 * n1;
+                auto prod = [&](int r, T &n0, T &n1v, T &n2v) {
+                    const C p0 = buf[(3 * r) * n + x];
+                    const C p1 = buf[(3 * r + 1) * n + x];
+                    const C p2 = buf[(3 * r + 2) * n + x];
+                    const T uu = p0.x, vv = p0.y, ww = p1.x, ox = p1.y, oy = p2.x, oz = p2.y;
+                    n0 = vv * oz - ww * oy;
+                    n1v = ww * ox - uu * oz;
+                    n2v = uu * oy - vv * ox;
+                    if constexpr (MEAN) {
+                        // fluctuations about the FP64 mean profiles: + M x om' + u' x M_om
+                        // (M x M_om is added to the mean mode in FP64 after the analysis)
+                        n0 += (mv * oz - mw * oy) + (vv * moz - ww * moy);
+                        n1v += (mw * ox - mu * oz) + (ww * mox - uu * moz);
+                        n2v += (mu * oy - mv * ox) + (uu * moy - vv * mox);
+                    }
+                };
+                T a0, a1, a2, b0, b1, b2;
+                if (kind < 2) {
+                    prod(2 * pr + kind, a0, a1, a2);
+                    v[n1] = mkc<C>(a0, a1);
+                } else {
+                    prod(2 * pr, a0, a1, a2);
+                    prod(2 * pr + 1, b0, b1, b2);
+                    v[n1] = mkc<C>(a2, b2);
+                }
             }
-        } else {
-            const int z = z0 + 2 * pr;
-            C *h = H + 2 * fstride + ((long long)j * d.NZ2 + z) * nkx + k;
-            if (z < d.NZ2) h[0] = outA;                 // N2 of row r
-            if (z + 1 < d.NZ2) h[nkx] = outB;           // N2 of row r+1
+        }
+        __syncthreads();
+        if (act3) {
+            C(&w)[N1] = reinterpret_cast<C(&)[N1]>(v);
+            dft_reg<N1, -1>(w, tw, N2);
+    #pragma unroll
+            for (int k1 = 0; k1 < N1; ++k1) {
+                const C t = (k1 == 0 || sub == 0) ? w[k1] : tw.template mul<-1>(w[k1], sub * k1);
+                buf[(slot * N1 + k1) * SP + sub] = t;
+            }
+        }
+        __syncthreads();
+        // ---- phase 4: N2-point DFTs, unpack, modes k <= NXS -------------------
+        const bool act4 = slot < L2 && sub < N1;
+        if (act4) {
+    #pragma unroll
+            for (int n2 = 0; n2 < N2; ++n2) v[n2] = buf[(slot * N1 + sub) * SP + n2];
+            C(&w)[N2] = reinterpret_cast<C(&)[N2]>(v);
+            dft_reg<N2, -1>(w, tw, N1);
+        }
+        // partner of frequency k1 + N1 k2 is n - k = k1' + N1 k2' with
+        // k1' = (N1 - k1) mod N1, k2' = N2 - 1 - k2 (k1 > 0) or (N2 - k2) mod N2 (k1 = 0)
+        const int lane = threadIdx.x & 31;
+        const int partner = (lane & 16) + (sub < N1 ? (N1 - sub) % N1 : sub);
+        const int pr = slot / 3, kind = slot - (slot / 3) * 3;
+        // FP32: no 1/NX2 here (not exact in FP32); the FP64 y analysis applies 1/(NX2 NZ2)
+        const T invn = (T)(sizeof(C) == 8 ? 1.0 : 1.0 / (double)n);
+    #pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) {
+            C pm;
+            pm.x = __shfl_sync(0xffffffffu, v[N2 - 1 - k2].x, partner);
+            pm.y = __shfl_sync(0xffffffffu, v[N2 - 1 - k2].y, partner);
+            const int k = sub + N1 * k2;
+            if (!act4 || k > nxs) continue;
+            if (sub == 0) pm = v[(N2 - k2) % N2];
+            const C p0 = v[k2];
+            const C outA = cscale(invn, mkc<C>(T(0.5) * (p0.x + pm.x), T(0.5) * (p0.y - pm.y)));
+            const C outB = cscale(invn, mkc<C>(T(0.5) * (p0.y + pm.y), T(-0.5) * (p0.x - pm.x)));
+            if (kind < 2) {
+                const int z = z0 + 2 * pr + kind;
+                if (z < d.NZ2) {
+                    C *h = H + ((long long)j * d.NZ2 + z) * nkx + k;
+                    h[0] = outA;            // N0
+                    h[fstride] = outB;      // N1
+                }
+            } else {
+                const int z = z0 + 2 * pr;
+                C *h = H + 2 * fstride + ((long long)j * d.NZ2 + z) * nkx + k;
+                if (z < d.NZ2) h[0] = outA;                 // N2 of row r
+                if (z + 1 < d.NZ2) h[nkx] = outB;           // N2 of row r+1
+            }
         }
     }
 }
@@ -1515,6 +1632,9 @@ template <class C> cudaError_t configure_register_forms(const Dims &d) {
     with_xsplit(d.NX2, [&](auto a, auto b) {
         constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
         e = raise_smem(k_x_cross_r<N1, N2, C, sizeof(C) == 8>, smem_xcross_r(N1, N2, sizeof(C)));
+        if constexpr (N1 % 2 == 0 && N2 % 2 == 0)
+            if (e == cudaSuccess)
+                e = raise_smem(k_x_cross_r<N1, N2, C, sizeof(C) == 8, true>, smem_xcross_r(N1, N2, sizeof(C)));
         if (e == cudaSuccess)
             e = raise_smem(k_x_cross_h<N1, N2, C, sizeof(C) == 8>, smem_xcross_h(N1, N2, sizeof(C)));
         if (e == cudaSuccess && sizeof(C) == 16) e = raise_smem(k_x_adjoint_r<N1, N2>, smem_xadjoint_r(N1, N2));
@@ -1602,6 +1722,13 @@ bool x_cross_r(const Dims &d, const double2 *roots, const C *G, C *H, const doub
     return with_xsplit(d.NX2, [&](auto a, auto b) {
         constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
         dim3 grid((d.NZ2 + rw - 1) / rw, d.ny2);
+        if constexpr (N1 % 2 == 0 && N2 % 2 == 0) {
+            if (d.xrw == 3) {   // 4 rows, forward phases split over lane pairs
+                k_x_cross_r<N1, N2, C, MEAN, true><<<grid, 16 * 3 * rw, smem_xcross_r(N1, N2, sizeof(C)), s>>>(
+                    d, roots, G, H, rw, mean);
+                return;
+            }
+        }
         k_x_cross_r<N1, N2, C, MEAN><<<grid, 16 * 3 * rw, smem_xcross_r(N1, N2, sizeof(C)), s>>>(
             d, roots, G, H, rw, mean);
     });

@@ -3,12 +3,12 @@
 // src/fft/wisdom.cpp:11-32).
 //
 // For each mesh, the first FP64 context times on its own device buffers, with
-// CUDA events on its stream (a mixed-precision context times only the two
-// Chebyshev forms, on its FP32 buffers, under a key of its own),
+// CUDA events on its stream (a mixed-precision context times the x-stage and
+// Chebyshev forms on its FP32 buffers, under a key of its own),
 //   - the kx lines per block of the z transforms (8..17): the z synthesis of
 //     the six nonlinear-term fields plus the z analysis of three, and
-//   - the form of the register-form x stage: 2 or 4 rows per block, or a
-//     half-warp per row pair,
+//   - the form of the register-form x stage: 2 or 4 rows per block, 4 rows
+//     with the forward phases split over lane pairs, or a half-warp per row pair,
 //   - the Chebyshev synthesis (six fields) and analysis (three fields) in the
 //     matrix form (FP64 MMA products) and in the FFT form (DCT-I through one
 //     length-NY2 FFT per column; meshes whose NY2 has a register split),
@@ -72,13 +72,29 @@ template <typename Fn> int time_min(cdns_ctx *c, int reps, Fn fn, float &best) {
     return CDNS_OK;
 }
 
-// FP32 stage buffers (mixed form): only the Chebyshev forms are timed, on
-// the context's FP32 buffers; the z and x shapes keep their rules.
+// FP32 stage buffers (mixed form): the forms of the x stage and of the
+// Chebyshev transforms are timed on the context's FP32 buffers; the z
+// transforms keep their rule.
 int measure_fp32(cdns_ctx *c, Choice &out) {
     const Dims d = c->d;
     cudaStream_t s = c->stream;
     const int reps = 3;
     out = Choice{};
+    {
+        float2 *G = reinterpret_cast<float2 *>(c->G), *H = reinterpret_cast<float2 *>(c->H);
+        float best_x = 1e30f;
+        for (int rw : {4, 2, 1, 3}) {
+            Dims dx = d;
+            dx.xrw = rw;
+            float ms;
+            int r = time_min(c, reps, [&] { launch_x_cross(dx, c->t.root_x, G, H, c->mean, s); }, ms);
+            if (r) return r;
+            if (ms < best_x) {
+                best_x = ms;
+                out.xrw = rw;
+            }
+        }
+    }
     if (!ydct_available(d, c->t)) return CDNS_OK;
     float2 *F = reinterpret_cast<float2 *>(c->F);
     Tables t = c->t;
@@ -123,7 +139,7 @@ int measure(cdns_ctx *c, Choice &out) {
     // barrier) or the half-warp form (1: a half-warp per row pair, no block barrier)
     {
         float best_x = 1e30f;
-        for (int rw : {4, 2, 1}) {
+        for (int rw : {4, 2, 1, 3}) {
             Dims dx = d;
             dx.xrw = rw;
             float ms;
@@ -151,13 +167,14 @@ int measure(cdns_ctx *c, Choice &out) {
     return CDNS_OK;
 }
 
-// CDNS_X_STAGE=rows4|rows2|halfwarp fixes the form of the register-form x
+// CDNS_X_STAGE=rows4|rows2|halfwarp|split fixes the form of the register-form x
 // stage (comparisons, tests); FP32 contexts honour it too.
 void apply_x_stage_env(cdns_ctx *c) {
     if (const char *e = std::getenv("CDNS_X_STAGE")) {
         if (std::strcmp(e, "rows4") == 0) c->d.xrw = 4;
         else if (std::strcmp(e, "rows2") == 0) c->d.xrw = 2;
         else if (std::strcmp(e, "halfwarp") == 0) c->d.xrw = 1;
+        else if (std::strcmp(e, "split") == 0) c->d.xrw = 3;
     }
 }
 
@@ -307,7 +324,7 @@ int cdns_wisdom_import(const char *path) {
                             &ch.yform, &ch.xrw);
         if (n == 2) ch.xrw = 0;   // entries written before the x-stage choice existed
         if (n < 2 || ch.ztl < 0 || ch.ztl > 17 || (ch.ztl != 0 && ch.ztl < 8) || ch.yform < 0 || ch.yform > 3 ||
-            (ch.xrw != 0 && ch.xrw != 1 && ch.xrw != 2 && ch.xrw != 4))
+            (ch.xrw != 0 && (ch.xrw < 1 || ch.xrw > 4)))
             return fail(CDNS_ERR_ARG, "malformed wisdom entry");
         got[key] = ch;
         pos = end;

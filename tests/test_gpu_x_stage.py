@@ -1,5 +1,6 @@
 """Every form of the register-form x stage (k_x_cross_r with 4 or 2 rows per
-block, k_x_cross_h with a half-warp per row pair) against the oracle's
+block, with 4 rows and the forward phases split over lane pairs, k_x_cross_h
+with a half-warp per row pair) against the oracle's
 nonlinear term (src/solver/vector_ops.cpp:250-272 with the fine transforms
 of src/fft/transforms.cpp:641-741), on every x length split the register
 forms cover and at a full x spectrum (Nyquist branches); the FP32 stages of
@@ -14,7 +15,7 @@ from test_gpu_parity import ctx_for, rel_max
 
 pytestmark = pytest.mark.gpu
 
-FORMS = ["rows4", "rows2", "halfwarp"]
+FORMS = ["rows4", "rows2", "halfwarp", "split"]
 
 
 def mesh_x(nxs, nx2, nzs=8, nz2=32, nys=14, ny2=24):
@@ -41,7 +42,8 @@ def test_x_stage_forms_nonlinear_term(monkeypatch, form, case):
     cst = orc.make_constants(m, p.Re)
     N_ref, _, B_ref = orc.nonlinear_term(m, cst, u)
     c = ctx_for(m, p)
-    assert c.tuning()["x_rows"] == {"rows4": 4, "rows2": 2, "halfwarp": 1}[form]
+    # (72 = 8 x 9 has an odd factor: "split" runs the 4-rows form there)
+    assert c.tuning()["x_rows"] == {"rows4": 4, "rows2": 2, "halfwarp": 1, "split": 3}[form]
     N, B = c.nonlinear(np.stack(u, axis=-1))
     for k in range(3):
         assert rel_max(N[..., k], N_ref[k]) <= 1e-12
@@ -49,17 +51,18 @@ def test_x_stage_forms_nonlinear_term(monkeypatch, form, case):
     assert np.abs(B[:, 0] - B_ref[0]).max() <= 1e-12 * scale
 
 
+@pytest.mark.parametrize("form", ["halfwarp", "split"])
 @pytest.mark.parametrize("case", ["x48", "x196"])
-def test_x_stage_halfwarp_mixed(monkeypatch, case):
-    """FP32 stages (mean profiles kept in FP64) through the half-warp form
-    against the FP64 nonlinear term: the bound of test_gpu_mixed.py."""
+def test_x_stage_halfwarp_mixed(monkeypatch, case, form):
+    """FP32 stages (mean profiles kept in FP64) through the half-warp and the
+    split forms against the FP64 nonlinear term: the bound of test_gpu_mixed.py."""
     m, p = CASES[case]()
     u = np.stack(divergence_free_field(m, p, seed=19, amp=0.05, kmax=4), axis=-1)
     N64, _ = ctx_for(m, p).nonlinear(u)
-    monkeypatch.setenv("CDNS_X_STAGE", "halfwarp")
+    monkeypatch.setenv("CDNS_X_STAGE", form)
     mesh = cdns.Mesh(m.NX, m.NY, m.NZ, m.NXS, m.NYS, m.NZS, m.NX2, m.NY2, m.NZ2, m.XL, m.ZL)
     cm = cdns.Context(mesh, cdns.Params(Re=p.Re, DT=p.DT), precision=cdns.PRECISION_MIXED)
-    assert cm.tuning()["x_rows"] == 1
+    assert cm.tuning()["x_rows"] == {"halfwarp": 1, "split": 3}[form]
     N32, _ = cm.nonlinear(u)
     for k in range(3):
         assert orc.rel_l2(N32[..., k], N64[..., k]) <= 1e-5
