@@ -83,11 +83,11 @@ def stage_bytes(mesh):
 # only reported while these files are unchanged since its ncu capture.
 STAGE_SOURCES = {
     "curl": ["chebyshev.cu", "warp_columns.cuh"],
-    "y_synthesis": ["chebyshev.cu"],
+    "y_synthesis": ["chebyshev.cu", "transforms.cu", "reg_fft.cuh"],
     "z_backward": ["transforms.cu", "reg_fft.cuh", "fft_lines.cuh"],
     "x_cross": ["transforms.cu", "reg_fft.cuh", "fft_lines.cuh"],
     "z_forward": ["transforms.cu", "reg_fft.cuh", "fft_lines.cuh"],
-    "y_analysis": ["chebyshev.cu"],
+    "y_analysis": ["chebyshev.cu", "transforms.cu", "reg_fft.cuh"],
     "solve": ["solver.cu", "warp_columns.cuh"],
 }
 TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "dram_traffic_retau180.md")
