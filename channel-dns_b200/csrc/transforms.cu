@@ -133,6 +133,21 @@ template <class C> __device__ __forceinline__ Twiddles<C> load_twiddles(double2 
     }
     return Twiddles<C>{hi, lo};
 }
+// Inter-step twiddles of an N1 x N2 register transform (N2 <= 16) as N1 rows of
+// 16: entry (k1, s) = exp(-2 pi i s k1 / n), in 16 N1 double2 slots (FP32: the
+// roots and their rounding residues).  The view returned is offset to the
+// calling lane's column s = sub, so that row k1 is at index 16 k1.
+template <int N1, class C>
+__device__ __forceinline__ Twiddles<C> load_lane_twiddles(double2 *sm_d, const double2 *roots, int n, int sub) {
+    C *hi = reinterpret_cast<C *>(sm_d);
+    C *lo = sizeof(C) == 8 ? hi + 16 * N1 : hi;
+    for (int i = threadIdx.x; i < 16 * N1; i += blockDim.x) {
+        const double2 r = roots[((i & 15) * (i >> 4)) % n];
+        hi[i] = cto<C>(r);
+        if (sizeof(C) == 8) lo[i] = mkc<C>(r.x - (double)hi[i].x, r.y - (double)hi[i].y);
+    }
+    return Twiddles<C>{hi + sub, lo + sub};
+}
 
 template <int N1, int N2, int SIGN, class C, class Src, class Dst>
 __device__ __forceinline__ void fft2_lines(int TL, const Twiddles<C> &tw, C *S, const Src &src, const Dst &dst) {
@@ -540,15 +555,18 @@ k_x_cross(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 *_
 // by W_N^k, and the butterfly X_k = E_k + W^k O_k, X_{k+N/2} = E_k - W^k O_k
 // exchanged by __shfl_xor(16): lane h then holds outputs k + h N/2.  So all
 // 3 RW slots work in every phase (without SPLIT, half of them idle in 3, 4).
+// FP64 is held to 3 blocks per SM (at most 112 registers; left free, the
+// compiler moves all twiddle loads of a phase ahead and takes 138); FP32 has
+// no minimum (with one it takes 64 registers instead of 56).
 template <int N1, int N2, class C, bool MEAN, bool SPLIT = false>
-__global__ void __launch_bounds__(16 * 3 * 4)
+__global__ void __launch_bounds__(16 * 3 * 4, sizeof(C) == 16 ? 3 : 0)
 k_x_cross_r(Dims d, const double2 *__restrict__ roots, const C *__restrict__ G, C *__restrict__ H, int RW,
             const double *__restrict__ mean) {
     using T = typename CReal<C>::T;
     constexpr int n = N1 * N2;
     constexpr int SP = N2 + 1;   // padded row of the step-1 output
     extern __shared__ double2 sm_d[];
-    C *buf = reinterpret_cast<C *>(sm_d + n);
+    C *buf = reinterpret_cast<C *>(sm_d + n + 16 * N1);
     const int L = 3 * RW, L2 = 3 * (RW / 2);
     const int slot = threadIdx.x >> 4, sub = threadIdx.x & 15;
     const int j = blockIdx.y, z0 = blockIdx.x * RW;
@@ -556,6 +574,19 @@ k_x_cross_r(Dims d, const double2 *__restrict__ roots, const C *__restrict__ G, 
     const long long fstride = (long long)d.ny2 * d.NZ2 * nkx;
     const C *Gj = G + (long long)j * d.NZ2 * nkx;
     const Twiddles<C> tw = load_twiddles<C>(sm_d, roots, n);
+    // FP64: the inter-step twiddles W_n^(sub k1) as rows k1 of 16 lanes, so
+    // that the 16 lanes of a line read 16 consecutive entries (no bank
+    // conflicts).  FP32 reads them from the root table at index sub k1.
+    Twiddles<C> tws = tw;
+    if constexpr (sizeof(C) == 16) tws = load_lane_twiddles<N1, C>(sm_d + n, roots, n, sub);
+    // FP32 skips the product by the unit twiddle of lane 0 (without that
+    // branch the loads of all its twiddles move ahead: 80 registers, not 56)
+    constexpr bool FP32 = sizeof(C) == 8;
+    auto inter = [&](auto sign, C v, int k1) -> C {
+        constexpr int SIGN = decltype(sign)::value;
+        if constexpr (sizeof(C) == 16) return tws.template mul<SIGN>(v, 16 * k1);
+        else return tw.template mul<SIGN>(v, sub * k1);
+    };
     const int nyq = (n % 2 == 0) ? n / 2 : -1;
     C v[N1 > N2 ? N1 : N2];
 
@@ -592,7 +623,7 @@ k_x_cross_r(Dims d, const double2 *__restrict__ roots, const C *__restrict__ G, 
         dft_reg<N1, +1>(w, tw, N2);
 #pragma unroll
         for (int k1 = 0; k1 < N1; ++k1) {
-            const C t = (k1 == 0 || sub == 0) ? w[k1] : tw.template mul<+1>(w[k1], sub * k1);
+            const C t = (k1 == 0 || (FP32 && sub == 0)) ? w[k1] : inter(std::integral_constant<int, +1>{}, w[k1], k1);
             buf[(slot * N1 + k1) * SP + sub] = t;
         }
     }
@@ -675,7 +706,7 @@ k_x_cross_r(Dims d, const double2 *__restrict__ roots, const C *__restrict__ G, 
             if (!act3) continue;
             const C xk = h ? csub(q, v[k]) : cadd(v[k], q);
             const int k1 = k + h * H1;
-            buf[(ol * N1 + k1) * SP + sub] = (k1 == 0 || sub == 0) ? xk : tw.template mul<-1>(xk, sub * k1);
+            buf[(ol * N1 + k1) * SP + sub] = (k1 == 0 || (FP32 && sub == 0)) ? xk : inter(std::integral_constant<int, -1>{}, xk, k1);
         }
         __syncthreads();
         // ---- phase 4: N2/2-point DFTs over n2 = 2m + h, unpack, modes k <= NXS ---
@@ -699,20 +730,20 @@ k_x_cross_r(Dims d, const double2 *__restrict__ roots, const C *__restrict__ G, 
         }
         // partner of q = k1 + N1 k2 (k2 = h H2 + c) is n - q: for k1 > 0 lane
         // (1 - h, N1 - k1), c' = H2 - 1 - c; for k1 = 0 lane (1 - h, 0), c' = H2 - c
-        // (c = 0: the lane itself)
-        const int base = 16 * (1 - h);
-        const int pA = base + (sub < N1 ? (N1 - sub) % N1 : sub);
+        // (c = 0: the lane itself).  Lanes k1 = 0 serve only the k1 = 0 lane of the
+        // other half, so each lane sends the register its readers want: one
+        // shuffle per output.
+        const int pA = 16 * (1 - h) + (sub < N1 ? (N1 - sub) % N1 : sub);
         const T invn = (T)(sizeof(C) == 8 ? 1.0 : 1.0 / (double)n);
 #pragma unroll
         for (int c = 0; c < H2; ++c) {
-            C pa, pb;
-            pa.x = __shfl_sync(0xffffffffu, v[H2 - 1 - c].x, pA);
-            pa.y = __shfl_sync(0xffffffffu, v[H2 - 1 - c].y, pA);
-            pb.x = __shfl_sync(0xffffffffu, v[(H2 - c) % H2].x, base);
-            pb.y = __shfl_sync(0xffffffffu, v[(H2 - c) % H2].y, base);
+            const C send = sub == 0 ? v[(H2 - c) % H2] : v[H2 - 1 - c];
+            C pa;
+            pa.x = __shfl_sync(0xffffffffu, send.x, pA);
+            pa.y = __shfl_sync(0xffffffffu, send.y, pA);
             const int k = sub + N1 * (h * H2 + c);
             if (!act4 || k > nxs) continue;
-            const C pm = sub > 0 ? pa : (c == 0 ? v[0] : pb);
+            const C pm = (sub == 0 && c == 0) ? v[0] : pa;
             const C p0 = v[c];
             const C outA = cscale(invn, mkc<C>(T(0.5) * (p0.x + pm.x), T(0.5) * (p0.y - pm.y)));
             const C outB = cscale(invn, mkc<C>(T(0.5) * (p0.y + pm.y), T(-0.5) * (p0.x - pm.x)));
@@ -771,7 +802,7 @@ k_x_cross_r(Dims d, const double2 *__restrict__ roots, const C *__restrict__ G, 
             dft_reg<N1, -1>(w, tw, N2);
     #pragma unroll
             for (int k1 = 0; k1 < N1; ++k1) {
-                const C t = (k1 == 0 || sub == 0) ? w[k1] : tw.template mul<-1>(w[k1], sub * k1);
+                const C t = (k1 == 0 || (FP32 && sub == 0)) ? w[k1] : inter(std::integral_constant<int, -1>{}, w[k1], k1);
                 buf[(slot * N1 + k1) * SP + sub] = t;
             }
         }
@@ -1624,7 +1655,7 @@ size_t smem_xcross_h(int n1, int n2, size_t elem) {
 size_t smem_xcross_r(int n1, int n2, size_t elem) {
     const size_t L = 3 * kRWr;
     const size_t s1 = L * n1 * (n2 + 1), s2 = L * n1 * n2;
-    return sizeof(double2) * n1 * n2 + elem * (s1 > s2 ? s1 : s2);
+    return sizeof(double2) * (n1 * n2 + 16 * n1) + elem * (s1 > s2 ? s1 : s2);
 }
 
 template <class C> cudaError_t configure_register_forms(const Dims &d) {
