@@ -101,11 +101,18 @@ __device__ bool tau_chain(int par, int ny, double g, double a, double b, bool ze
 // B-problem right-hand side (MODE_COUPLED), velocity taus of Re grad P, wall
 // divergence, and for MODE_COUPLED the influence correction
 // (src/solver/eqsolve_pv.cpp:241-264, 311-450 without sigma).
+//
+// Only the columns kz <= 0 are solved.  Column -kz has the same k^2, so the
+// same pivots and pressure; its right-hand sides differ only by the sign of
+// the kz derivative, and every operation is linear with the rounding of a
+// negated operand negated, so its solution is this column's with w negated,
+// bit for bit, and its wall divergences are equal.  Both columns are written.
 template <int MODE>
 __global__ void __launch_bounds__(kThreads)
 k_setup_solve(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, SetupArgs A) {
     extern __shared__ double2 sm2[];
     const int ncy = d.ncy, ny = d.NYS, nkx = d.nkx;
+    const int nhalf = (d.NZS + 1) * nkx;   // columns kz <= 0 (kz index 0 .. NZS)
     const int S = ncy * TC;
     double2 *rv = sm2;            // [3][ncy][TC]
     double2 *pc = rv + 3 * S;     // [ncy][TC]
@@ -129,7 +136,7 @@ k_setup_solve(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, Setup
         const int y = i / TC, l = i - (i / TC) * TC;
         const int col = col0 + l;
         double rp = 0.0;
-        if (col < d.ncol) {
+        if (col < nhalf) {
             const long long cm = (long long)col * ncy + y;
             adp[i] = st.ad_p[cm];
             adv[i] = st.ad_v[cm];
@@ -153,7 +160,7 @@ k_setup_solve(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, Setup
         const unsigned mask = (1u << (2 * TC)) - 1u;
         const int l = tid >> 1, par = tid & 1;
         const int col = col0 + l;
-        const bool active = col < d.ncol;
+        const bool active = col < nhalf;
         const int kzi = active ? col / nkx : 0;
         const int kx = active ? col - kzi * nkx : 0;
         const double ax = t.wavx[kx], az = t.wavz[kzi];
@@ -190,8 +197,11 @@ k_setup_solve(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, Setup
                 div1 = (y & 1) ? cadd(div1, cadd(mk(-tang.x, -tang.y), nrm)) : cadd(div1, csub(tang, nrm));
             }
             if (MODE == MODE_BASE) {
+                const int mir = (2 * d.NZS - kzi) * nkx + kx;   // column -kz
                 A.divb_out[col] = div0;
                 A.divb_out[d.ncol + col] = div1;
+                A.divb_out[mir] = div0;
+                A.divb_out[d.ncol + mir] = div1;
                 s_c0[l] = mk(0, 0);
                 s_c1[l] = mk(0, 0);
             } else {
@@ -207,7 +217,7 @@ k_setup_solve(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, Setup
     for (int i = tid; i < S; i += blockDim.x) {
         const int y = i / TC, l = i - (i / TC) * TC;
         const int col = col0 + l;
-        if (col >= d.ncol) continue;
+        if (col >= nhalf) continue;
         const int kzi = col / nkx, kx = col - (col / nkx) * nkx;
         const long long cm = ((long long)kzi * ncy + y) * nkx + kx;   // planar
         double2 p = pc[i];
@@ -220,6 +230,14 @@ k_setup_solve(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, Setup
         }
         A.p_out[cm] = p;
         for (int c = 0; c < 3; ++c) A.v_out[c * d.Ns + cm] = v[c];
+        const int kzm = 2 * d.NZS - kzi;
+        if (kzm != kzi) {
+            const long long mm = ((long long)kzm * ncy + y) * nkx + kx;
+            A.p_out[mm] = p;
+            A.v_out[mm] = v[0];
+            A.v_out[d.Ns + mm] = v[1];
+            A.v_out[2 * d.Ns + mm] = mk(-v[2].x, -v[2].y);
+        }
     }
 }
 
@@ -339,7 +357,7 @@ void setup_solver(const Dims &d, const Tables &t, const PhysParams &pp, double g
     const int nb = (d.ncol + 127) / 128;
     k_wn_ad<<<nb, 128, 0, s>>>(d, t, pp.G_pre, st.wn_p, st.ad_p);
     k_wn_ad<<<nb, 128, 0, s>>>(d, t, g_v, st.wn_v, st.ad_v);
-    const int blocks = (d.ncol + TC - 1) / TC;
+    const int blocks = ((d.NZS + 1) * d.nkx + TC - 1) / TC;   // columns kz <= 0
     const size_t sm = setup_smem(d);
     // influence responses: pressure Dirichlet data (1,0) and (0,1)
     for (int i = 0; i < 2; ++i) {

@@ -66,7 +66,8 @@ def test_local_pencil_matches_single_context(case, ranks, exchange, monkeypatch)
     case at constant flow rate, full Nyquist spectrum, ragged blocks), with the
     exchange by packed buffers and with the fused exchange (z transforms on
     the other ranks' column buffers)."""
-    monkeypatch.setenv("CDNS_Y_TRANSFORM", "matrix")   # the form the rank contexts use
+    monkeypatch.setenv("CDNS_Y_TRANSFORM", "matrix")   # the forms the rank contexts use
+    monkeypatch.setenv("CDNS_X_STAGE", "rows4")
     if case == "channel32":
         m, p = channel_case(32)
         u0 = np.stack(divergence_free_field(m, p, seed=2, amp=0.1, spectrum="k53", mean="loglaw"), axis=-1)
@@ -140,7 +141,8 @@ def test_nccl_step_one_rank(monkeypatch):
     context."""
     import torch
     import torch.distributed as dist
-    monkeypatch.setenv("CDNS_Y_TRANSFORM", "matrix")   # the form the rank contexts use
+    monkeypatch.setenv("CDNS_Y_TRANSFORM", "matrix")   # the forms the rank contexts use
+    monkeypatch.setenv("CDNS_X_STAGE", "rows4")
     m, p = channel_case(32)
     u0 = np.stack(divergence_free_field(m, p, seed=4, amp=0.1), axis=-1)
     uref, pref, _ = _reference(m, p, u0, 3)

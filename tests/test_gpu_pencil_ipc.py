@@ -47,7 +47,8 @@ def _worker(rank, world, port, q):
     here = os.path.dirname(os.path.abspath(__file__))
     root = os.path.dirname(here)
     sys.path[:0] = [here, os.path.join(root, "oracle"), os.path.join(root, "channel-dns_b200")]
-    os.environ["CDNS_Y_TRANSFORM"] = "matrix"   # the form the rank contexts use
+    os.environ["CDNS_Y_TRANSFORM"] = "matrix"   # the forms the rank contexts use
+    os.environ["CDNS_X_STAGE"] = "rows4"
     import torch.distributed as dist
     from cdns import pencil
     dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
@@ -102,7 +103,8 @@ def test_fused_exchange_across_processes(world, monkeypatch):
                 p.kill()
     assert all(p.exitcode == 0 for p in procs)
     m, p, u0 = _case()
-    monkeypatch.setenv("CDNS_Y_TRANSFORM", "matrix")   # the form the rank contexts use
+    monkeypatch.setenv("CDNS_Y_TRANSFORM", "matrix")   # the forms the rank contexts use
+    monkeypatch.setenv("CDNS_X_STAGE", "rows4")
     c = ctx_for(m, p)
     c.set_velocity(u0)
     c.run(1, NSTEPS)
