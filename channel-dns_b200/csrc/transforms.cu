@@ -357,21 +357,39 @@ k_ydct_r(Dims d, const double2 *__restrict__ roots, const double *__restrict__ c
     const bool lok = kx < nkx;
     const Twiddles<double2> tw = load_twiddles<double2>(sm_d, roots, N);
     // ---- x_n, n = 0..N, and partials of Y_1 = sum_{n=1}^{N-1} x_n cos(pi n / N)
+    // rows n = r + R i: all loads of a thread are issued before the first use
+    constexpr int NI = N / R + 1;
     double2 y1 = mk(0.0, 0.0);
+    double2 xv[NI];
     if (!ANA) {
         const double2 *S = (f < A.nsplit ? A.spec0 + (long long)f * d.Ns : A.spec1 + (long long)(f - A.nsplit) * d.Ns) +
                            (long long)kzi * ncy * nkx + kx;
-        for (int n = r; n <= N; n += R) {
-            double2 v = (n < ncy && lok) ? cscale(n == 0 ? A.in0 : A.in1, S[(long long)n * nkx]) : mk(0.0, 0.0);
+#pragma unroll
+        for (int i = 0; i < NI; ++i) {
+            const int n = r + R * i;
+            xv[i] = (n <= N && n < ncy && lok) ? S[(long long)n * nkx] : mk(0.0, 0.0);
+        }
+#pragma unroll
+        for (int i = 0; i < NI; ++i) {
+            const int n = r + R * i;
+            if (n > N) break;
+            double2 v = cscale(n == 0 ? A.in0 : A.in1, xv[i]);
             if (n == 0) v = cadd(v, v);
             X[n * TL + l] = v;
             if (n >= 1 && n < N) y1 = cadd(y1, cscale(cosy[n], v));
         }
     } else {
         const CT *F = A.Fin + (long long)f * d.ny2 * d.fcol + (long long)kzi * nkx + kx;
-        for (int n = r; n <= N; n += R) {
-            const double2 v =
-                lok ? cscale(n == 0 || n == N ? A.inE : A.inI, cto<double2>(F[(long long)n * d.fcol])) : mk(0.0, 0.0);
+#pragma unroll
+        for (int i = 0; i < NI; ++i) {
+            const int n = r + R * i;
+            xv[i] = (n <= N && lok) ? cto<double2>(F[(long long)n * d.fcol]) : mk(0.0, 0.0);
+        }
+#pragma unroll
+        for (int i = 0; i < NI; ++i) {
+            const int n = r + R * i;
+            if (n > N) break;
+            const double2 v = cscale(n == 0 || n == N ? A.inE : A.inI, xv[i]);
             X[n * TL + l] = v;
             if (n >= 1 && n < N) y1 = cadd(y1, cscale(cosy[n], v));
         }
