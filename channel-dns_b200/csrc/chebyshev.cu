@@ -102,15 +102,30 @@ k_curl(Dims d, Tables t, const double2 *__restrict__ u, double2 *__restrict__ om
     const int S = ncy * kColsPerBlock;
     const int col0 = blockIdx.x * kColsPerBlock;
     const int tid = threadIdx.x, w = tid >> 5, L = tid & 31, p = L & 1;
-    for (int i = tid; i < S; i += blockDim.x) {
-        const int y = i / kColsPerBlock, l = i - (i / kColsPerBlock) * kColsPerBlock;
-        const int c2 = col0 + l;
-        if (c2 >= ncol) continue;
-        const int kzi = c2 / nkx, kx = c2 - (c2 / nkx) * nkx;
-        const long long off = ((long long)kzi * ncy + y) * nkx + kx;
-        const int sl = tile_slot<E>(y, l);
+    // the loads of kBatch rows of the tile are issued before the first store
+    constexpr int kBatch = 4;
+    for (int i0 = tid; i0 < S; i0 += kBatch * blockDim.x) {
+        double2 v[kBatch][3];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) tile[c * S + sl] = u[c * d.Ns + off];
+        for (int b = 0; b < kBatch; ++b) {
+            const int i = i0 + b * blockDim.x;
+            const int y = i / kColsPerBlock, l = i - (i / kColsPerBlock) * kColsPerBlock;
+            const int c2 = col0 + l;
+            const bool ok = i < S && c2 < ncol;
+            const int kzi = c2 / nkx, kx = c2 - (c2 / nkx) * nkx;
+            const long long off = ((long long)kzi * ncy + y) * nkx + kx;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) v[b][c] = ok ? u[c * d.Ns + off] : mk(0.0, 0.0);
+        }
+#pragma unroll
+        for (int b = 0; b < kBatch; ++b) {
+            const int i = i0 + b * blockDim.x;
+            const int y = i / kColsPerBlock, l = i - (i / kColsPerBlock) * kColsPerBlock;
+            if (i >= S || col0 + l >= ncol) continue;
+            const int sl = tile_slot<E>(y, l);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) tile[c * S + sl] = v[b][c];
+        }
     }
     __syncthreads();
     const int col = col0 + w;
