@@ -576,6 +576,10 @@ k_x_cross(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 *_
 // FP64 is held to 3 blocks per SM (at most 112 registers; left free, the
 // compiler moves all twiddle loads of a phase ahead and takes 138); FP32 has
 // no minimum (with one it takes 64 registers instead of 56).
+constexpr int kRWr = 4;   // rows per block of the register-form x stage (at most)
+// exchange buffer of k_x_cross_r in complex elements: the step-1 output of 3 kRWr
+// lines ([line][k1][n2], rows padded to n2 + 1; larger than their physical rows)
+__host__ __device__ constexpr int xcross_buf_elems(int n1, int n2) { return 3 * kRWr * n1 * (n2 + 1); }
 template <int N1, int N2, class C, bool MEAN, bool SPLIT = false>
 __global__ void __launch_bounds__(16 * 3 * 4, sizeof(C) == 16 ? 3 : 0)
 k_x_cross_r(Dims d, const double2 *__restrict__ roots, const C *__restrict__ G, C *__restrict__ H, int RW,
@@ -585,6 +589,7 @@ k_x_cross_r(Dims d, const double2 *__restrict__ roots, const C *__restrict__ G, 
     constexpr int SP = N2 + 1;   // padded row of the step-1 output
     extern __shared__ double2 sm_d[];
     C *buf = reinterpret_cast<C *>(sm_d + n + 16 * N1);
+    T *n2s = reinterpret_cast<T *>(buf + xcross_buf_elems(N1, N2));   // [kRWr][n], SPLIT only
     const int L = 3 * RW, L2 = 3 * (RW / 2);
     const int slot = threadIdx.x >> 4, sub = threadIdx.x & 15;
     const int j = blockIdx.y, z0 = blockIdx.x * RW;
@@ -696,24 +701,30 @@ k_x_cross_r(Dims d, const double2 *__restrict__ roots, const C *__restrict__ G, 
                         n2v += (mu * oy - mv * ox) + (uu * moy - vv * mox);
                     }
                 };
-                T a0, a1, a2, b0, b1, b2;
+                // lines (N0 + i N1) of rows 2 pr, 2 pr + 1 leave N2 in n2s for the
+                // line N2(2 pr) + i N2(2 pr + 1), which reads it after the barrier
                 if (kind < 2) {
+                    T a0, a1, a2;
                     prod(2 * pr + kind, a0, a1, a2);
                     v[m] = mkc<C>(a0, a1);
-                } else {
-                    prod(2 * pr, a0, a1, a2);
-                    prod(2 * pr + 1, b0, b1, b2);
-                    v[m] = mkc<C>(a2, b2);
+                    n2s[(2 * pr + kind) * n + x] = a2;
                 }
             }
         }
         __syncthreads();
         if (act3) {
+            if (kind == 2) {
+#pragma unroll
+                for (int m = 0; m < H1; ++m) {
+                    const int x = sub + N2 * (2 * m + h);
+                    v[m] = mkc<C>(n2s[(2 * pr) * n + x], n2s[(2 * pr + 1) * n + x]);
+                }
+            }
             C(&w)[H1] = reinterpret_cast<C(&)[H1]>(v);
             dft_reg<H1, -1>(w, tw, 2 * N2);
             if (h) {
 #pragma unroll
-                for (int k = 1; k < H1; ++k) w[k] = tw.template mul<-1>(w[k], k * N2);   // W_N1^k
+                for (int k = 1; k < H1; ++k) w[k] = mul_kroot<N1, -1>(w[k], k);   // W_N1^k
             }
         }
 #pragma unroll
@@ -736,7 +747,7 @@ k_x_cross_r(Dims d, const double2 *__restrict__ roots, const C *__restrict__ G, 
             dft_reg<H2, -1>(w, tw, 2 * N1);
             if (h) {
 #pragma unroll
-                for (int k = 1; k < H2; ++k) w[k] = tw.template mul<-1>(w[k], k * N1);   // W_N2^k
+                for (int k = 1; k < H2; ++k) w[k] = mul_kroot<N2, -1>(w[k], k);   // W_N2^k
             }
         }
 #pragma unroll
@@ -1650,7 +1661,7 @@ template <typename Fn> bool with_xsplit(int nx2, Fn &&fn) {
     default: return false;
     }
 }
-constexpr int kRWr = 4;
+
 constexpr int kRWm = 4;    // rows per block of the output-reduction x stage
 size_t smem_xmoments_r(int n1, int n2) {
     const size_t L = 3 * kRWm;
@@ -1671,9 +1682,7 @@ size_t smem_xcross_h(int n1, int n2, size_t elem) {
     return sizeof(double2) * n1 * n2 + (size_t)(2 * kXHWarps) * xh_bytes(n1, n2, (int)elem);
 }
 size_t smem_xcross_r(int n1, int n2, size_t elem) {
-    const size_t L = 3 * kRWr;
-    const size_t s1 = L * n1 * (n2 + 1), s2 = L * n1 * n2;
-    return sizeof(double2) * (n1 * n2 + 16 * n1) + elem * (s1 > s2 ? s1 : s2);
+    return sizeof(double2) * (n1 * n2 + 16 * n1) + elem * xcross_buf_elems(n1, n2) + (elem / 2) * kRWr * n1 * n2;
 }
 
 template <class C> cudaError_t configure_register_forms(const Dims &d) {
