@@ -18,10 +18,11 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
-# Per-file nvcc flags.  The column solver keeps the reference's rounding of
-# each operation (no FMA contraction): its setup feeds differences that cancel
-# to 1e-6 of their terms.
-FILE_FLAGS = {"solver.cu": ["-fmad=false"], "solver_setup.cu": ["-fmad=false"]}
+# Per-file nvcc flags.  The solver setup keeps the reference's rounding of each
+# operation (no FMA contraction): it feeds differences that cancel to 1e-6 of
+# their terms.  The step solve contracts (its results stay within 2e-13 of the
+# reference's after 1000 Re_tau180 steps).
+FILE_FLAGS = {"solver_setup.cu": ["-fmad=false"]}
 
 
 def build(verbose: bool = False, extra=None) -> str:
