@@ -21,6 +21,8 @@ constexpr int TC = kColsPerBlock;
 constexpr int kThreads = 32 * TC;
 
 __device__ __forceinline__ double2 cmulc(double2 a, double2 b) { return cmul(cconj(a), b); }   // conj(a) b
+// conj(a) b for an influence value a stored by its nonzero part (inf_imag)
+__device__ __forceinline__ double2 cmulc_inf(double part, bool imag, double2 b) { return cmulc(inf_value(part, imag), b); }
 
 // Transpose of the Chebyshev derivative d_k = sum_{j>k, j-k odd} 2 j f_j,
 // d_0 halved, d_NYS = 0: lf_j = 2 j sum_{k<j, k=j-1 mod 2} g_k, g_0 = ld_0 / 2.
@@ -217,18 +219,18 @@ k_solve_adj(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, AdjArgs
         tile[sl] = lp;
 #pragma unroll
         for (int c = 0; c < 3; ++c) tile[(1 + c) * S + sl] = lv[c];
-        acc[0] = cadd(acc[0], cmulc(st.p_inf[off], lp));
-        acc[1] = cadd(acc[1], cmulc(st.p_inf[Ns + off], lp));
+        acc[0] = cadd(acc[0], cmulc_inf(st.p_inf[off], false, lp));
+        acc[1] = cadd(acc[1], cmulc_inf(st.p_inf[Ns + off], false, lp));
         const int qi = (y + 1) & 1, vi = y & 1;
-        double2 sq = cmulc(st.p_b[off], lp);
+        double2 sq = cmulc_inf(st.p_b[off], false, lp);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            acc[0] = cadd(acc[0], cmulc(st.v_inf[c * Ns + off], lv[c]));
-            acc[1] = cadd(acc[1], cmulc(st.v_inf[(3 + c) * Ns + off], lv[c]));
-            if (c != 1) sq = cadd(sq, cmulc(st.v_b[c * Ns + off], lv[c]));
+            acc[0] = cadd(acc[0], cmulc_inf(st.v_inf[c * Ns + off], inf_imag(c), lv[c]));
+            acc[1] = cadd(acc[1], cmulc_inf(st.v_inf[(3 + c) * Ns + off], inf_imag(c), lv[c]));
+            if (c != 1) sq = cadd(sq, cmulc_inf(st.v_b[c * Ns + off], inf_imag(c), lv[c]));
         }
         acc[2 + qi] = cadd(acc[2 + qi], sq);
-        acc[2 + vi] = cadd(acc[2 + vi], cmulc(st.v_b[Ns + off], lv[1]));
+        acc[2 + vi] = cadd(acc[2 + vi], cmulc_inf(st.v_b[Ns + off], false, lv[1]));
     }
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -274,10 +276,10 @@ k_solve_adj(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, AdjArgs
         const double2 ltail0 = cscale(-pp.Re, ln0), ltail1 = cscale(-pp.Re, ln1);
         const double2 lptop = cscale(pp.Re * 2.0 * ny, ln1);
         const long long o_n = ((long long)kzi * ncy + ny) * nkx + kx, o_n1 = o_n - nkx;
-        lc0 = cadd(lc0, cadd(cmulc(st.p_inf[o_n], lptop),
-                             cadd(cmulc(st.v_inf[Ns + o_n], lvt0), cmulc(st.v_inf[Ns + o_n1], lvt1))));
-        lc1 = cadd(lc1, cadd(cmulc(st.p_inf[Ns + o_n], lptop),
-                             cadd(cmulc(st.v_inf[4 * Ns + o_n], lvt0), cmulc(st.v_inf[4 * Ns + o_n1], lvt1))));
+        lc0 = cadd(lc0, cadd(cmulc_inf(st.p_inf[o_n], false, lptop),
+                             cadd(cmulc_inf(st.v_inf[Ns + o_n], false, lvt0), cmulc_inf(st.v_inf[Ns + o_n1], false, lvt1))));
+        lc1 = cadd(lc1, cadd(cmulc_inf(st.p_inf[Ns + o_n], false, lptop),
+                             cadd(cmulc_inf(st.v_inf[4 * Ns + o_n], false, lvt0), cmulc_inf(st.v_inf[4 * Ns + o_n1], false, lvt1))));
         // c0 = div1 i10 - div0 i11, c1 = div0 i01 - div1 i00
         const double2 i00 = st.inf_div[col], i01 = st.inf_div[ncol + col];
         const double2 i10 = st.inf_div[2 * ncol + col], i11 = st.inf_div[3 * ncol + col];

@@ -106,14 +106,28 @@ void launch_x_adjoint(const Dims &d, const FftPlan &P, const double2 *roots, con
 struct SolverState {
     double *wn_p, *wn_v;        // [ncol]
     double *ad_p, *ad_v;        // [ncol][ncy] (column-major)
-    double2 *p_inf;             // [2][Ns] planar
-    double2 *v_inf;             // [2][3][Ns] planar
+    // Influence and B-problem fields, planar, each stored by its one nonzero
+    // part: the pressure and v are real, u and w purely imaginary (real wall
+    // data and real operators; i kx, i kz enter only through the gradient), so
+    // the other part is an exact zero and is not kept (inf_part).
+    double *p_inf;              // [2][Ns]
+    double *v_inf;              // [2][3][Ns]
     double2 *inf_div;           // [2 (response)][2 (wall)][ncol]
-    double2 *p_b;               // [Ns] planar
-    double2 *v_b;               // [3][Ns] planar
+    double *p_b;                // [Ns]
+    double *v_b;                // [3][Ns]
     double2 *sigma0;            // [2][ncol]
     double *unit;               // [2][ncy] u_dpdx_unit, w_dpdz_unit ; [2*ncy..] qx, qz
 };
+
+// Velocity component c of an influence or B-problem field: imaginary for u
+// and w (c = 0, 2), real for v (c = 1).
+__host__ __device__ inline bool inf_imag(int c) { return c != 1; }
+// The complex value of a stored part; c * value without the products by the
+// exact zero (cmul with a zero part gives the same bits for finite c).
+__device__ inline double2 inf_value(double part, bool imag) { return imag ? mk(0.0, part) : mk(part, 0.0); }
+__device__ inline double2 inf_mul(double2 c, double part, bool imag) {
+    return imag ? fderiv(part, c) : cscale(part, c);
+}
 
 struct PhysParams {
     double Re, G_pre, a_pre0, b_pre0;

@@ -721,14 +721,28 @@ int cdns_debug_copy(cdns_ctx *c, int which, double *out, size_t count) {
         int r;
         if ((r = nonfinite(st.ad_p, Ns, out[0])) || (r = nonfinite(st.ad_v, Ns, out[1])) ||
             (r = nonfinite(st.inf_div, 8 * nc, out[2])) || (r = nonfinite(st.sigma0, 4 * nc, out[3])) ||
-            (r = nonfinite(st.p_inf, 4 * Ns, out[4])) || (r = nonfinite(st.v_b, 6 * Ns, out[5])) ||
+            (r = nonfinite(st.p_inf, 2 * Ns, out[4])) || (r = nonfinite(st.v_b, 3 * Ns, out[5])) ||
             (r = nonfinite(st.unit, 2 * (size_t)d.ncy + 2, out[6])))
             return r;
         return CDNS_OK;
     }
     case 5: src = c->st.inf_div; n = 4 * (size_t)d.ncol; break;
-    case 6: src = c->st.v_inf; n = 6 * (size_t)d.Ns; break;
-    case 7: src = c->st.p_inf; n = 2 * (size_t)d.Ns; break;
+    case 6:
+    case 7: {
+        // stored by their nonzero parts: returned as complex values
+        n = (which == 6 ? 6 : 2) * (size_t)d.Ns;
+        if (count < 2 * n) return fail(CDNS_ERR_ARG, "debug buffer too small");
+        std::vector<double> h(n);
+        CK(cudaMemcpyAsync(h.data(), which == 6 ? c->st.v_inf : c->st.p_inf, n * sizeof(double),
+                           cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        for (size_t i = 0; i < n; ++i) {
+            const int comp = which == 6 ? (int)((i / (size_t)d.Ns) % 3) : 1;
+            out[2 * i] = inf_imag(comp) ? 0.0 : h[i];
+            out[2 * i + 1] = inf_imag(comp) ? h[i] : 0.0;
+        }
+        return CDNS_OK;
+    }
     case 8: src = c->st.sigma0; n = 2 * (size_t)d.ncol; break;
     case 9: src = c->st.wn_p; n = (size_t)d.ncol; break;   // wn_p then wn_v as [2][ncol] doubles
     default: return fail(CDNS_ERR_ARG, "unknown debug buffer");

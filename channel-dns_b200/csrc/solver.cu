@@ -285,11 +285,12 @@ k_solve(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, SolveArgs A
         const double2 c0 = csub(cmul(div1, i10), cmul(div0, i11));
         const double2 c1 = csub(cmul(div0, i01), cmul(div1, i00));
         const long long o_n = ((long long)kzi * ncy + ny) * nkx + kx, o_n1 = o_n - nkx;
-        const double2 ptop = cadd(elem<E>(pv, ny), cadd(cmul(c0, st.p_inf[o_n]), cmul(c1, st.p_inf[d.Ns + o_n])));
-        const double2 vt0 =
-            cadd(elem<E>(v1, ny), cadd(cmul(c0, st.v_inf[d.Ns + o_n]), cmul(c1, st.v_inf[4 * d.Ns + o_n])));
-        const double2 vt1 =
-            cadd(elem<E>(v1, ny - 1), cadd(cmul(c0, st.v_inf[d.Ns + o_n1]), cmul(c1, st.v_inf[4 * d.Ns + o_n1])));
+        const double2 ptop = cadd(elem<E>(pv, ny), cadd(inf_mul(c0, st.p_inf[o_n], false),
+                                                        inf_mul(c1, st.p_inf[d.Ns + o_n], false)));
+        const double2 vt0 = cadd(elem<E>(v1, ny), cadd(inf_mul(c0, st.v_inf[d.Ns + o_n], false),
+                                                       inf_mul(c1, st.v_inf[4 * d.Ns + o_n], false)));
+        const double2 vt1 = cadd(elem<E>(v1, ny - 1), cadd(inf_mul(c0, st.v_inf[d.Ns + o_n1], false),
+                                                           inf_mul(c1, st.v_inf[4 * d.Ns + o_n1], false)));
         const double2 n0 = csub(cscale(-wv, vt0), cscale(pp.Re, tail0));
         const double2 n1 = cadd(cscale(-wv, vt1), cscale(pp.Re, csub(cscale(2.0 * ny, ptop), tail1)));
         if (L == 0) {
@@ -327,14 +328,14 @@ k_solve(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, SolveArgs A
         const int sl = tile_slot<E>(y, l);
         const double2 c0 = s_c0[l], c1 = s_c1[l];
         const double2 sq = s_sg[(y + 1) & 1][l], sv = s_sg[y & 1][l];
-        double2 pr = cadd(tile[sl], cadd(cmul(c0, st.p_inf[off]), cmul(c1, st.p_inf[d.Ns + off])));
-        pr = cadd(pr, cmul(sq, st.p_b[off]));
+        double2 pr = cadd(tile[sl], cadd(inf_mul(c0, st.p_inf[off], false), inf_mul(c1, st.p_inf[d.Ns + off], false)));
+        pr = cadd(pr, inf_mul(sq, st.p_b[off], false));
         double2 v[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            v[c] = cadd(tile[(1 + c) * S + sl],
-                        cadd(cmul(c0, st.v_inf[c * d.Ns + off]), cmul(c1, st.v_inf[(3 + c) * d.Ns + off])));
-            v[c] = cadd(v[c], cmul(c == 1 ? sv : sq, st.v_b[c * d.Ns + off]));
+            v[c] = cadd(tile[(1 + c) * S + sl], cadd(inf_mul(c0, st.v_inf[c * d.Ns + off], inf_imag(c)),
+                                                     inf_mul(c1, st.v_inf[(3 + c) * d.Ns + off], inf_imag(c))));
+            v[c] = cadd(v[c], inf_mul(c == 1 ? sv : sq, st.v_b[c * d.Ns + off], inf_imag(c)));
         }
         if (fix_zero && c2 == zc) {
             tile[sl] = pr;

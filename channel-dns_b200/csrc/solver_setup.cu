@@ -24,8 +24,8 @@ enum SetupMode { MODE_BASE = 1, MODE_COUPLED = 2 };
 
 struct SetupArgs {
     double2 bcp_top, bcp_bot;  // constant pressure wall data
-    double2 *p_out;            // [Ns] planar
-    double2 *v_out;            // [3][Ns] planar
+    double *p_out;             // [Ns] planar, real
+    double *v_out;             // [3][Ns] planar, parts as inf_imag(c)
     double2 *divb_out;         // [2][ncol] raw wall divergence (MODE_BASE)
 };
 
@@ -224,19 +224,22 @@ k_setup_solve(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, Setup
         double2 v[3] = {rv[i], rv[S + i], rv[2 * S + i]};
         if (MODE == MODE_COUPLED) {
             const double2 c0 = s_c0[l], c1 = s_c1[l];
-            p = cadd(p, cadd(cmul(c0, st.p_inf[cm]), cmul(c1, st.p_inf[d.Ns + cm])));
+            p = cadd(p, cadd(cmul(c0, inf_value(st.p_inf[cm], false)), cmul(c1, inf_value(st.p_inf[d.Ns + cm], false))));
             for (int c = 0; c < 3; ++c)
-                v[c] = cadd(v[c], cadd(cmul(c0, st.v_inf[c * d.Ns + cm]), cmul(c1, st.v_inf[(3 + c) * d.Ns + cm])));
+                v[c] = cadd(v[c], cadd(cmul(c0, inf_value(st.v_inf[c * d.Ns + cm], inf_imag(c))),
+                                       cmul(c1, inf_value(st.v_inf[(3 + c) * d.Ns + cm], inf_imag(c)))));
         }
-        A.p_out[cm] = p;
-        for (int c = 0; c < 3; ++c) A.v_out[c * d.Ns + cm] = v[c];
+        // the nonzero parts (the other parts are exact zeros)
+        const double pv = p.x, vv[3] = {v[0].y, v[1].x, v[2].y};
+        A.p_out[cm] = pv;
+        for (int c = 0; c < 3; ++c) A.v_out[c * d.Ns + cm] = vv[c];
         const int kzm = 2 * d.NZS - kzi;
         if (kzm != kzi) {
             const long long mm = ((long long)kzm * ncy + y) * nkx + kx;
-            A.p_out[mm] = p;
-            A.v_out[mm] = v[0];
-            A.v_out[d.Ns + mm] = v[1];
-            A.v_out[2 * d.Ns + mm] = mk(-v[2].x, -v[2].y);
+            A.p_out[mm] = pv;
+            A.v_out[mm] = vv[0];
+            A.v_out[d.Ns + mm] = vv[1];
+            A.v_out[2 * d.Ns + mm] = -vv[2];
         }
     }
 }
@@ -291,17 +294,17 @@ __global__ void k_inf_normalize(Dims d, double a_v1, double2 *inf_div) {
 }
 
 // sigma0 denominators (src/solver/eqsolve_pv.cpp:466-476).
-__global__ void k_sigma0(Dims d, double re, const double *wn_v, const double2 *p_b,
-                         const double2 *v_b, double2 *sigma0) {
+__global__ void k_sigma0(Dims d, double re, const double *wn_v, const double *p_b,
+                         const double *v_b, double2 *sigma0) {
     const int col = blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= d.ncol) return;
     const int kzi = col / d.nkx, kx = col - (col / d.nkx) * d.nkx;
     const int n = d.NYS;
     const long long on = ((long long)kzi * d.ncy + n) * d.nkx + kx;   // planar (kz, n, kx)
     const double w = wn_v[col];
-    const double2 vbn = v_b[d.Ns + on];
-    const double2 vbn1 = v_b[d.Ns + on - d.nkx];
-    const double2 pbn = p_b[on];
+    const double2 vbn = inf_value(v_b[d.Ns + on], false);
+    const double2 vbn1 = inf_value(v_b[d.Ns + on - d.nkx], false);
+    const double2 pbn = inf_value(p_b[on], false);
     sigma0[col] = mk(re + w * vbn.x, w * vbn.y);
     double2 s1 = csub(mk(re + w * vbn1.x, w * vbn1.y), cscale(re * (2.0 * n), pbn));
     if (col == d.zc) s1 = mk(1.0, 0.0);
