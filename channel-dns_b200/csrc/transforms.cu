@@ -149,8 +149,14 @@ __device__ __forceinline__ Twiddles<C> load_lane_twiddles(double2 *sm_d, const d
     return Twiddles<C>{hi + sub, lo + sub};
 }
 
+// Row stride of fft2_lines' exchange between k1 groups: N2 TL padded to = TL
+// (mod 8), so that a quarter-warp whose threads span two k1 groups touches 8
+// distinct 16-byte bank groups (unpadded, N2 TL = 0 mod 8 for the even N2 used).
+__host__ __device__ constexpr int fft2_kstride(int n2, int tl) { return n2 * tl + (((tl - n2 * tl) % 8) + 8) % 8; }
+
 template <int N1, int N2, int SIGN, class C, class Src, class Dst>
 __device__ __forceinline__ void fft2_lines(int TL, const Twiddles<C> &tw, C *S, const Src &src, const Dst &dst) {
+    const int KS = fft2_kstride(N2, TL);
     constexpr int NM = N1 > N2 ? N1 : N2;
     const int t = threadIdx.x;
     C v[NM];
@@ -166,13 +172,13 @@ __device__ __forceinline__ void fft2_lines(int TL, const Twiddles<C> &tw, C *S, 
         dft_reg<N1, SIGN>(w, tw, N2);
 #pragma unroll
         for (int k1 = 0; k1 < N1; ++k1)
-            S[(k1 * N2 + n2) * TL + l1] = (k1 == 0 || n2 == 0) ? w[k1] : tw.template mul<SIGN>(w[k1], n2 * k1);
+            S[k1 * KS + n2 * TL + l1] = (k1 == 0 || n2 == 0) ? w[k1] : tw.template mul<SIGN>(w[k1], n2 * k1);
     }
     __syncthreads();
     if (t < N1 * TL) {
         const int k1 = t / TL, l = t - (t / TL) * TL;
 #pragma unroll
-        for (int m = 0; m < N2; ++m) v[m] = S[(k1 * N2 + m) * TL + l];
+        for (int m = 0; m < N2; ++m) v[m] = S[k1 * KS + m * TL + l];
         C(&w)[N2] = reinterpret_cast<C(&)[N2]>(v);
         dft_reg<N2, SIGN>(w, tw, N1);
 #pragma unroll
@@ -313,8 +319,12 @@ struct YdctDst {
 };
 
 constexpr int kYdctRows = 16;   // row groups of the DCT kernel (16 TL threads)
-__host__ __device__ constexpr size_t ydct_slots(int n, int tl) {
-    return (size_t)n + (size_t)(n + 1) * tl + (size_t)n * tl + (size_t)kYdctRows * tl + tl;
+// x / exchange region of the DCT kernel: the N + 1 rows, or the padded exchange
+__host__ __device__ constexpr int ydct_xslots(int n1, int n2, int tl) {
+    return (n1 * n2 + 1) * tl > n1 * fft2_kstride(n2, tl) ? (n1 * n2 + 1) * tl : n1 * fft2_kstride(n2, tl);
+}
+__host__ __device__ constexpr size_t ydct_slots(int n1, int n2, int tl) {
+    return (size_t)n1 * n2 + (size_t)ydct_xslots(n1, n2, tl) + (size_t)n1 * n2 * tl + (size_t)kYdctRows * tl + tl;
 }
 
 // Operands of the DCT kernels; CT is the stage buffer's complex type (double2,
@@ -347,7 +357,7 @@ k_ydct_r(Dims d, const double2 *__restrict__ roots, const double *__restrict__ c
     constexpr int CH = (N / 2 + R) / R;         // k = 0..N/2 in R chunks of CH
     extern __shared__ double2 sm_d[];
     double2 *X = sm_d + N;
-    double2 *Z = X + (N + 1) * TL;
+    double2 *Z = X + ydct_xslots(N1, N2, TL);
     double2 *P = Z + N * TL;
     double2 *Y1 = P + R * TL;
     const int f = blockIdx.z, kzi = blockIdx.y, kx0 = blockIdx.x * TL;
@@ -1600,6 +1610,7 @@ int z_lines(const Dims &d) {
     return best;
 }
 
+template <typename Fn> bool with_xsplit(int nx2, Fn &&fn);
 // kx lines per block of the DCT kernels: of {8, 11, 13, 16}, the width that
 // keeps the most threads per SM on real lines -- blocks per SM by shared
 // memory (228 KB, 1 KB reserved per block) x 16 TL threads x nkx / (nkx
@@ -1608,10 +1619,15 @@ int ydct_lines(const Dims &d) {
     const char *e = std::getenv("CDNS_YDCT_LINES");
     const int forced = e ? std::atoi(e) : 0;
     if (forced == 8 || forced == 11 || forced == 13 || forced == 16) return forced;
+    int n1 = 1, n2 = d.NY2;
+    with_xsplit(d.NY2, [&](auto a, auto b) {
+        n1 = decltype(a)::value;
+        n2 = decltype(b)::value;
+    });
     int best = 16;
     double best_useful = -1.0;
     for (int tl : {16, 13, 11, 8}) {
-        const size_t bytes = sizeof(double2) * ydct_slots(d.NY2, tl) + 1024;
+        const size_t bytes = sizeof(double2) * ydct_slots(n1, n2, tl) + 1024;
         const int blocks = (int)std::min<size_t>((228u * 1024u) / bytes, 2048 / (16 * tl));
         const int padded = ((d.nkx + tl - 1) / tl) * tl;
         const double useful = (double)blocks * 16 * tl * d.nkx / padded;
@@ -1630,7 +1646,7 @@ template <typename Fn> void with_ydct_lines(int tl, Fn &&fn) {
     default: fn(std::integral_constant<int, 16>{}); break;
     }
 }
-size_t smem_ydct(int n, int tl) { return sizeof(double2) * ydct_slots(n, tl); }
+size_t smem_ydct(int n1, int n2, int tl) { return sizeof(double2) * ydct_slots(n1, n2, tl); }
 // Dims with the widest line tile, for raising the kernels' shared-memory limits
 Dims widest_lines(Dims d) {
     d.ztl = kMaxZLines;
@@ -1670,7 +1686,8 @@ size_t smem_xmoments_r(int n1, int n2) {
 }
 size_t smem_xmoments(const Dims &d) { return sizeof(double2) * (size_t)d.NX2 * (1 + 2 * 3 * kRWm); }
 size_t smem_zfft_r(const Dims &d, int n1, int n2, size_t elem) {
-    return sizeof(double2) * n1 * n2 + elem * ((size_t)n1 * n2 * z_lines(d));
+    // twiddles, then the exchange of fft2_lines: n1 rows of the padded k1 stride
+    return sizeof(double2) * n1 * n2 + elem * ((size_t)n1 * fft2_kstride(n2, z_lines(d)));
 }
 constexpr int kRWar = 2;   // rows per block of the register-form x adjoint (16 * 5 * kRWar threads)
 size_t smem_xadjoint_r(int n1, int n2) {
@@ -1717,7 +1734,7 @@ cudaError_t configure_ydct(const Dims &d) {
         constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
         with_ydct_lines(ydct_lines(d), [&](auto w) {
             constexpr int TL = decltype(w)::value;
-            const int sm = (int)smem_ydct(N1 * N2, TL);
+            const int sm = (int)smem_ydct(N1, N2, TL);
             e = raise_smem(k_ydct_r<N1, N2, true, TL, double2>, sm);
             if (e == cudaSuccess) e = raise_smem(k_ydct_r<N1, N2, false, TL, double2>, sm);
             if (e == cudaSuccess) e = raise_smem(k_ydct_r<N1, N2, true, TL, float2>, sm);
@@ -1885,7 +1902,7 @@ bool ydct(const Dims &d, const Tables &t, int nf, bool ana, const YdctArgs<CT> &
         constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
         with_ydct_lines(tl, [&](auto w) {
             constexpr int TL = decltype(w)::value;
-            const size_t sm = smem_ydct(N1 * N2, TL);
+            const size_t sm = smem_ydct(N1, N2, TL);
             if (ana)
                 k_ydct_r<N1, N2, true, TL, CT><<<grid, 16 * TL, sm, s>>>(d, t.root_y, t.cosy, A);
             else
