@@ -23,9 +23,9 @@ struct Dims {
     int nyh;             // NY2/2+1 (half of the y points, symmetric pairs)
     long long Ns;        // nkz*ncy*nkx complex values per spectral component
     int ztl;             // kx lines per block of the z transforms (0: the padding rule)
-    int xrw;             // register-form x stage: (z, y) rows per block (2 or 4; 0: 4), 3: 4 rows
-                         // with the forward phases split over lane pairs (even N1, N2), or 1:
-                         // the half-warp form (a half-warp per row pair)
+    int xrw;             // register-form x stage: (z, y) rows per block (2 or 4; 0: 4), 3 or 5:
+                         // 4 or 2 rows with the forward phases split over lane pairs (even N1,
+                         // N2), or 1: the half-warp form (a half-warp per row pair)
     int kx0;             // global kx of local column kx = 0 (a pencil rank's kx block; else 0)
     int zc;              // local index of the (kz, kx) = (0, 0) column, -1 if not held here
 };

@@ -587,9 +587,10 @@ k_x_cross(Dims d, FftPlan P, const double2 *__restrict__ roots, const double2 *_
 // compiler moves all twiddle loads of a phase ahead and takes 138); FP32 has
 // no minimum (with one it takes 64 registers instead of 56).
 constexpr int kRWr = 4;   // rows per block of the register-form x stage (at most)
-// exchange buffer of k_x_cross_r in complex elements: the step-1 output of 3 kRWr
-// lines ([line][k1][n2], rows padded to n2 + 1; larger than their physical rows)
-__host__ __device__ constexpr int xcross_buf_elems(int n1, int n2) { return 3 * kRWr * n1 * (n2 + 1); }
+// exchange buffer of k_x_cross_r in complex elements for rw rows: the step-1
+// output of 3 rw lines ([line][k1][n2], rows padded to n2 + 1; larger than their
+// physical rows)
+__host__ __device__ constexpr int xcross_buf_elems(int n1, int n2, int rw) { return 3 * rw * n1 * (n2 + 1); }
 template <int N1, int N2, class C, bool MEAN, bool SPLIT = false>
 __global__ void __launch_bounds__(16 * 3 * 4, sizeof(C) == 16 ? 3 : 0)
 k_x_cross_r(Dims d, const double2 *__restrict__ roots, const C *__restrict__ G, C *__restrict__ H, int RW,
@@ -599,7 +600,7 @@ k_x_cross_r(Dims d, const double2 *__restrict__ roots, const C *__restrict__ G, 
     constexpr int SP = N2 + 1;   // padded row of the step-1 output
     extern __shared__ double2 sm_d[];
     C *buf = reinterpret_cast<C *>(sm_d + n + 16 * N1);
-    T *n2s = reinterpret_cast<T *>(buf + xcross_buf_elems(N1, N2));   // [kRWr][n], SPLIT only
+    T *n2s = reinterpret_cast<T *>(buf + xcross_buf_elems(N1, N2, RW));   // [RW][n], SPLIT only
     const int L = 3 * RW, L2 = 3 * (RW / 2);
     const int slot = threadIdx.x >> 4, sub = threadIdx.x & 15;
     const int j = blockIdx.y, z0 = blockIdx.x * RW;
@@ -1698,8 +1699,8 @@ size_t smem_xadjoint_r(int n1, int n2) {
 size_t smem_xcross_h(int n1, int n2, size_t elem) {
     return sizeof(double2) * n1 * n2 + (size_t)(2 * kXHWarps) * xh_bytes(n1, n2, (int)elem);
 }
-size_t smem_xcross_r(int n1, int n2, size_t elem) {
-    return sizeof(double2) * (n1 * n2 + 16 * n1) + elem * xcross_buf_elems(n1, n2) + (elem / 2) * kRWr * n1 * n2;
+size_t smem_xcross_r(int n1, int n2, size_t elem, int rw = kRWr) {
+    return sizeof(double2) * (n1 * n2 + 16 * n1) + elem * xcross_buf_elems(n1, n2, rw) + (elem / 2) * rw * n1 * n2;
 }
 
 template <class C> cudaError_t configure_register_forms(const Dims &d) {
@@ -1798,9 +1799,11 @@ bool x_cross_r(const Dims &d, const double2 *roots, const C *G, C *H, const doub
         constexpr int N1 = decltype(a)::value, N2 = decltype(b)::value;
         dim3 grid((d.NZ2 + rw - 1) / rw, d.ny2);
         if constexpr (N1 % 2 == 0 && N2 % 2 == 0) {
-            if (d.xrw == 3) {   // 4 rows, forward phases split over lane pairs
-                k_x_cross_r<N1, N2, C, MEAN, true><<<grid, 16 * 3 * rw, smem_xcross_r(N1, N2, sizeof(C)), s>>>(
-                    d, roots, G, H, rw, mean);
+            if (d.xrw == 3 || d.xrw == 5) {   // 4 or 2 rows, forward phases split over lane pairs
+                const int srw = d.xrw == 3 ? 4 : 2;
+                dim3 sgrid((d.NZ2 + srw - 1) / srw, d.ny2);
+                k_x_cross_r<N1, N2, C, MEAN, true><<<sgrid, 16 * 3 * srw, smem_xcross_r(N1, N2, sizeof(C), srw), s>>>(
+                    d, roots, G, H, srw, mean);
                 return;
             }
         }

@@ -83,7 +83,7 @@ int measure_fp32(cdns_ctx *c, Choice &out) {
     {
         float2 *G = reinterpret_cast<float2 *>(c->G), *H = reinterpret_cast<float2 *>(c->H);
         float best_x = 1e30f;
-        for (int rw : {4, 2, 1, 3}) {
+        for (int rw : {4, 2, 1, 3, 5}) {
             Dims dx = d;
             dx.xrw = rw;
             float ms;
@@ -139,7 +139,7 @@ int measure(cdns_ctx *c, Choice &out) {
     // barrier) or the half-warp form (1: a half-warp per row pair, no block barrier)
     {
         float best_x = 1e30f;
-        for (int rw : {4, 2, 1, 3}) {
+        for (int rw : {4, 2, 1, 3, 5}) {
             Dims dx = d;
             dx.xrw = rw;
             float ms;
@@ -175,6 +175,7 @@ void apply_x_stage_env(cdns_ctx *c) {
         else if (std::strcmp(e, "rows2") == 0) c->d.xrw = 2;
         else if (std::strcmp(e, "halfwarp") == 0) c->d.xrw = 1;
         else if (std::strcmp(e, "split") == 0) c->d.xrw = 3;
+        else if (std::strcmp(e, "split2") == 0) c->d.xrw = 5;
     }
 }
 
@@ -324,7 +325,7 @@ int cdns_wisdom_import(const char *path) {
                             &ch.yform, &ch.xrw);
         if (n == 2) ch.xrw = 0;   // entries written before the x-stage choice existed
         if (n < 2 || ch.ztl < 0 || ch.ztl > 17 || (ch.ztl != 0 && ch.ztl < 8) || ch.yform < 0 || ch.yform > 3 ||
-            (ch.xrw != 0 && (ch.xrw < 1 || ch.xrw > 4)))
+            (ch.xrw != 0 && (ch.xrw < 1 || ch.xrw > 5)))
             return fail(CDNS_ERR_ARG, "malformed wisdom entry");
         got[key] = ch;
         pos = end;

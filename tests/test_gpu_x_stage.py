@@ -1,5 +1,5 @@
 """Every form of the register-form x stage (k_x_cross_r with 4 or 2 rows per
-block, with 4 rows and the forward phases split over lane pairs, k_x_cross_h
+block, with 4 or 2 rows and the forward phases split over lane pairs, k_x_cross_h
 with a half-warp per row pair) against the oracle's
 nonlinear term (src/solver/vector_ops.cpp:250-272 with the fine transforms
 of src/fft/transforms.cpp:641-741), on every x length split the register
@@ -15,7 +15,7 @@ from test_gpu_parity import ctx_for, rel_max
 
 pytestmark = pytest.mark.gpu
 
-FORMS = ["rows4", "rows2", "halfwarp", "split"]
+FORMS = ["rows4", "rows2", "halfwarp", "split", "split2"]
 
 
 def mesh_x(nxs, nx2, nzs=8, nz2=32, nys=14, ny2=24):
@@ -43,7 +43,7 @@ def test_x_stage_forms_nonlinear_term(monkeypatch, form, case):
     N_ref, _, B_ref = orc.nonlinear_term(m, cst, u)
     c = ctx_for(m, p)
     # (72 = 8 x 9 has an odd factor: "split" runs the 4-rows form there)
-    assert c.tuning()["x_rows"] == {"rows4": 4, "rows2": 2, "halfwarp": 1, "split": 3}[form]
+    assert c.tuning()["x_rows"] == {"rows4": 4, "rows2": 2, "halfwarp": 1, "split": 3, "split2": 5}[form]
     N, B = c.nonlinear(np.stack(u, axis=-1))
     for k in range(3):
         assert rel_max(N[..., k], N_ref[k]) <= 1e-12
@@ -51,7 +51,7 @@ def test_x_stage_forms_nonlinear_term(monkeypatch, form, case):
     assert np.abs(B[:, 0] - B_ref[0]).max() <= 1e-12 * scale
 
 
-@pytest.mark.parametrize("form", ["halfwarp", "split"])
+@pytest.mark.parametrize("form", ["halfwarp", "split", "split2"])
 @pytest.mark.parametrize("case", ["x48", "x196"])
 def test_x_stage_halfwarp_mixed(monkeypatch, case, form):
     """FP32 stages (mean profiles kept in FP64) through the half-warp and the
@@ -62,7 +62,7 @@ def test_x_stage_halfwarp_mixed(monkeypatch, case, form):
     monkeypatch.setenv("CDNS_X_STAGE", form)
     mesh = cdns.Mesh(m.NX, m.NY, m.NZ, m.NXS, m.NYS, m.NZS, m.NX2, m.NY2, m.NZ2, m.XL, m.ZL)
     cm = cdns.Context(mesh, cdns.Params(Re=p.Re, DT=p.DT), precision=cdns.PRECISION_MIXED)
-    assert cm.tuning()["x_rows"] == {"halfwarp": 1, "split": 3}[form]
+    assert cm.tuning()["x_rows"] == {"halfwarp": 1, "split": 3, "split2": 5}[form]
     N32, _ = cm.nonlinear(u)
     for k in range(3):
         assert orc.rel_l2(N32[..., k], N64[..., k]) <= 1e-5

@@ -32,7 +32,7 @@ def test_wisdom_round_trip(tmp_path):
 @pytest.mark.parametrize("text", ['{"entries": []}',
                                   '{"cdns_wisdom": 1, "entries": [{"key": "k", "ztl": 5, "yform": 0}]}',
                                   '{"cdns_wisdom": 1, "entries": [{"key": "k", "ztl": 12, "yform": 7}]}',
-                                  '{"cdns_wisdom": 1, "entries": [{"key": "k", "ztl": 12, "yform": 1, "xrw": 5}]}'])
+                                  '{"cdns_wisdom": 1, "entries": [{"key": "k", "ztl": 12, "yform": 1, "xrw": 6}]}'])
 def test_wisdom_rejects_malformed(tmp_path, text):
     cdns.wisdom_forget()
     bad = tmp_path / "bad.json"
