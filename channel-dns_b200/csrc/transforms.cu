@@ -295,12 +295,13 @@ k_z_forward_peers(Dims d, const double2 *__restrict__ roots, const double2 *__re
 // shared rows [n][l].  Phases (barriers between):
 //   load x_n (n = 0..N) and each thread's partial of Y_1's sum over its rows;
 //   Z = DFT_N(y) (fft2_lines; the exchange aliases x, read before its barrier);
-//   even outputs from Z pairs, and each thread's chunk of the odd outputs'
-//   prefix sum (16 consecutive-k chunks per line);
+//   even outputs from Z pairs, stored from registers, and each thread's chunk
+//   of the odd outputs' prefix sum (16 consecutive-k chunks per line);
 //   the carry of the earlier chunks (a fixed-order sum of their totals) and
-//   the odd outputs; stores along kx.
-// Shared memory: twiddles [N], x / exchange / outputs [(N+1)][TL], Z [N][TL],
-// partials [16][TL] (Y_1's, then the chunk totals), Y_1 [TL].
+//   the odd outputs, stored from registers.  Stores run along kx (11-16 lines of
+//   one row per thread group), as the loads do.
+// Shared memory: twiddles [N], x / exchange [(N+1)][TL] (or the padded
+// exchange), Z [N][TL], partials [16][TL] (Y_1's, then the chunk totals), Y_1 [TL].
 // ---------------------------------------------------------------------------
 struct YdctSrc {
     const double2 *X;
@@ -415,6 +416,28 @@ k_ydct_r(Dims d, const double2 *__restrict__ roots, const double *__restrict__ c
     // ---- Z = DFT_N(y) (the exchange buffer aliases X: read before its barrier)
     fft2_lines<N1, N2, -1>(TL, tw, X, YdctSrc{X, cosy, TL, N}, YdctDst{Z, TL});
     __syncthreads();
+    // ---- outputs, stored from registers as they are formed ----------------
+    // (row j of the line: synthesis F_j, j = 0..N; analysis S_j, j <= NYS)
+    CT *Fo = nullptr;
+    double2 *So = nullptr;
+    if (!ANA) Fo = A.Fout + (long long)f * d.ny2 * d.fcol + (long long)kzi * nkx + kx;
+    else So = A.S + (long long)f * d.Ns + (long long)kzi * ncy * nkx + kx;
+    // mean profile (kz, kx) = (0, 0) of FP32 stages: kept in FP64, out of the
+    // FP32 buffer (its imaginary part is round-off of a real profile)
+    const bool to_mean = !ANA && A.mean && kzi == d.NZS && kx == 0;
+    auto out = [&](int j, double2 v) {
+        if (!lok) return;
+        if (!ANA) {
+            if (to_mean) {
+                A.mean[f * d.ny2 + j] = v.x;
+                Fo[(long long)j * d.fcol] = mkc<CT>(0.0, 0.0);
+            } else {
+                Fo[(long long)j * d.fcol] = cto<CT>(cscale(j == 0 || j == N ? A.outE : A.outI, v));
+            }
+        } else if (j < ncy) {
+            So[(long long)j * nkx] = cscale(j == 0 ? A.s0 : A.sk, v);
+        }
+    };
     // ---- even outputs X_2k = (Z_k + Z_{N-k}) / 2; chunk sums of i (Z_q - Z_{N-q}) / 2
     double2 part[CH];
     double2 run = mk(0.0, 0.0);
@@ -423,7 +446,7 @@ k_ydct_r(Dims d, const double2 *__restrict__ roots, const double *__restrict__ c
         const int k = r * CH + c;
         if (k <= N / 2) {
             const double2 zk = Z[k * TL + l], zm = Z[((N - k) % N) * TL + l];
-            X[(2 * k) * TL + l] = cscale(0.5, cadd(zk, zm));
+            out(2 * k, cscale(0.5, cadd(zk, zm)));
             if (k >= 1 && k <= M) {
                 const double2 dz = csub(zk, zm);
                 run = cadd(run, mk(-0.5 * dz.y, 0.5 * dz.x));
@@ -434,36 +457,14 @@ k_ydct_r(Dims d, const double2 *__restrict__ roots, const double *__restrict__ c
     P[r * TL + l] = run;
     __syncthreads();
     // ---- odd outputs X_{2k+1} = Y_1 + sum_{q=1..k} i (Z_q - Z_{N-q}) / 2 -------
-    {
-        double2 carry = mk(0.0, 0.0);
-        for (int q = 0; q < r; ++q) carry = cadd(carry, P[q * TL + l]);
-        const double2 y = Y1[l];
-        if (r == 0) X[1 * TL + l] = y;
+    double2 carry = mk(0.0, 0.0);
+    for (int q = 0; q < r; ++q) carry = cadd(carry, P[q * TL + l]);
+    const double2 y = Y1[l];
+    if (r == 0) out(1, y);
 #pragma unroll
-        for (int c = 0; c < CH; ++c) {
-            const int k = r * CH + c;
-            if (k >= 1 && k <= M) X[(2 * k + 1) * TL + l] = cadd(y, cadd(carry, part[c]));
-        }
-    }
-    __syncthreads();
-    // ---- store along kx ------------------------------------------------------
-    if (!lok) return;
-    if (!ANA) {
-        CT *Fo = A.Fout + (long long)f * d.ny2 * d.fcol + (long long)kzi * nkx + kx;
-        if (A.mean && kzi == d.NZS && kx == 0) {
-            // mean profile (kz, kx) = (0, 0): kept in FP64, out of the FP32 stages
-            // (its imaginary part is round-off of a real profile)
-            for (int j = r; j <= N; j += R) {
-                A.mean[f * d.ny2 + j] = X[j * TL + l].x;
-                Fo[(long long)j * d.fcol] = mkc<CT>(0.0, 0.0);
-            }
-        } else {
-            for (int j = r; j <= N; j += R)
-                Fo[(long long)j * d.fcol] = cto<CT>(cscale(j == 0 || j == N ? A.outE : A.outI, X[j * TL + l]));
-        }
-    } else {
-        double2 *So = A.S + (long long)f * d.Ns + (long long)kzi * ncy * nkx + kx;
-        for (int k = r; k < ncy; k += R) So[(long long)k * nkx] = cscale(k == 0 ? A.s0 : A.sk, X[k * TL + l]);
+    for (int c = 0; c < CH; ++c) {
+        const int k = r * CH + c;
+        if (k >= 1 && k <= M) out(2 * k + 1, cadd(y, cadd(carry, part[c])));
     }
 }
 
