@@ -2,6 +2,7 @@
 // graphs) and the extern "C" entry points declared in include/cdns.h.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -844,7 +845,14 @@ int batch_step(cdns_batch *b, int it) {
         cudaGraph_t graph;
         CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
         CK(cudaEventRecord(b->fork, b->stream));
-        for (size_t i = 0; i < b->members.size(); ++i) {
+        // branches captured largest member first (more spectral values first), so
+        // that the long launches start early and the small members fill in
+        std::vector<size_t> order(b->members.size());
+        for (size_t i = 0; i < order.size(); ++i) order[i] = i;
+        std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) {
+            return b->members[x]->d.Ns > b->members[y]->d.Ns;
+        });
+        for (size_t i : order) {
             cdns_ctx *m = b->members[i];
             double a0, a1, b0, b1, g;
             step_coefficients(it, m->DT, m->pp.Re, a0, a1, b0, b1, g);
