@@ -111,6 +111,14 @@ template <int MODE>
 __global__ void __launch_bounds__(kThreads)
 k_setup_solve(Dims d, Tables t, PhysParams pp, double g_v, SolverState st, SetupArgs A) {
     extern __shared__ double2 sm2[];
+    if (MODE == MODE_BASE && blockIdx.y == 1) {
+        // the second influence response: pressure data (0, 1), its own outputs
+        A.bcp_top = mk(0.0, 0.0);
+        A.bcp_bot = mk(1.0, 0.0);
+        A.p_out += d.Ns;
+        A.v_out += 3 * d.Ns;
+        A.divb_out += 2 * d.ncol;
+    }
     const int ncy = d.ncy, ny = d.NYS, nkx = d.nkx;
     const int nhalf = (d.NZS + 1) * nkx;   // columns kz <= 0 (kz index 0 .. NZS)
     const int S = ncy * TC;
@@ -249,10 +257,15 @@ size_t setup_smem(const Dims &d) {
     return sizeof(double2) * 6 * S + sizeof(double) * (2 * S + 3 * (size_t)d.ncy);
 }
 
-// EqSolvePV::build_wn_ad (src/solver/eqsolve_pv.cpp:148-168), one thread per column.
-__global__ void k_wn_ad(Dims d, Tables t, double g, double *wn, double *ad) {
+// EqSolvePV::build_wn_ad (src/solver/eqsolve_pv.cpp:148-168), one thread per column;
+// blockIdx.y = 0: the pressure operator (g = G_pre), 1: the velocity operator (g_v).
+__global__ void k_wn_ad(Dims d, Tables t, double g_p, double g_v, double *wn_p, double *ad_p, double *wn_v,
+                        double *ad_v) {
     const int col = blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= d.ncol) return;
+    const bool vel = blockIdx.y == 1;
+    const double g = vel ? g_v : g_p;
+    double *wn = vel ? wn_v : wn_p, *ad = vel ? ad_v : ad_p;
     const int kzi = col / d.nkx, kx = col - (col / d.nkx) * d.nkx;
     const double ax = t.wavx[kx], az = t.wavz[kzi];
     const double w = -((ax * ax + az * az) + g);
@@ -358,19 +371,19 @@ cudaError_t configure_setup_kernels(const Dims &d) {
 void setup_solver(const Dims &d, const Tables &t, const PhysParams &pp, double g_v, SolverState &st,
                   double2 *, cudaStream_t s) {
     const int nb = (d.ncol + 127) / 128;
-    k_wn_ad<<<nb, 128, 0, s>>>(d, t, pp.G_pre, st.wn_p, st.ad_p);
-    k_wn_ad<<<nb, 128, 0, s>>>(d, t, g_v, st.wn_v, st.ad_v);
+    k_wn_ad<<<dim3(nb, 2), 128, 0, s>>>(d, t, pp.G_pre, g_v, st.wn_p, st.ad_p, st.wn_v, st.ad_v);
     const int blocks = ((d.NZS + 1) * d.nkx + TC - 1) / TC;   // columns kz <= 0
     const size_t sm = setup_smem(d);
-    // influence responses: pressure Dirichlet data (1,0) and (0,1)
-    for (int i = 0; i < 2; ++i) {
+    // influence responses: pressure Dirichlet data (1,0) and (0,1), in one launch
+    // (blockIdx.y = the response)
+    {
         SetupArgs A{};
-        A.bcp_top = mk((double)(1 - i), 0.0);
-        A.bcp_bot = mk((double)i, 0.0);
-        A.p_out = st.p_inf + (long long)i * d.Ns;
-        A.v_out = st.v_inf + (long long)i * 3 * d.Ns;
-        A.divb_out = st.inf_div + (long long)i * 2 * d.ncol;
-        k_setup_solve<MODE_BASE><<<blocks, kThreads, sm, s>>>(d, t, pp, g_v, st, A);
+        A.bcp_top = mk(1.0, 0.0);
+        A.bcp_bot = mk(0.0, 0.0);
+        A.p_out = st.p_inf;
+        A.v_out = st.v_inf;
+        A.divb_out = st.inf_div;
+        k_setup_solve<MODE_BASE><<<dim3(blocks, 2), kThreads, sm, s>>>(d, t, pp, g_v, st, A);
     }
     k_inf_normalize<<<nb, 128, 0, s>>>(d, pp.a_V[1], st.inf_div);
     {
