@@ -431,8 +431,9 @@ class Context:
 
     def tuning(self) -> dict:
         """{"z_lines": kx lines per z-transform block (0: rule), "y_synthesis":
-        "fft" or "matrix", "y_analysis": "fft" or "matrix", "x_rows": rows per
-        x-stage block (0: 4)}."""
+        "fft" or "matrix", "y_analysis": "fft" or "matrix", "x_rows": the
+        x-stage form (4 or 2 rows per block, 0: 4; 1: half-warp form; 3 or 5:
+        lane-pair split form with 4 or 2 rows)}."""
         out = np.zeros(4, dtype=np.int32)
         _check(lib().cdns_get_tuning(self._h, out.ctypes.data_as(ctypes.c_void_p)))
         return {"z_lines": int(out[0]), "y_synthesis": "fft" if out[1] else "matrix",

@@ -227,9 +227,12 @@ int cdns_solve(cdns_ctx *ctx, double g, const double *rhs_velocity, const double
  * length-NY2 FFT per column), by timing the candidates on its own buffers the
  * first time a mesh is seen on a device in the process (CDNS_TUNE=0 in the
  * environment keeps fixed rules; CDNS_Y_TRANSFORM=matrix|fft fixes the
- * Chebyshev form; CDNS_WISDOM=<file> imports that wisdom file once per process
+ * Chebyshev form, CDNS_X_STAGE=rows4|rows2|halfwarp|split|split2 the x-stage
+ * form; CDNS_WISDOM=<file> imports that wisdom file once per process
  * and exports to it after each new measurement).  cdns_tune times again; cdns_get_tuning writes
- * {z lines, synthesis FFT form, analysis FFT form, x-stage rows} into out[4];
+ * {z lines, synthesis FFT form, analysis FFT form, x-stage form} into out[4]
+ * (x-stage form: 4 or 2 rows per block, 1 the half-warp form, 3 or 5 the
+ * lane-pair split form with 4 or 2 rows);
  * cdns_wisdom_export / _import save and load the choices as JSON (host-only
  * calls); cdns_wisdom_forget empties the process cache. */
 int cdns_tune(cdns_ctx *ctx);
